@@ -1,0 +1,299 @@
+"""Python bindings of the checkers for the all-sources shortest-path hot path.
+
+TEST INFRASTRUCTURE ONLY. Nothing in the product library imports this package: only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use it, as the checker and as the
+timed CPU baseline, never as the thing measured or shipped.
+
+Two checkers live here:
+
+* ``Restatement`` binds ``libngx_oracle.so``, the project's C restatement (``ngx_oracle.c``) of the
+  reference's Dijkstra, APSP summary, Brandes and the CPL/efficiency gradient, with FP64 arc lengths.
+* ``Reference`` binds ``_ref/libngx_ref.so``, the reference implementation's own C++ sources compiled
+  against single-rank shims (``ref_harness.cpp``, ``Makefile``). It exists only where the reference
+  sources were present at build time; on other machines the committed golden fixtures under
+  ``tests/golden/`` carry its outputs.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATEMENT_SO = os.path.join(HERE, "libngx_oracle.so")
+REFERENCE_SO = os.path.join(HERE, "_ref", "libngx_ref.so")
+REFERENCE_GTESTS = os.path.join(HERE, "_ref", "ref_gtests")
+REFERENCE_SOURCES = os.environ.get("NGX_REFERENCE_DIR", "/root/reference")
+
+METRIC_REGULAR = 0
+METRIC_INVERSE = 1
+
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+
+
+def build(reference: bool | None = None, quiet: bool = True) -> None:
+    """Compile the restatement and, when the reference sources exist here, the reference harness."""
+    out = subprocess.DEVNULL if quiet else None
+    subprocess.run(["make", "-C", HERE, "restatement"], check=True, stdout=out)
+    if reference is None:
+        reference = os.path.isdir(os.path.join(REFERENCE_SOURCES, "source"))
+    if reference:
+        subprocess.run(["make", "-C", HERE, "-j8", "reference", f"REF={REFERENCE_SOURCES}"], check=True, stdout=out)
+
+
+class _Graph(C.Structure):
+    _fields_ = [
+        ("n", C.c_int64),
+        ("m", C.c_int64),
+        ("row_ptr", C.POINTER(C.c_int64)),
+        ("col", C.POINTER(C.c_int32)),
+        ("w", C.POINTER(C.c_double)),
+    ]
+
+
+class _Totals(C.Structure):
+    _fields_ = [
+        ("sum_distances", C.c_double),
+        ("sum_inverse", C.c_double),
+        ("sum_distances_sequential", C.c_double),
+        ("sum_inverse_sequential", C.c_double),
+        ("diameter", C.c_double),
+        ("unreachable", C.c_uint64),
+        ("reached_pairs", C.c_uint64),
+        ("traversed_arcs", C.c_uint64),
+        ("hist_overflow", C.c_uint64),
+        ("cpl", C.c_double),
+        ("efficiency", C.c_double),
+    ]
+
+
+@dataclass
+class Csr:
+    """Out-arc CSR with FP64 weights (int32 targets, int64 offsets)."""
+
+    n: int
+    row_ptr: np.ndarray
+    col: np.ndarray
+    w: np.ndarray
+
+    @property
+    def m(self) -> int:
+        return int(self.row_ptr[-1]) if self.n > 0 else 0
+
+    @staticmethod
+    def from_arrays(n, row_ptr, col, w) -> "Csr":
+        return Csr(
+            int(n),
+            np.ascontiguousarray(row_ptr, dtype=np.int64),
+            np.ascontiguousarray(col, dtype=np.int32),
+            np.ascontiguousarray(w, dtype=np.float64),
+        )
+
+
+def _totals_dict(t: _Totals) -> dict:
+    return {name: getattr(t, name) for name, _ in _Totals._fields_}
+
+
+class Restatement:
+    """ctypes binding of libngx_oracle.so (see ngx_oracle.h)."""
+
+    def __init__(self, path: str = RESTATEMENT_SO):
+        if not os.path.exists(path):
+            build(reference=False)
+        lib = C.CDLL(path)
+        lib.ngxo_sssp.argtypes = [C.POINTER(_Graph), C.c_int64, C.c_int, _f64p]
+        lib.ngxo_apsp.argtypes = [
+            C.POINTER(_Graph), C.c_void_p, C.c_int64, C.c_int, C.c_int64, C.c_double, C.c_void_p,
+            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(_Totals),
+        ]
+        lib.ngxo_brandes.argtypes = [C.POINTER(_Graph), C.c_void_p, C.c_int64, _f64p]
+        lib.ngxo_apsp_grad.argtypes = [C.POINTER(_Graph), C.c_void_p, C.c_int64, _f64p, _f64p, C.POINTER(_Totals)]
+        lib.ngxo_exact_sum.argtypes = [_f64p, C.c_int64]
+        lib.ngxo_exact_sum.restype = C.c_double
+        self.lib = lib
+
+    @staticmethod
+    def _graph(g: Csr) -> _Graph:
+        return _Graph(
+            g.n, g.m,
+            g.row_ptr.ctypes.data_as(C.POINTER(C.c_int64)),
+            g.col.ctypes.data_as(C.POINTER(C.c_int32)),
+            g.w.ctypes.data_as(C.POINTER(C.c_double)),
+        )
+
+    def exact_sum(self, x) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        return self.lib.ngxo_exact_sum(x, x.size)
+
+    def sssp(self, g: Csr, source: int, metric: int = METRIC_REGULAR) -> np.ndarray:
+        dist = np.empty(max(g.n, 1), dtype=np.float64)
+        rc = self.lib.ngxo_sssp(C.byref(self._graph(g)), source, metric, dist)
+        if rc != 0:
+            raise ValueError(f"ngxo_sssp failed ({rc})")
+        return dist[: g.n]
+
+    def apsp(self, g: Csr, sources=None, metric: int = METRIC_REGULAR, bins: int = 0, hist_max: float = 0.0) -> dict:
+        srcs = None if sources is None else np.ascontiguousarray(sources, dtype=np.int64)
+        k = g.n if srcs is None else srcs.size
+        per = {
+            "sum": np.zeros(k, np.float64), "max": np.zeros(k, np.float64), "sum_inv": np.zeros(k, np.float64),
+            "sum_inv_seq": np.zeros(k, np.float64), "unreachable": np.zeros(k, np.uint64),
+            "arcs": np.zeros(k, np.uint64),
+        }
+        hist = np.zeros(bins, np.uint64) if bins > 0 else None
+        totals = _Totals()
+        ptr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
+        rc = self.lib.ngxo_apsp(
+            C.byref(self._graph(g)), ptr(srcs), k, metric, bins, hist_max, ptr(hist),
+            ptr(per["sum"]), ptr(per["max"]), ptr(per["sum_inv"]), ptr(per["sum_inv_seq"]),
+            ptr(per["unreachable"]), ptr(per["arcs"]), C.byref(totals),
+        )
+        if rc != 0:
+            raise ValueError(f"ngxo_apsp failed ({rc})")
+        out = _totals_dict(totals)
+        out["per_source"] = per
+        out["hist"] = hist
+        out["cluster_sizes"] = _cluster_sizes(g.n, per["unreachable"])
+        return out
+
+    def brandes(self, g: Csr, sources=None) -> np.ndarray:
+        srcs = None if sources is None else np.ascontiguousarray(sources, dtype=np.int64)
+        k = g.n if srcs is None else srcs.size
+        bc = np.zeros(max(g.n, 1), np.float64)
+        rc = self.lib.ngxo_brandes(C.byref(self._graph(g)), None if srcs is None else srcs.ctypes.data, k, bc)
+        if rc != 0:
+            raise ValueError(f"ngxo_brandes failed ({rc})")
+        return bc[: g.n]
+
+    def apsp_grad(self, g: Csr, sources=None):
+        srcs = None if sources is None else np.ascontiguousarray(sources, dtype=np.int64)
+        k = g.n if srcs is None else srcs.size
+        dcpl = np.zeros(max(g.m, 1), np.float64)
+        deff = np.zeros(max(g.m, 1), np.float64)
+        totals = _Totals()
+        rc = self.lib.ngxo_apsp_grad(C.byref(self._graph(g)), None if srcs is None else srcs.ctypes.data, k, dcpl, deff, C.byref(totals))
+        if rc != 0:
+            raise ValueError(f"ngxo_apsp_grad failed ({rc})")
+        return dcpl[: g.m], deff[: g.m], _totals_dict(totals)
+
+
+def _cluster_sizes(n: int, unreachable: np.ndarray) -> dict:
+    """cluster_sizes of AllPairsShortestPath.h:139-140: reachable count (incl. the source) -> number of sources."""
+    out: dict[int, int] = {}
+    for u in np.asarray(unreachable, dtype=np.int64):
+        key = int(n - u)
+        out[key] = out.get(key, 0) + 1
+    return out
+
+
+class Reference:
+    """ctypes binding of the reference's own code built from source (oracle/_ref/libngx_ref.so)."""
+
+    def __init__(self, path: str = REFERENCE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        lib = C.CDLL(path)
+        lib.ngxref_last_error.restype = C.c_char_p
+        lib.ngxref_fixture_name.restype = C.c_char_p
+        self.lib = lib
+
+    @staticmethod
+    def available(path: str = REFERENCE_SO) -> bool:
+        return os.path.exists(path)
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise RuntimeError(self.lib.ngxref_last_error().decode())
+
+    def fixture_names(self) -> list[str]:
+        return [self.lib.ngxref_fixture_name(i).decode() for i in range(self.lib.ngxref_fixture_count())]
+
+    def _read_csr(self, call) -> tuple[int, np.ndarray, np.ndarray, np.ndarray]:
+        n, m = C.c_int64(), C.c_int64()
+        self._check(call(C.byref(n), C.byref(m), None, None, None, C.c_int64(0)))
+        row_ptr = np.zeros(n.value + 1, np.int64)
+        col = np.zeros(max(m.value, 1), np.int32)
+        w = np.zeros(max(m.value, 1), np.int32)
+        self._check(call(C.byref(n), C.byref(m), row_ptr.ctypes.data_as(C.c_void_p), col.ctypes.data_as(C.c_void_p),
+                         w.ctypes.data_as(C.c_void_p), C.c_int64(m.value)))
+        return n.value, row_ptr, col[: m.value], w[: m.value]
+
+    def fixture_csr(self, index: int):
+        return self._read_csr(lambda *a: self.lib.ngxref_fixture_csr(C.c_int(index), *a))
+
+    def load_csr(self, path: str, remove_self_arcs=False, undirected=False, one_weight=False):
+        return self._read_csr(lambda *a: self.lib.ngxref_load_csr(path.encode(), int(remove_self_arcs), int(undirected), int(one_weight), *a))
+
+    def graph(self, n, row_ptr, col, w_int) -> "RefGraph":
+        handle = C.c_void_p()
+        row_ptr = np.ascontiguousarray(row_ptr, np.int64)
+        col = np.ascontiguousarray(col, np.int32)
+        w_int = np.ascontiguousarray(w_int, np.int32)
+        self._check(self.lib.ngxref_graph_create(C.c_int64(n), row_ptr.ctypes.data_as(C.c_void_p), col.ctypes.data_as(C.c_void_p),
+                                                  w_int.ctypes.data_as(C.c_void_p), C.byref(handle)))
+        return RefGraph(self, handle, n)
+
+    def fixture_graph(self, index: int) -> "RefGraph":
+        handle = C.c_void_p()
+        self._check(self.lib.ngxref_fixture_graph(C.c_int(index), C.byref(handle)))
+        n, _, _, _ = self.fixture_csr(index)
+        return RefGraph(self, handle, n)
+
+
+class RefGraph:
+    def __init__(self, ref: Reference, handle, n: int):
+        self.ref, self.handle, self.n = ref, handle, n
+
+    def __del__(self):
+        try:
+            self.ref.lib.ngxref_graph_destroy(self.handle)
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+    def csr(self):
+        """(n, row_ptr, col, w_int32) in the reference's stored arc order."""
+        return self.ref._read_csr(lambda *a: self.ref.lib.ngxref_graph_csr(self.handle, *a))
+
+    def _apsp_out(self, call) -> dict:
+        cpl, eff, dia, un, ln = C.c_double(), C.c_double(), C.c_double(), C.c_uint64(), C.c_int64()
+        cap = 4096
+        keys = np.zeros(cap, np.uint64)
+        cnts = np.zeros(cap, np.uint64)
+        self.ref._check(call(C.byref(cpl), C.byref(eff), C.byref(dia), C.byref(un), keys.ctypes.data_as(C.c_void_p),
+                             cnts.ctypes.data_as(C.c_void_p), C.c_int64(cap), C.byref(ln)))
+        return {"cpl": cpl.value, "efficiency": eff.value, "diameter": dia.value, "unreachable": un.value,
+                "cluster_sizes": {int(keys[i]): int(cnts[i]) for i in range(min(ln.value, cap))}}
+
+    def apsp(self, inverse=False, queue=0) -> dict:
+        return self._apsp_out(lambda *a: self.ref.lib.ngxref_apsp(self.handle, int(inverse), int(queue), *a))
+
+    def apsp_delta_stepping(self, delta: int, epoch: int) -> dict:
+        return self._apsp_out(lambda *a: self.ref.lib.ngxref_apsp_delta_stepping(self.handle, C.c_uint64(delta), int(epoch), *a))
+
+    def sssp_rows(self, sources, inverse=False, queue=0):
+        srcs = np.ascontiguousarray(sources, np.int64)
+        rows = np.zeros((srcs.size, self.n), np.float64 if inverse else np.uint64)
+        summary = np.zeros((srcs.size, 4), np.float64)
+        self.ref._check(self.ref.lib.ngxref_sssp_rows(self.handle, int(inverse), int(queue), srcs.ctypes.data_as(C.c_void_p),
+                                                      C.c_int64(srcs.size), rows.ctypes.data_as(C.c_void_p), summary.ctypes.data_as(C.c_void_p)))
+        return rows, summary
+
+    def delta_stepping(self, sources, delta: int, epoch: int):
+        srcs = np.ascontiguousarray(sources, np.int64)
+        summary = np.zeros((srcs.size, 4), np.float64)
+        self.ref._check(self.ref.lib.ngxref_delta_stepping(self.handle, C.c_uint64(delta), int(epoch), srcs.ctypes.data_as(C.c_void_p),
+                                                           C.c_int64(srcs.size), summary.ctypes.data_as(C.c_void_p)))
+        return summary
+
+    def betweenness(self, algorithm=0):
+        bc = np.zeros(max(self.n, 1), np.float64)
+        avg = C.c_double()
+        self.ref._check(self.ref.lib.ngxref_betweenness(self.handle, int(algorithm), bc.ctypes.data_as(C.c_void_p), C.byref(avg)))
+        return bc[: self.n], avg.value
