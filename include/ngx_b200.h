@@ -1,0 +1,150 @@
+/*
+ * neurograph-b200: C ABI of the B200 (sm_100a) library for neurograph's all-sources shortest-path hot path.
+ *
+ * One call covers what the reference computes with one Dijkstra (or delta-stepping, or Brandes) run per source:
+ * all sources run as batched multi-source delta-stepping on the GPU, each distance row is reduced on the fly into
+ * the APSP summaries, and the N x N distance matrix never reaches memory.
+ *
+ * Conventions
+ *  - Every entry point returns an ngx_status and never aborts or throws; ngx_last_error() describes the last failure
+ *    of the calling thread.
+ *  - The library owns all device memory it allocates and never frees caller pointers. Output arrays are
+ *    caller-allocated HOST arrays of the documented length.
+ *  - Handles are opaque. One graph handle owns one CUDA stream and is not thread-safe; separate handles may be used
+ *    from separate threads.
+ *  - Vertex ids are 0-based and global (the reference's prefix_distribution[rank] + local id, one rank).
+ *  - Arc lengths: |w| (regular metric) or 1/|w| (inverse metric), as DijkstraCommon::transform_weight
+ *    (source/metrics/paths/DijkstraVariants/DijkstraCommon.h:36-54). A zero weight is an absent arc, as the
+ *    reference drops zero-weight arcs when it builds its graph (source/graph/DistributedGraph.cpp:174-176).
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *  - ngx_graph_create        DistributedGraph::construct_graph + the per-rank RMA arc windows
+ *                            (source/graph/DistributedGraph.cpp:46-127, DistributedGraph.h:218-311)
+ *  - ngx_apsp                AllPairsShortestPath::compute_apsp / compute_apsp_inverse / compute_apsp_delta_stepping
+ *                            (source/metrics/paths/AllPairsShortestPath.h:54-98), with the per-source loop over
+ *                            Dijkstra::compute_sssp (Dijkstra.h:55-98) or DeltaStepping::compute_shortest_distances
+ *                            (DeltaStepping.h:36-82) and summarize_distances (types/SsspResult.h:42-64) fused in
+ *  - ngx_sssp_rows           Dijkstra::compute_sssp's distance buffer (Dijkstra.h:55-98), for chosen sources
+ *  - ngx_brandes             BetweennessCentrality::compute_average_betweenness_centrality with BrandesVariant
+ *                            (BetweennessCentrality.h:46-80, BetweennessCentralityVariants/BrandesVariant.h:50-159)
+ *  - ngx_apsp_grad           no reference counterpart: gradient of CPL and efficiency w.r.t. every arc length
+ */
+#ifndef NGX_B200_H
+#define NGX_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NGX_API __attribute__((visibility("default")))
+#else
+#define NGX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    NGX_OK = 0,
+    NGX_INVALID_ARGUMENT = 1,
+    NGX_OUT_OF_MEMORY = 2,
+    NGX_CUDA_ERROR = 3,
+    NGX_TIMEOUT = 4,  /* a kernel hit its iteration cap (opts.max_iterations) and stopped */
+    NGX_ABORTED = 5,  /* ngx_graph_request_abort() was called while a run was in flight */
+    NGX_UNSUPPORTED = 6
+} ngx_status;
+
+typedef enum { NGX_METRIC_REGULAR = 0, NGX_METRIC_INVERSE = 1 } ngx_metric;
+
+/* How sources are mapped onto the GPU. */
+typedef enum {
+    NGX_MODE_BATCHED = 0, /* a tile of NGX_TILE sources per CTA; lanes of a warp are sources, arcs are shared */
+    NGX_MODE_PLAIN = 1    /* one source per CTA; lanes of a warp stride over one vertex's arcs */
+} ngx_mode;
+
+#define NGX_TILE 32
+
+/* Host CSR of out-arcs: arc e = (u -> col[e], w[e]) for row_ptr[u] <= e < row_ptr[u + 1]. */
+typedef struct {
+    int64_t n;
+    int64_t m;
+    const int64_t* row_ptr; /* n + 1 entries, row_ptr[0] == 0, non-decreasing, row_ptr[n] == m */
+    const int32_t* col;     /* m entries in [0, n) */
+    const double* w;        /* m entries, finite */
+} ngx_csr;
+
+typedef struct ngx_graph ngx_graph;
+
+typedef struct {
+    int metric;              /* ngx_metric */
+    int mode;                /* ngx_mode */
+    const int64_t* sources;  /* host list of source vertices, or NULL for all n in id order */
+    int64_t num_sources;     /* entries in sources (ignored when sources is NULL) */
+    double delta;            /* bucket width of the delta-stepping; <= 0 picks one from the arc lengths */
+    int block_threads;       /* threads per CTA; 0 picks the default */
+    int ctas_per_sm;         /* concurrent CTAs per SM; 0 picks the default (bounded by the memory budget) */
+    int64_t hist_bins;       /* bins of the shortest-path distance histogram; 0 = no histogram */
+    double hist_max;         /* exclusive upper bound of the histogram; <= 0 = sampled eccentricity x 1.5 */
+    uint64_t max_iterations; /* cap on delta-stepping phases per source tile; 0 = 4 * n + 64 */
+} ngx_apsp_opts;
+
+/* Totals over all requested sources; per-source arrays are optional caller-allocated host arrays (NULL to skip). */
+typedef struct {
+    double sum_distances;     /* exactly rounded sum of finite d(s,t), t != s */
+    double sum_inverse;       /* exactly rounded sum of 1/d(s,t), finite d != 0 */
+    double diameter;          /* maximum finite distance */
+    uint64_t unreachable;     /* pairs (s,t) with t unreachable from s */
+    uint64_t reached_pairs;   /* R = sum over sources of (reached vertices - 1) */
+    uint64_t traversed_arcs;  /* sum over sources of the out-degrees of the reached vertices (GTEPS numerator) */
+    uint64_t hist_overflow;   /* reached pairs with d >= hist_max */
+    double hist_max;          /* the histogram bound actually used */
+    double cpl;               /* characteristic path length sum_distances / R (AllPairsShortestPath.h:154-157) */
+    double efficiency;        /* global efficiency sum_inverse / R (AllPairsShortestPath.h:158) */
+    double kernel_ms;         /* device time of the run's kernels (CUDA events) */
+    /* optional outputs */
+    uint64_t* hist;           /* hist_bins entries */
+    double* src_sum;          /* per source: exactly rounded sum of distances */
+    double* src_max;          /* per source: maximum finite distance (eccentricity) */
+    double* src_sum_inverse;  /* per source: exactly rounded sum of 1/d */
+    uint64_t* src_unreachable;/* per source: unreachable vertices */
+    uint64_t* src_arcs;       /* per source: traversed arcs */
+} ngx_apsp_result;
+
+NGX_API const char* ngx_status_string(int status);
+NGX_API const char* ngx_last_error(void);
+/* Library build identifier (compute capability the kernels were built for, CUDA version). */
+NGX_API const char* ngx_version(void);
+
+/* Validates and uploads the graph to `device`, building the device CSR and reverse CSR. */
+NGX_API int ngx_graph_create(const ngx_csr* csr, int device, ngx_graph** out);
+NGX_API void ngx_graph_destroy(ngx_graph* graph);
+NGX_API int ngx_graph_size(const ngx_graph* graph, int64_t* n, int64_t* m);
+/* Asks an in-flight run on this graph to stop at its next phase boundary; the run returns NGX_ABORTED. */
+NGX_API int ngx_graph_request_abort(ngx_graph* graph);
+/* Caps the device memory the graph's runs may use for workspaces (bytes; 0 = no cap beyond free memory). */
+NGX_API int ngx_graph_set_memory_budget(ngx_graph* graph, uint64_t bytes);
+
+/* APSP summaries (and optional histogram / per-source outputs) over the requested sources. */
+NGX_API int ngx_apsp(ngx_graph* graph, const ngx_apsp_opts* opts, ngx_apsp_result* result);
+
+/* Full distance rows of the requested sources: rows has num_sources * n entries, +inf where unreachable. */
+NGX_API int ngx_sssp_rows(ngx_graph* graph, const ngx_apsp_opts* opts, double* rows);
+
+/*
+ * Brandes betweenness (regular metric) of the requested sources: bc (n entries) is overwritten with the sum over
+ * sources of the pair dependencies; result (optional) receives the APSP summaries of the same run.
+ */
+NGX_API int ngx_brandes(ngx_graph* graph, const ngx_apsp_opts* opts, double* bc, ngx_apsp_result* result);
+
+/*
+ * Gradient of CPL and of global efficiency (regular metric, over the requested sources) with respect to every arc
+ * length |w_e|: dcpl, deff have m entries each; arcs on no shortest path get 0. result (optional) receives the APSP
+ * summaries of the same run.
+ */
+NGX_API int ngx_apsp_grad(ngx_graph* graph, const ngx_apsp_opts* opts, double* dcpl, double* deff, ngx_apsp_result* result);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,242 @@
+"""neurograph-b200: B200-native all-sources shortest paths for neurograph connectomes.
+
+Python binding of the C ABI in ``include/ngx_b200.h`` (``neurograph_b200/lib/libngx_b200.so``). The library is
+the product; this module only marshals host arrays through ctypes. There is no CPU fallback: importing works
+without a GPU, but every call needs the CUDA library and a B200, and fails loudly otherwise.
+
+Mapping to the reference (paths relative to the reference project):
+
+* ``Graph(...)``                 DistributedGraph::construct_graph (source/graph/DistributedGraph.cpp:46-127)
+* ``Graph.apsp()``               AllPairsShortestPath::compute_apsp / compute_apsp_inverse /
+                                 compute_apsp_delta_stepping (source/metrics/paths/AllPairsShortestPath.h:54-98)
+* ``Graph.sssp_rows()``          Dijkstra::compute_sssp's distance rows (source/metrics/paths/Dijkstra.h:55-98)
+* ``Graph.brandes()``            BetweennessCentrality::compute_average_betweenness_centrality with the Brandes
+                                 variant (source/metrics/paths/BetweennessCentrality.h:46-80)
+* ``Graph.apsp_grad()``          new: gradient of CPL and global efficiency w.r.t. every arc length
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libngx_b200.so")
+
+NGX_OK = 0
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARGUMENT", 2: "OUT_OF_MEMORY", 3: "CUDA_ERROR", 4: "TIMEOUT", 5: "ABORTED", 6: "UNSUPPORTED"}
+METRICS = {"regular": 0, "inverse": 1}
+MODES = {"batched": 0, "plain": 1}
+TILE = 32
+
+
+class NgxError(RuntimeError):
+    """A non-OK status from the CUDA library."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class _Csr(C.Structure):
+    _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("row_ptr", C.c_void_p), ("col", C.c_void_p), ("w", C.c_void_p)]
+
+
+class _Opts(C.Structure):
+    _fields_ = [
+        ("metric", C.c_int), ("mode", C.c_int), ("sources", C.c_void_p), ("num_sources", C.c_int64),
+        ("delta", C.c_double), ("block_threads", C.c_int), ("ctas_per_sm", C.c_int), ("hist_bins", C.c_int64),
+        ("hist_max", C.c_double), ("max_iterations", C.c_uint64),
+    ]
+
+
+class _Result(C.Structure):
+    _fields_ = [
+        ("sum_distances", C.c_double), ("sum_inverse", C.c_double), ("diameter", C.c_double),
+        ("unreachable", C.c_uint64), ("reached_pairs", C.c_uint64), ("traversed_arcs", C.c_uint64),
+        ("hist_overflow", C.c_uint64), ("hist_max", C.c_double), ("cpl", C.c_double), ("efficiency", C.c_double),
+        ("kernel_ms", C.c_double),
+        ("hist", C.c_void_p), ("src_sum", C.c_void_p), ("src_max", C.c_void_p), ("src_sum_inverse", C.c_void_p),
+        ("src_unreachable", C.c_void_p), ("src_arcs", C.c_void_p),
+    ]
+
+
+_LIB = None
+
+# Every symbol include/ngx_b200.h declares (checked by the CPU test suite against the built library).
+EXPORTED = [
+    "ngx_status_string", "ngx_last_error", "ngx_version", "ngx_graph_create", "ngx_graph_destroy", "ngx_graph_size",
+    "ngx_graph_request_abort", "ngx_graph_set_memory_budget", "ngx_apsp", "ngx_sssp_rows", "ngx_brandes",
+    "ngx_apsp_grad",
+]
+
+
+def library() -> C.CDLL:
+    """Loads libngx_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m neurograph_b200.build`")
+        lib = C.CDLL(LIB_PATH)
+        lib.ngx_status_string.restype = C.c_char_p
+        lib.ngx_last_error.restype = C.c_char_p
+        lib.ngx_version.restype = C.c_char_p
+        lib.ngx_graph_create.argtypes = [C.POINTER(_Csr), C.c_int, C.POINTER(C.c_void_p)]
+        lib.ngx_graph_destroy.argtypes = [C.c_void_p]
+        lib.ngx_graph_destroy.restype = None
+        lib.ngx_graph_size.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        lib.ngx_graph_request_abort.argtypes = [C.c_void_p]
+        lib.ngx_graph_set_memory_budget.argtypes = [C.c_void_p, C.c_uint64]
+        lib.ngx_apsp.argtypes = [C.c_void_p, C.POINTER(_Opts), C.POINTER(_Result)]
+        lib.ngx_sssp_rows.argtypes = [C.c_void_p, C.POINTER(_Opts), C.c_void_p]
+        if hasattr(lib, "ngx_brandes"):
+            lib.ngx_brandes.argtypes = [C.c_void_p, C.POINTER(_Opts), C.c_void_p, C.POINTER(_Result)]
+        if hasattr(lib, "ngx_apsp_grad"):
+            lib.ngx_apsp_grad.argtypes = [C.c_void_p, C.POINTER(_Opts), C.c_void_p, C.c_void_p, C.POINTER(_Result)]
+        _LIB = lib
+    return _LIB
+
+
+def _check(status: int) -> None:
+    if status != NGX_OK:
+        raise NgxError(status, library().ngx_last_error().decode())
+
+
+@dataclass
+class ApspResult:
+    """Mirror of ApspGlobalResult (source/Types.h:237-244) plus the new outputs."""
+
+    cpl: float
+    efficiency: float
+    diameter: float
+    unreachable: int
+    reached_pairs: int
+    traversed_arcs: int
+    sum_distances: float
+    sum_inverse: float
+    hist_max: float
+    hist_overflow: int
+    kernel_ms: float
+    hist: np.ndarray | None = None
+    per_source: dict | None = None
+    cluster_sizes: dict = field(default_factory=dict)
+
+    @property
+    def gteps(self) -> float:
+        return self.traversed_arcs / (self.kernel_ms * 1e-3) / 1e9 if self.kernel_ms > 0 else 0.0
+
+
+class Graph:
+    """A graph resident on one GPU (device CSR + reverse CSR)."""
+
+    def __init__(self, n: int, row_ptr, col, w, device: int = 0):
+        lib = library()
+        self.n = int(n)
+        self.row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+        self.col = np.ascontiguousarray(col, dtype=np.int32)
+        self.w = np.ascontiguousarray(w, dtype=np.float64)
+        self.m = int(self.col.size)
+        csr = _Csr(self.n, self.m, self.row_ptr.ctypes.data, self.col.ctypes.data if self.m else None,
+                   self.w.ctypes.data if self.m else None)
+        handle = C.c_void_p()
+        _check(lib.ngx_graph_create(C.byref(csr), int(device), C.byref(handle)))
+        self._handle = handle
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            library().ngx_graph_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def request_abort(self) -> None:
+        _check(library().ngx_graph_request_abort(self._handle))
+
+    def set_memory_budget(self, nbytes: int) -> None:
+        _check(library().ngx_graph_set_memory_budget(self._handle, int(nbytes)))
+
+    def _opts(self, sources, metric, mode, delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations):
+        srcs = None if sources is None else np.ascontiguousarray(sources, dtype=np.int64)
+        opts = _Opts(
+            METRICS[metric] if isinstance(metric, str) else int(metric),
+            MODES[mode] if isinstance(mode, str) else int(mode),
+            None if srcs is None else srcs.ctypes.data,
+            0 if srcs is None else srcs.size,
+            float(delta), int(block_threads), int(ctas_per_sm), int(hist_bins), float(hist_max), int(max_iterations),
+        )
+        k = self.n if srcs is None else srcs.size
+        return opts, srcs, k
+
+    def _result(self, r: _Result, hist, per, k) -> ApspResult:
+        out = ApspResult(
+            cpl=r.cpl, efficiency=r.efficiency, diameter=r.diameter, unreachable=r.unreachable,
+            reached_pairs=r.reached_pairs, traversed_arcs=r.traversed_arcs, sum_distances=r.sum_distances,
+            sum_inverse=r.sum_inverse, hist_max=r.hist_max, hist_overflow=r.hist_overflow, kernel_ms=r.kernel_ms,
+            hist=hist, per_source=per,
+        )
+        if per is not None:
+            sizes: dict[int, int] = {}
+            for u in per["unreachable"].astype(np.int64):
+                sizes[int(self.n - u)] = sizes.get(int(self.n - u), 0) + 1
+            out.cluster_sizes = sizes
+        return out
+
+    @staticmethod
+    def _result_struct(hist_bins, per_source, k):
+        r = _Result()
+        hist = np.zeros(hist_bins, np.uint64) if hist_bins > 0 else None
+        per = None
+        if per_source:
+            per = {"sum": np.zeros(k), "max": np.zeros(k), "sum_inv": np.zeros(k),
+                   "unreachable": np.zeros(k, np.uint64), "arcs": np.zeros(k, np.uint64)}
+            r.src_sum, r.src_max, r.src_sum_inverse = per["sum"].ctypes.data, per["max"].ctypes.data, per["sum_inv"].ctypes.data
+            r.src_unreachable, r.src_arcs = per["unreachable"].ctypes.data, per["arcs"].ctypes.data
+        if hist is not None:
+            r.hist = hist.ctypes.data
+        return r, hist, per
+
+    def apsp(self, sources=None, metric="regular", mode="batched", delta=0.0, hist_bins=0, hist_max=0.0,
+             per_source=False, block_threads=0, ctas_per_sm=0, max_iterations=0) -> ApspResult:
+        opts, srcs, k = self._opts(sources, metric, mode, delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations)
+        r, hist, per = self._result_struct(hist_bins, per_source, k)
+        _check(library().ngx_apsp(self._handle, C.byref(opts), C.byref(r)))
+        return self._result(r, hist, per, k)
+
+    def sssp_rows(self, sources, metric="regular", mode="batched", delta=0.0) -> np.ndarray:
+        opts, srcs, k = self._opts(sources, metric, mode, delta, 0, 0.0, 0, 0, 0)
+        rows = np.zeros((k, self.n), np.float64)
+        _check(library().ngx_sssp_rows(self._handle, C.byref(opts), rows.ctypes.data))
+        return rows
+
+    def brandes(self, sources=None, delta=0.0, hist_bins=0, hist_max=0.0, per_source=False, block_threads=0,
+                ctas_per_sm=0, max_iterations=0):
+        opts, srcs, k = self._opts(sources, "regular", "batched", delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations)
+        r, hist, per = self._result_struct(hist_bins, per_source, k)
+        bc = np.zeros(max(self.n, 1), np.float64)
+        _check(library().ngx_brandes(self._handle, C.byref(opts), bc.ctypes.data, C.byref(r)))
+        return bc[: self.n], self._result(r, hist, per, k)
+
+    def apsp_grad(self, sources=None, delta=0.0, block_threads=0, ctas_per_sm=0, max_iterations=0):
+        opts, srcs, k = self._opts(sources, "regular", "batched", delta, 0, 0.0, block_threads, ctas_per_sm, max_iterations)
+        r, hist, per = self._result_struct(0, False, k)
+        dcpl = np.zeros(max(self.m, 1), np.float64)
+        deff = np.zeros(max(self.m, 1), np.float64)
+        _check(library().ngx_apsp_grad(self._handle, C.byref(opts), dcpl.ctypes.data, deff.ctypes.data, C.byref(r)))
+        return dcpl[: self.m], deff[: self.m], self._result(r, hist, per, k)
+
+
+def version() -> str:
+    return library().ngx_version().decode()

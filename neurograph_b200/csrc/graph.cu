@@ -1,0 +1,307 @@
+// Graph handle: validation, CSR + reverse CSR upload, status strings and error reporting.
+//
+// Replaces the reference's DistributedGraph adjacency (source/graph/DistributedGraph.{h,cpp}): per-rank RMA windows of
+// 12-byte {rank, id, weight} arcs read through get_out_arcs (DistributedGraph.h:275-311) become one device-resident
+// CSR of 16-byte {target, arc id, FP64 length} records, plus a reverse CSR for the pull passes of Brandes and the
+// gradient. Zero-weight arcs are left out, as DistributedGraph::upload_out_arcs skips them (DistributedGraph.cpp:223).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "ngx_common.cuh"
+#include "ngx_graph.h"
+
+namespace ngx {
+
+namespace {
+thread_local std::string last_error_message;
+}
+
+void set_last_error(const std::string& message) { last_error_message = message; }
+
+int fail(int status, const std::string& message) {
+    set_last_error(message);
+    return status;
+}
+
+int cuda_fail(cudaError_t err, const char* what) {
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(err));
+    return err == cudaErrorMemoryAllocation ? NGX_OUT_OF_MEMORY : NGX_CUDA_ERROR;
+}
+
+size_t workspace_budget(const ngx_graph* g) {
+    size_t free_bytes = 0, total_bytes = 0;
+    if (cudaMemGetInfo(&free_bytes, &total_bytes) != cudaSuccess) {
+        return 0;
+    }
+    size_t usable = free_bytes + g->workspace_bytes;
+    usable = usable > (size_t(1) << 30) ? usable - (size_t(1) << 30) : usable / 2;  // keep 1 GiB headroom
+    if (g->memory_budget != 0 && g->memory_budget < usable) {
+        usable = static_cast<size_t>(g->memory_budget);
+    }
+    return usable;
+}
+
+int ensure_workspace(ngx_graph* g, size_t bytes) {
+    if (bytes <= g->workspace_bytes) {
+        return NGX_OK;
+    }
+    if (g->d_workspace != nullptr) {
+        NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        NGX_CUDA_TRY(cudaFree(g->d_workspace));
+        g->d_workspace = nullptr;
+        g->workspace_bytes = 0;
+    }
+    NGX_CUDA_TRY(cudaMalloc(&g->d_workspace, bytes));
+    g->workspace_bytes = bytes;
+    return NGX_OK;
+}
+
+namespace {
+
+void release(ngx_graph* g) {
+    if (g == nullptr) {
+        return;
+    }
+    cudaSetDevice(g->device);
+    if (g->stream != nullptr) {
+        cudaStreamSynchronize(g->stream);
+    }
+    cudaFree(g->d_row_ptr);
+    cudaFree(g->d_arcs_regular);
+    cudaFree(g->d_arcs_inverse);
+    cudaFree(g->d_rrow_ptr);
+    cudaFree(g->d_rarcs);
+    cudaFree(g->d_workspace);
+    if (g->h_abort != nullptr) {
+        cudaFreeHost(g->h_abort);
+    }
+    if (g->stream != nullptr) {
+        cudaStreamDestroy(g->stream);
+    }
+    delete g;
+}
+
+int validate(const ngx_csr* csr) {
+    if (csr == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: csr is NULL");
+    }
+    if (csr->n < 0 || csr->m < 0) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: negative n or m");
+    }
+    if (csr->n >= (int64_t(1) << 31) - 1 || csr->m >= (int64_t(1) << 31) - 1) {
+        return fail(NGX_UNSUPPORTED, "ngx_graph_create: n and m must be below 2^31 - 1 (int32 vertex and arc ids)");
+    }
+    if (csr->n > 0 && csr->row_ptr == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: row_ptr is NULL");
+    }
+    if (csr->m > 0 && (csr->col == nullptr || csr->w == nullptr)) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: col or w is NULL");
+    }
+    if (csr->n == 0) {
+        return csr->m == 0 ? NGX_OK : fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: arcs without vertices");
+    }
+    if (csr->row_ptr[0] != 0 || csr->row_ptr[csr->n] != csr->m) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: row_ptr must start at 0 and end at m");
+    }
+    for (int64_t u = 0; u < csr->n; ++u) {
+        if (csr->row_ptr[u + 1] < csr->row_ptr[u]) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: row_ptr is not monotone at vertex " + std::to_string(u));
+        }
+    }
+    for (int64_t e = 0; e < csr->m; ++e) {
+        if (csr->col[e] < 0 || csr->col[e] >= csr->n) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: arc " + std::to_string(e) + " has an out-of-range target");
+        }
+        if (!std::isfinite(csr->w[e])) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: arc " + std::to_string(e) + " has a non-finite weight");
+        }
+    }
+    return NGX_OK;
+}
+
+}  // namespace
+}  // namespace ngx
+
+using namespace ngx;
+
+extern "C" {
+
+const char* ngx_status_string(int status) {
+    switch (status) {
+    case NGX_OK: return "ok";
+    case NGX_INVALID_ARGUMENT: return "invalid argument";
+    case NGX_OUT_OF_MEMORY: return "out of memory";
+    case NGX_CUDA_ERROR: return "CUDA error";
+    case NGX_TIMEOUT: return "iteration cap reached";
+    case NGX_ABORTED: return "aborted";
+    case NGX_UNSUPPORTED: return "unsupported";
+    default: return "unknown status";
+    }
+}
+
+const char* ngx_last_error(void) { return last_error_message.c_str(); }
+
+const char* ngx_version(void) {
+    static const std::string version = [] {
+        int runtime = 0;
+        cudaRuntimeGetVersion(&runtime);
+        return std::string("neurograph-b200 sm_100a, CUDA runtime ") + std::to_string(runtime / 1000) + "." + std::to_string((runtime % 1000) / 10);
+    }();
+    return version.c_str();
+}
+
+int ngx_graph_create(const ngx_csr* csr, int device, ngx_graph** out) {
+    if (out == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: out is NULL");
+    }
+    *out = nullptr;
+    if (const int rc = validate(csr); rc != NGX_OK) {
+        return rc;
+    }
+    int device_count = 0;
+    NGX_CUDA_TRY(cudaGetDeviceCount(&device_count));
+    if (device < 0 || device >= device_count) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: no CUDA device " + std::to_string(device));
+    }
+    NGX_CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop{};
+    NGX_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        return fail(NGX_UNSUPPORTED, std::string("ngx_graph_create: the kernels are built for sm_100a (B200); device is ") + prop.name);
+    }
+
+    auto* g = new (std::nothrow) ngx_graph{};
+    if (g == nullptr) {
+        return fail(NGX_OUT_OF_MEMORY, "ngx_graph_create: host allocation failed");
+    }
+    g->device = device;
+    g->sm_count = prop.multiProcessorCount;
+    g->n = csr->n;
+    g->m_user = csr->m;
+
+    const auto finish = [&](int rc) -> int {
+        if (rc != NGX_OK) {
+            release(g);
+            return rc;
+        }
+        *out = g;
+        return NGX_OK;
+    };
+
+    if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaHostAlloc(reinterpret_cast<void**>(&g->h_abort), sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&g->d_abort), g->h_abort, 0) != cudaSuccess) {
+        return finish(fail(NGX_CUDA_ERROR, "ngx_graph_create: stream or abort flag setup failed"));
+    }
+    *g->h_abort = 0;
+
+    const int64_t n = csr->n;
+    // Host compaction: drop zero-weight arcs, keep the caller's arc index, precompute both metrics' lengths.
+    std::vector<int64_t> row_ptr(static_cast<size_t>(n) + 1, 0);
+    std::vector<Arc> regular;
+    std::vector<Arc> inverse;
+    regular.reserve(static_cast<size_t>(csr->m));
+    inverse.reserve(static_cast<size_t>(csr->m));
+    std::vector<int64_t> in_degree(static_cast<size_t>(n) + 1, 0);
+    double sum_regular = 0.0, sum_inverse = 0.0;
+    double min_regular = INFINITY, max_regular = 0.0;
+    for (int64_t u = 0; u < n; ++u) {
+        for (int64_t e = csr->row_ptr[u]; e < csr->row_ptr[u + 1]; ++e) {
+            const double a = std::fabs(csr->w[e]);
+            if (a == 0.0) {
+                continue;
+            }
+            const int32_t v = csr->col[e];
+            regular.push_back(Arc{ v, static_cast<int32_t>(e), a });
+            inverse.push_back(Arc{ v, static_cast<int32_t>(e), 1.0 / a });
+            sum_regular += a;
+            sum_inverse += 1.0 / a;
+            min_regular = std::min(min_regular, a);
+            max_regular = std::max(max_regular, a);
+            in_degree[static_cast<size_t>(v) + 1] += 1;
+        }
+        row_ptr[static_cast<size_t>(u) + 1] = static_cast<int64_t>(regular.size());
+        g->max_out_degree = std::max(g->max_out_degree, row_ptr[static_cast<size_t>(u) + 1] - row_ptr[static_cast<size_t>(u)]);
+    }
+    const int64_t m = static_cast<int64_t>(regular.size());
+    g->m_stored = m;
+    if (m > 0) {
+        g->mean_len_regular = sum_regular / static_cast<double>(m);
+        g->mean_len_inverse = sum_inverse / static_cast<double>(m);
+        g->min_len_regular = min_regular;
+        g->max_len_regular = max_regular;
+    }
+
+    // Reverse CSR by counting sort over targets; within a target, in-arcs keep ascending source order.
+    std::vector<int64_t> rrow_ptr(static_cast<size_t>(n) + 1, 0);
+    for (int64_t v = 0; v < n; ++v) {
+        rrow_ptr[static_cast<size_t>(v) + 1] = rrow_ptr[static_cast<size_t>(v)] + in_degree[static_cast<size_t>(v) + 1];
+    }
+    std::vector<Arc> rarcs(static_cast<size_t>(m));
+    std::vector<int64_t> fill(rrow_ptr.begin(), rrow_ptr.end() - 1);
+    for (int64_t u = 0; u < n; ++u) {
+        for (int64_t e = row_ptr[static_cast<size_t>(u)]; e < row_ptr[static_cast<size_t>(u) + 1]; ++e) {
+            const Arc& a = regular[static_cast<size_t>(e)];
+            rarcs[static_cast<size_t>(fill[static_cast<size_t>(a.col)]++)] = Arc{ static_cast<int32_t>(u), a.id, a.len };
+        }
+    }
+
+    const auto upload = [&](auto** dst, const auto& src) -> int {
+        using T = std::remove_reference_t<decltype(src[0])>;
+        const size_t bytes = std::max<size_t>(1, src.size()) * sizeof(T);
+        NGX_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(dst), bytes));
+        if (!src.empty()) {
+            NGX_CUDA_TRY(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, g->stream));
+        }
+        return NGX_OK;
+    };
+    int rc = upload(&g->d_row_ptr, row_ptr);
+    if (rc == NGX_OK) rc = upload(&g->d_arcs_regular, regular);
+    if (rc == NGX_OK) rc = upload(&g->d_arcs_inverse, inverse);
+    if (rc == NGX_OK) rc = upload(&g->d_rrow_ptr, rrow_ptr);
+    if (rc == NGX_OK) rc = upload(&g->d_rarcs, rarcs);
+    if (rc == NGX_OK) {
+        const cudaError_t err = cudaStreamSynchronize(g->stream);
+        if (err != cudaSuccess) {
+            rc = cuda_fail(err, "ngx_graph_create: upload");
+        }
+    }
+    return finish(rc);
+}
+
+void ngx_graph_destroy(ngx_graph* graph) { release(graph); }
+
+int ngx_graph_size(const ngx_graph* graph, int64_t* n, int64_t* m) {
+    if (graph == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_size: graph is NULL");
+    }
+    if (n != nullptr) *n = graph->n;
+    if (m != nullptr) *m = graph->m_user;
+    return NGX_OK;
+}
+
+int ngx_graph_request_abort(ngx_graph* graph) {
+    if (graph == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_request_abort: graph is NULL");
+    }
+    *reinterpret_cast<volatile int*>(graph->h_abort) = 1;
+    return NGX_OK;
+}
+
+int ngx_graph_set_memory_budget(ngx_graph* graph, uint64_t bytes) {
+    if (graph == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_set_memory_budget: graph is NULL");
+    }
+    graph->memory_budget = bytes;
+    return NGX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,750 @@
+// Batched and plain multi-source delta-stepping kernels with the fused APSP epilogue (sm_100a).
+//
+// Both kernels are persistent: one CTA per workspace slot, each CTA takes source tiles from a device work counter until
+// none are left. A tile is either NGX_TILE sources (batched form: lane s of every warp owns source s of the tile) or
+// one source (plain form: the lanes of a warp stride over one vertex's arcs).
+//
+// Per tile the CTA runs delta-stepping with a common bucket bound theta for all its sources:
+//   near phase   vertices whose pending (vertex, source) pairs lie below theta are expanded; an improvement below
+//                theta is queued for the next iteration, one at or above theta is marked "far";
+//   bucket step  when no near work is left, one pass over the far marks finds the smallest pending distance d_min,
+//                theta becomes (floor(d_min / delta) + 1) * delta, and the pairs below it move to the near queue.
+// Relaxation is fl(d[u] + len) compared and stored with a 64-bit atomicMin on the bit pattern, which orders
+// non-negative doubles like their values. The label-correcting fixed point is the same as the reference Dijkstra's
+// (PriorityQueueVariant.h:47-93: d[v] = min over arcs of fl(d[u] + |w|)), so distances are bit-identical.
+//
+// Race-freedom of the pending marks: expansions of iteration k read and clear pend[k % 2]; improvements made during
+// iteration k set pend[(k + 1) % 2] and the far marks; iterations are separated by __syncthreads(). A pair improved
+// while its vertex is being expanded is therefore always expanded again in the next iteration, with the new distance.
+// All distance reads go through L2 (__ldcg), where the atomics are performed.
+//
+// Epilogue (after a tile's distances are final), per (vertex, source), replacing summarize_distances
+// (types/SsspResult.h:42-64) and the aggregation of AllPairsShortestPath::compute_apsp_impl (:110-163): unreachable
+// count, exact sums of d and of 1/d (order-independent integer accumulators, rounded once), maximum finite distance,
+// traversed arcs, and the distance histogram (bin floor(d / (hist_max / bins)), clamped to the last bin, as
+// FixedSizeHistogram::add_data_point, external/cpp-utility/data-structure/Histogram.hpp:166-180). The distances are
+// reset to +inf in the same pass, so the N x N distances never leave the per-CTA workspace.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "ngx_common.cuh"
+
+namespace ngx {
+
+constexpr unsigned kFullMask = 0xFFFFFFFFu;
+
+struct TileOutputs {
+    unsigned long long* acc_sum;    // kAccDigits: exact sum of distances over all sources
+    unsigned long long* acc_inv;    // kAccDigits: exact sum of 1/d
+    unsigned long long* counters;   // see Counter
+    unsigned long long* hist;       // hist_bins (or nullptr)
+    int hist_bins;
+    double hist_width;
+    double hist_max;
+    double* src_sum;                // per tile position (or nullptr)
+    double* src_max;
+    double* src_inv;
+    unsigned long long* src_unreach;
+    unsigned long long* src_arcs;
+    double* rows;                   // num_sources x n distance rows (or nullptr)
+};
+
+enum Counter : int { kUnreachable = 0, kReachedPairs = 1, kTraversedArcs = 2, kHistOverflow = 3, kDiameterBits = 4, kIterations = 5, kCounterCount = 8 };
+
+struct SsspParams {
+    DeviceCsr g;
+    const int32_t* sources;        // tile order
+    int64_t num_sources;
+    int64_t num_tiles;
+    double delta;
+    unsigned long long max_iterations;  // per tile
+    unsigned long long* tile_counter;
+    int* error;
+    const volatile int* abort_flag;
+    // workspace, carved per slot (blockIdx.x)
+    unsigned long long* ws_dist;   // slots * n * width (width = kTile batched, 1 plain)
+    uint32_t* ws_pend;             // slots * 2n
+    uint32_t* ws_far;              // slots * n
+    int32_t* ws_queue;             // slots * 2n
+    uint32_t* ws_stamp;            // slots * n
+    TileOutputs out;
+};
+
+// Bytes of per-slot workspace for a graph with n vertices.
+inline size_t sssp_slot_bytes(int64_t n, int width) {
+    return static_cast<size_t>(n) * (static_cast<size_t>(width) * 8 + 4 * 2 + 4 + 4 * 2 + 4) + 256;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned mask;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(mask));
+    return mask;
+}
+
+__device__ __forceinline__ double next_theta(double d_min, double delta) {
+    const double theta = (floor(__ddiv_rn(d_min, delta)) + 1.0) * delta;
+    return theta > d_min ? theta : INFINITY;
+}
+
+// Shared state of a CTA working on one tile.
+struct TileShared {
+    long long tile;
+    int qlen[2];
+    int cur;
+    int stop;
+    unsigned stamp;                 // id of the iteration about to run (queue dedup)
+    double theta;
+    unsigned long long min_bits;
+    unsigned long long iterations;
+    unsigned long long overflow;
+};
+
+// ------------------------------------------------------------------------------------------ batched form
+template <int kUnroll>
+__device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, int lane, unsigned long long* __restrict__ dist, uint32_t* pend_cur,
+                                               uint32_t* pend_nxt, uint32_t* far, int32_t* q_nxt, int* qlen_nxt, uint32_t* stamp, unsigned next_stamp,
+                                               double theta) {
+    const uint32_t amask = __ldcg(&pend_cur[v]);
+    if (amask == 0) {
+        return;
+    }
+    __syncwarp();
+    const bool act = (amask >> lane) & 1u;
+    const double dv = act ? __longlong_as_double(static_cast<long long>(__ldcg(&dist[static_cast<int64_t>(v) * kTile + lane]))) : 0.0;
+    if (lane == 0) {
+        pend_cur[v] = 0u;
+        if (__ldcg(&far[v]) & amask) {
+            atomicAnd(&far[v], ~amask);  // those far marks are superseded by the near values expanded now
+        }
+    }
+    const int64_t beg = __ldg(&g.row_ptr[v]);
+    const int64_t end = __ldg(&g.row_ptr[v + 1]);
+    for (int64_t e0 = beg; e0 < end; e0 += 32) {
+        const int cnt = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
+        Arc a{ 0, 0, 0.0 };
+        if (lane < cnt) {
+            a = g.arcs[e0 + lane];
+        }
+        for (int j = 0; j < cnt; j += kUnroll) {
+            int x[kUnroll];
+            double nd[kUnroll];
+            unsigned long long cur[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) {
+                const int jj = j + u;
+                const int from = jj < cnt ? jj : 0;
+                x[u] = __shfl_sync(kFullMask, a.col, from);
+                const double len = __shfl_sync(kFullMask, a.len, from);
+                nd[u] = __dadd_rn(dv, len);
+                cur[u] = (act && jj < cnt) ? __ldcg(&dist[static_cast<int64_t>(x[u]) * kTile + lane]) : 0ull;
+            }
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u) {
+                const int jj = j + u;
+                bool improved = false;
+                if (act && jj < cnt) {
+                    const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd[u]));
+                    if (nb < cur[u]) {
+                        const unsigned long long old = atomicMin(&dist[static_cast<int64_t>(x[u]) * kTile + lane], nb);
+                        improved = nb < old;
+                    }
+                }
+                const unsigned imask = __ballot_sync(kFullMask, improved);
+                if (imask != 0u) {
+                    const unsigned nmask = __ballot_sync(kFullMask, improved && nd[u] < theta);
+                    if (lane == 0) {
+                        const int xv = x[u];
+                        if (nmask != 0u) {
+                            atomicOr(&pend_nxt[xv], nmask);
+                            if (atomicExch(&stamp[xv], next_stamp) != next_stamp) {
+                                q_nxt[atomicAdd(qlen_nxt, 1)] = xv;
+                            }
+                        }
+                        const unsigned fmask = imask & ~nmask;
+                        if (fmask != 0u) {
+                            atomicOr(&far[xv], fmask);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int kUnroll>
+__global__ void __launch_bounds__(512, 2) sssp_batched_kernel(const SsspParams p) {
+    extern __shared__ __align__(16) unsigned long long smem[];
+    unsigned long long* s_acc_sum = smem;                                // kTile * kAccDigits
+    unsigned long long* s_acc_inv = smem + kTile * kAccDigits;          // kTile * kAccDigits
+    unsigned int* s_hist = reinterpret_cast<unsigned int*>(smem + 2 * kTile * kAccDigits);
+    __shared__ TileShared s;
+    __shared__ int s_src[kTile];
+    __shared__ unsigned long long s_unreach[kTile];
+    __shared__ unsigned long long s_arcs[kTile];
+    __shared__ unsigned long long s_max[kTile];
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int64_t n = p.g.n;
+    const int64_t slot = blockIdx.x;
+
+    unsigned long long* dist = p.ws_dist + slot * n * kTile;
+    uint32_t* pend0 = p.ws_pend + slot * 2 * n;
+    uint32_t* pend1 = pend0 + n;
+    uint32_t* far = p.ws_far + slot * n;
+    int32_t* q0 = p.ws_queue + slot * 2 * n;
+    int32_t* q1 = q0 + n;
+    uint32_t* stamp = p.ws_stamp + slot * n;
+
+    for (int64_t i = tid; i < n * kTile; i += blockDim.x) {
+        dist[i] = kInfBits;
+    }
+    for (int64_t i = tid; i < n; i += blockDim.x) {
+        pend0[i] = 0u;
+        pend1[i] = 0u;
+        far[i] = 0u;
+        stamp[i] = 0u;
+    }
+    for (int i = tid; i < 2 * kTile * kAccDigits; i += blockDim.x) {
+        smem[i] = 0ull;
+    }
+    for (int i = tid; i < p.out.hist_bins; i += blockDim.x) {
+        s_hist[i] = 0u;
+    }
+    if (tid == 0) {
+        s.stamp = 1u;
+    }
+    __syncthreads();
+
+    for (;;) {
+        if (tid == 0) {
+            s.tile = static_cast<long long>(atomicAdd(p.tile_counter, 1ull));
+            s.stop = (*reinterpret_cast<volatile int*>(p.error) != 0) ? 1 : 0;
+            s.qlen[0] = 0;
+            s.qlen[1] = 0;
+            s.cur = 0;
+            s.theta = p.delta;
+            s.iterations = 0;
+            s.overflow = 0;
+        }
+        __syncthreads();
+        if (s.stop != 0 || s.tile >= p.num_tiles) {
+            break;
+        }
+        const int64_t base = s.tile * kTile;
+        const int nsrc = static_cast<int>(p.num_sources - base < kTile ? p.num_sources - base : kTile);
+        if (tid < kTile) {
+            s_src[tid] = tid < nsrc ? p.sources[base + tid] : -1;
+            s_unreach[tid] = 0ull;
+            s_arcs[tid] = 0ull;
+            s_max[tid] = 0ull;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const int v = s_src[lane];
+            if (v >= 0) {
+                dist[static_cast<int64_t>(v) * kTile + lane] = 0ull;
+                atomicOr(&pend0[v], 1u << lane);
+                if (atomicExch(&stamp[v], s.stamp) != s.stamp) {
+                    q0[atomicAdd(&s.qlen[0], 1)] = v;
+                }
+            }
+        }
+        __syncthreads();
+
+        // ------------------------------------------------------------ delta-stepping over the tile
+        for (;;) {
+            for (;;) {
+                const int cur = s.cur;
+                const int qlen = s.qlen[cur];
+                if (qlen == 0) {
+                    break;
+                }
+                uint32_t* pend_cur = cur ? pend1 : pend0;
+                uint32_t* pend_nxt = cur ? pend0 : pend1;
+                const int32_t* q_cur = cur ? q1 : q0;
+                int32_t* q_nxt = cur ? q0 : q1;
+                const unsigned next_stamp = s.stamp + 1u;
+                const double theta = s.theta;
+                for (int i = warp; i < qlen; i += nwarps) {
+                    batched_expand<kUnroll>(p.g, __ldcg(&q_cur[i]), lane, dist, pend_cur, pend_nxt, far, q_nxt, &s.qlen[cur ^ 1], stamp, next_stamp, theta);
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    s.qlen[cur] = 0;
+                    s.cur = cur ^ 1;
+                    s.stamp = next_stamp;
+                    s.iterations += 1;
+                    if (s.iterations > p.max_iterations) {
+                        atomicCAS(p.error, kDevOk, kDevTimeout);
+                        s.stop = 1;
+                    } else if (*p.abort_flag != 0) {
+                        atomicCAS(p.error, kDevOk, kDevAborted);
+                        s.stop = 1;
+                    }
+                }
+                __syncthreads();
+                if (s.stop != 0) {
+                    break;
+                }
+            }
+            if (s.stop != 0) {
+                break;
+            }
+            // bucket step, pass 1: smallest pending far distance
+            if (tid == 0) {
+                s.min_bits = kInfBits;
+            }
+            __syncthreads();
+            unsigned long long local_min = kInfBits;
+            for (int64_t vb = static_cast<int64_t>(warp) * 32; vb < n; vb += static_cast<int64_t>(nwarps) * 32) {
+                const int64_t v = vb + lane;
+                const uint32_t fm = v < n ? __ldcg(&far[v]) : 0u;
+                unsigned any = __ballot_sync(kFullMask, fm != 0u);
+                while (any != 0u) {
+                    const int l = __ffs(any) - 1;
+                    any &= any - 1u;
+                    const uint32_t f = __shfl_sync(kFullMask, fm, l);
+                    if ((f >> lane) & 1u) {
+                        const unsigned long long d = __ldcg(&dist[(vb + l) * kTile + lane]);
+                        local_min = d < local_min ? d : local_min;
+                    }
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const unsigned long long o = __shfl_xor_sync(kFullMask, local_min, off);
+                local_min = o < local_min ? o : local_min;
+            }
+            if (lane == 0 && local_min != kInfBits) {
+                atomicMin(&s.min_bits, local_min);
+            }
+            __syncthreads();
+            if (s.min_bits == kInfBits) {
+                break;  // nothing pending: the tile's distances are final
+            }
+            const double theta = next_theta(__longlong_as_double(static_cast<long long>(s.min_bits)), p.delta);
+            // pass 2: move the pairs below the new bound into the near queue of the next iteration
+            const int cur = s.cur;
+            uint32_t* pend_cur = cur ? pend1 : pend0;
+            int32_t* q_cur = cur ? q1 : q0;
+            for (int64_t vb = static_cast<int64_t>(warp) * 32; vb < n; vb += static_cast<int64_t>(nwarps) * 32) {
+                const int64_t v = vb + lane;
+                const uint32_t fm = v < n ? __ldcg(&far[v]) : 0u;
+                unsigned any = __ballot_sync(kFullMask, fm != 0u);
+                while (any != 0u) {
+                    const int l = __ffs(any) - 1;
+                    any &= any - 1u;
+                    const uint32_t f = __shfl_sync(kFullMask, fm, l);
+                    bool near = false;
+                    if ((f >> lane) & 1u) {
+                        near = __longlong_as_double(static_cast<long long>(__ldcg(&dist[(vb + l) * kTile + lane]))) < theta;
+                    }
+                    const unsigned nmask = __ballot_sync(kFullMask, near);
+                    if (nmask != 0u && lane == 0) {
+                        const int64_t vv = vb + l;
+                        far[vv] = f & ~nmask;
+                        pend_cur[vv] = nmask;
+                        q_cur[atomicAdd(&s.qlen[cur], 1)] = static_cast<int32_t>(vv);
+                    }
+                }
+            }
+            __syncthreads();
+            if (tid == 0) {
+                s.theta = theta;
+            }
+            __syncthreads();
+        }
+        if (s.stop != 0) {
+            break;
+        }
+
+        // ------------------------------------------------------------ epilogue: fused APSP summaries, reset
+        const int my_src = s_src[lane];
+        const bool valid = lane < nsrc;
+        unsigned long long unreach = 0, arcs = 0, mx = 0, overflow = 0;
+        for (int64_t v = warp; v < n; v += nwarps) {
+            unsigned long long* slot_ptr = &dist[v * kTile + lane];
+            const unsigned long long bits = __ldcg(slot_ptr);
+            *slot_ptr = kInfBits;
+            if (!valid) {
+                continue;
+            }
+            const double d = __longlong_as_double(static_cast<long long>(bits));
+            if (p.out.rows != nullptr) {
+                p.out.rows[(base + lane) * n + v] = d;
+            }
+            if (bits == kInfBits) {
+                ++unreach;
+                continue;
+            }
+            arcs += static_cast<unsigned long long>(__ldg(&p.g.row_ptr[v + 1]) - __ldg(&p.g.row_ptr[v]));
+            mx = bits > mx ? bits : mx;
+            acc_add_shared(&s_acc_sum[lane * kAccDigits], d);
+            if (bits != 0ull) {
+                acc_add_shared(&s_acc_inv[lane * kAccDigits], __ddiv_rn(1.0, d));
+            }
+            if (p.out.hist_bins > 0 && v != my_src) {
+                if (d >= p.out.hist_max) {
+                    ++overflow;
+                } else {
+                    unsigned long long bin = static_cast<unsigned long long>(__ddiv_rn(d, p.out.hist_width));
+                    if (bin >= static_cast<unsigned long long>(p.out.hist_bins)) {
+                        bin = static_cast<unsigned long long>(p.out.hist_bins) - 1ull;
+                    }
+                    atomicAdd(&s_hist[bin], 1u);
+                }
+            }
+        }
+        if (valid) {
+            atomicAdd(&s_unreach[lane], unreach);
+            atomicAdd(&s_arcs[lane], arcs);
+            atomicMax(&s_max[lane], mx);
+        }
+        if (overflow != 0) {
+            atomicAdd(&s.overflow, overflow);
+        }
+        __syncthreads();
+        if (tid < nsrc) {
+            unsigned long long* a_sum = &s_acc_sum[tid * kAccDigits];
+            unsigned long long* a_inv = &s_acc_inv[tid * kAccDigits];
+            acc_normalize(a_sum);
+            acc_normalize(a_inv);
+            const int64_t pos = base + tid;
+            if (p.out.src_sum != nullptr) p.out.src_sum[pos] = acc_round_normalized(a_sum);
+            if (p.out.src_inv != nullptr) p.out.src_inv[pos] = acc_round_normalized(a_inv);
+            if (p.out.src_max != nullptr) p.out.src_max[pos] = __longlong_as_double(static_cast<long long>(s_max[tid]));
+            if (p.out.src_unreach != nullptr) p.out.src_unreach[pos] = s_unreach[tid];
+            if (p.out.src_arcs != nullptr) p.out.src_arcs[pos] = s_arcs[tid];
+            const unsigned long long reached = static_cast<unsigned long long>(n) - s_unreach[tid];
+            atomicAdd(&p.out.counters[kUnreachable], s_unreach[tid]);
+            atomicAdd(&p.out.counters[kReachedPairs], reached - 1ull);
+            atomicAdd(&p.out.counters[kTraversedArcs], s_arcs[tid]);
+            atomicMax(&p.out.counters[kDiameterBits], s_max[tid]);
+        }
+        __syncthreads();
+        for (int i = tid; i < kAccDigits; i += blockDim.x) {
+            unsigned long long t_sum = 0, t_inv = 0;
+            for (int k = 0; k < nsrc; ++k) {
+                t_sum += s_acc_sum[k * kAccDigits + i];
+                t_inv += s_acc_inv[k * kAccDigits + i];
+            }
+            if (t_sum != 0) atomicAdd(&p.out.acc_sum[i], t_sum);
+            if (t_inv != 0) atomicAdd(&p.out.acc_inv[i], t_inv);
+        }
+        for (int i = tid; i < p.out.hist_bins; i += blockDim.x) {
+            if (s_hist[i] != 0u) {
+                atomicAdd(&p.out.hist[i], static_cast<unsigned long long>(s_hist[i]));
+                s_hist[i] = 0u;
+            }
+        }
+        if (tid == 0) {
+            if (s.overflow != 0) atomicAdd(&p.out.counters[kHistOverflow], s.overflow);
+            atomicAdd(&p.out.counters[kIterations], s.iterations);
+        }
+        __syncthreads();
+        for (int i = tid; i < 2 * kTile * kAccDigits; i += blockDim.x) {
+            smem[i] = 0ull;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------------------------ plain form
+__device__ __forceinline__ void plain_push(bool push, int x, int lane, int32_t* q, int* qlen) {
+    const unsigned mask = __ballot_sync(kFullMask, push);
+    if (mask == 0u) {
+        return;
+    }
+    int base = 0;
+    if (lane == __ffs(mask) - 1) {
+        base = atomicAdd(qlen, __popc(mask));
+    }
+    base = __shfl_sync(kFullMask, base, __ffs(mask) - 1);
+    if (push) {
+        q[base + __popc(mask & lanemask_lt())] = x;
+    }
+}
+
+__global__ void __launch_bounds__(512, 2) sssp_plain_kernel(const SsspParams p) {
+    extern __shared__ __align__(16) unsigned long long smem[];
+    const int nwarps_max = 16;
+    unsigned long long* s_acc_sum = smem;                             // nwarps_max * kAccDigits (one per warp)
+    unsigned long long* s_acc_inv = smem + nwarps_max * kAccDigits;
+    unsigned int* s_hist = reinterpret_cast<unsigned int*>(smem + 2 * nwarps_max * kAccDigits);
+    __shared__ TileShared s;
+    __shared__ unsigned long long s_unreach, s_arcs, s_max;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int64_t n = p.g.n;
+    const int64_t slot = blockIdx.x;
+
+    unsigned long long* dist = p.ws_dist + slot * n;
+    uint32_t* pend0 = p.ws_pend + slot * 2 * n;
+    uint32_t* pend1 = pend0 + n;
+    uint32_t* far = p.ws_far + slot * n;
+    int32_t* q0 = p.ws_queue + slot * 2 * n;
+    int32_t* q1 = q0 + n;
+    uint32_t* stamp = p.ws_stamp + slot * n;
+
+    for (int64_t i = tid; i < n; i += blockDim.x) {
+        dist[i] = kInfBits;
+        pend0[i] = 0u;
+        pend1[i] = 0u;
+        far[i] = 0u;
+        stamp[i] = 0u;
+    }
+    for (int i = tid; i < 2 * nwarps_max * kAccDigits; i += blockDim.x) {
+        smem[i] = 0ull;
+    }
+    for (int i = tid; i < p.out.hist_bins; i += blockDim.x) {
+        s_hist[i] = 0u;
+    }
+    if (tid == 0) {
+        s.stamp = 1u;
+    }
+    __syncthreads();
+
+    for (;;) {
+        if (tid == 0) {
+            s.tile = static_cast<long long>(atomicAdd(p.tile_counter, 1ull));
+            s.stop = (*reinterpret_cast<volatile int*>(p.error) != 0) ? 1 : 0;
+            s.qlen[0] = 0;
+            s.qlen[1] = 0;
+            s.cur = 0;
+            s.theta = p.delta;
+            s.iterations = 0;
+            s.overflow = 0;
+            s_unreach = 0;
+            s_arcs = 0;
+            s_max = 0;
+        }
+        __syncthreads();
+        if (s.stop != 0 || s.tile >= p.num_tiles) {
+            break;
+        }
+        const int64_t pos = s.tile;
+        const int src = p.sources[pos];
+        if (tid == 0) {
+            dist[src] = 0ull;
+            pend0[src] = 1u;
+            stamp[src] = s.stamp;
+            q0[0] = src;
+            s.qlen[0] = 1;
+        }
+        __syncthreads();
+
+        for (;;) {
+            for (;;) {
+                const int cur = s.cur;
+                const int qlen = s.qlen[cur];
+                if (qlen == 0) {
+                    break;
+                }
+                uint32_t* pend_cur = cur ? pend1 : pend0;
+                uint32_t* pend_nxt = cur ? pend0 : pend1;
+                const int32_t* q_cur = cur ? q1 : q0;
+                int32_t* q_nxt = cur ? q0 : q1;
+                const unsigned next_stamp = s.stamp + 1u;
+                const double theta = s.theta;
+                for (int i = warp; i < qlen; i += nwarps) {
+                    const int v = __ldcg(&q_cur[i]);
+                    if (__ldcg(&pend_cur[v]) == 0u) {
+                        continue;
+                    }
+                    const double dv = __longlong_as_double(static_cast<long long>(__ldcg(&dist[v])));
+                    if (lane == 0) {
+                        pend_cur[v] = 0u;
+                        far[v] = 0u;  // a near value supersedes any far mark; no far mark can be set while d[v] < theta
+                    }
+                    const int64_t beg = __ldg(&p.g.row_ptr[v]);
+                    const int64_t end = __ldg(&p.g.row_ptr[v + 1]);
+                    for (int64_t e0 = beg; e0 < end; e0 += 32) {
+                        const int64_t e = e0 + lane;
+                        bool push = false;
+                        int x = 0;
+                        if (e < end) {
+                            const Arc a = p.g.arcs[e];
+                            x = a.col;
+                            const double nd = __dadd_rn(dv, a.len);
+                            const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd));
+                            if (nb < __ldcg(&dist[x])) {
+                                const unsigned long long old = atomicMin(&dist[x], nb);
+                                if (nb < old) {
+                                    if (nd < theta) {
+                                        pend_nxt[x] = 1u;
+                                        push = atomicExch(&stamp[x], next_stamp) != next_stamp;
+                                    } else {
+                                        far[x] = 1u;
+                                    }
+                                }
+                            }
+                        }
+                        plain_push(push, x, lane, q_nxt, &s.qlen[cur ^ 1]);
+                    }
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    s.qlen[cur] = 0;
+                    s.cur = cur ^ 1;
+                    s.stamp = next_stamp;
+                    s.iterations += 1;
+                    if (s.iterations > p.max_iterations) {
+                        atomicCAS(p.error, kDevOk, kDevTimeout);
+                        s.stop = 1;
+                    } else if (*p.abort_flag != 0) {
+                        atomicCAS(p.error, kDevOk, kDevAborted);
+                        s.stop = 1;
+                    }
+                }
+                __syncthreads();
+                if (s.stop != 0) {
+                    break;
+                }
+            }
+            if (s.stop != 0) {
+                break;
+            }
+            if (tid == 0) {
+                s.min_bits = kInfBits;
+            }
+            __syncthreads();
+            unsigned long long local_min = kInfBits;
+            for (int64_t v = tid; v < n; v += blockDim.x) {
+                if (__ldcg(&far[v]) != 0u) {
+                    const unsigned long long d = __ldcg(&dist[v]);
+                    local_min = d < local_min ? d : local_min;
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const unsigned long long o = __shfl_xor_sync(kFullMask, local_min, off);
+                local_min = o < local_min ? o : local_min;
+            }
+            if (lane == 0 && local_min != kInfBits) {
+                atomicMin(&s.min_bits, local_min);
+            }
+            __syncthreads();
+            if (s.min_bits == kInfBits) {
+                break;
+            }
+            const double theta = next_theta(__longlong_as_double(static_cast<long long>(s.min_bits)), p.delta);
+            const int cur = s.cur;
+            uint32_t* pend_cur = cur ? pend1 : pend0;
+            int32_t* q_cur = cur ? q1 : q0;
+            for (int64_t vb = 0; vb < n; vb += blockDim.x) {
+                const int64_t v = vb + tid;
+                bool push = false;
+                if (v < n && __ldcg(&far[v]) != 0u) {
+                    if (__longlong_as_double(static_cast<long long>(__ldcg(&dist[v]))) < theta) {
+                        far[v] = 0u;
+                        pend_cur[v] = 1u;
+                        push = true;
+                    }
+                }
+                plain_push(push, static_cast<int>(v), lane, q_cur, &s.qlen[cur]);
+            }
+            __syncthreads();
+            if (tid == 0) {
+                s.theta = theta;
+            }
+            __syncthreads();
+        }
+        if (s.stop != 0) {
+            break;
+        }
+
+        // epilogue: one accumulator pair per warp, combined exactly
+        unsigned long long* a_sum = &s_acc_sum[warp * kAccDigits];
+        unsigned long long* a_inv = &s_acc_inv[warp * kAccDigits];
+        unsigned long long unreach = 0, arcs = 0, mx = 0, overflow = 0;
+        for (int64_t v = tid; v < n; v += blockDim.x) {
+            const unsigned long long bits = __ldcg(&dist[v]);
+            dist[v] = kInfBits;
+            const double d = __longlong_as_double(static_cast<long long>(bits));
+            if (p.out.rows != nullptr) {
+                p.out.rows[pos * n + v] = d;
+            }
+            if (bits == kInfBits) {
+                ++unreach;
+                continue;
+            }
+            arcs += static_cast<unsigned long long>(__ldg(&p.g.row_ptr[v + 1]) - __ldg(&p.g.row_ptr[v]));
+            mx = bits > mx ? bits : mx;
+            acc_add_shared(a_sum, d);
+            if (bits != 0ull) {
+                acc_add_shared(a_inv, __ddiv_rn(1.0, d));
+            }
+            if (p.out.hist_bins > 0 && v != src) {
+                if (d >= p.out.hist_max) {
+                    ++overflow;
+                } else {
+                    unsigned long long bin = static_cast<unsigned long long>(__ddiv_rn(d, p.out.hist_width));
+                    if (bin >= static_cast<unsigned long long>(p.out.hist_bins)) {
+                        bin = static_cast<unsigned long long>(p.out.hist_bins) - 1ull;
+                    }
+                    atomicAdd(&s_hist[bin], 1u);
+                }
+            }
+        }
+        atomicAdd(&s_unreach, unreach);
+        atomicAdd(&s_arcs, arcs);
+        atomicMax(&s_max, mx);
+        if (overflow != 0) {
+            atomicAdd(&s.overflow, overflow);
+        }
+        __syncthreads();
+        // fold the per-warp accumulators into warp 0's, digit-wise (each digit < 2^33 * adds, far below 2^64)
+        for (int i = tid; i < kAccDigits; i += blockDim.x) {
+            for (int w = 1; w < nwarps; ++w) {
+                s_acc_sum[i] += s_acc_sum[w * kAccDigits + i];
+                s_acc_inv[i] += s_acc_inv[w * kAccDigits + i];
+                s_acc_sum[w * kAccDigits + i] = 0ull;
+                s_acc_inv[w * kAccDigits + i] = 0ull;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            acc_normalize(s_acc_sum);
+            acc_normalize(s_acc_inv);
+            if (p.out.src_sum != nullptr) p.out.src_sum[pos] = acc_round_normalized(s_acc_sum);
+            if (p.out.src_inv != nullptr) p.out.src_inv[pos] = acc_round_normalized(s_acc_inv);
+            if (p.out.src_max != nullptr) p.out.src_max[pos] = __longlong_as_double(static_cast<long long>(s_max));
+            if (p.out.src_unreach != nullptr) p.out.src_unreach[pos] = s_unreach;
+            if (p.out.src_arcs != nullptr) p.out.src_arcs[pos] = s_arcs;
+            atomicAdd(&p.out.counters[kUnreachable], s_unreach);
+            atomicAdd(&p.out.counters[kReachedPairs], static_cast<unsigned long long>(n) - s_unreach - 1ull);
+            atomicAdd(&p.out.counters[kTraversedArcs], s_arcs);
+            atomicMax(&p.out.counters[kDiameterBits], s_max);
+            if (s.overflow != 0) atomicAdd(&p.out.counters[kHistOverflow], s.overflow);
+            atomicAdd(&p.out.counters[kIterations], s.iterations);
+        }
+        __syncthreads();
+        for (int i = tid; i < kAccDigits; i += blockDim.x) {
+            if (s_acc_sum[i] != 0) atomicAdd(&p.out.acc_sum[i], s_acc_sum[i]);
+            if (s_acc_inv[i] != 0) atomicAdd(&p.out.acc_inv[i], s_acc_inv[i]);
+        }
+        for (int i = tid; i < p.out.hist_bins; i += blockDim.x) {
+            if (s_hist[i] != 0u) {
+                atomicAdd(&p.out.hist[i], static_cast<unsigned long long>(s_hist[i]));
+                s_hist[i] = 0u;
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < kAccDigits; i += blockDim.x) {
+            s_acc_sum[i] = 0ull;
+            s_acc_inv[i] = 0ull;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace ngx
