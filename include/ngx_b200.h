@@ -101,6 +101,9 @@ typedef struct {
     double cpl;               /* characteristic path length sum_distances / R (AllPairsShortestPath.h:154-157) */
     double efficiency;        /* global efficiency sum_inverse / R (AllPairsShortestPath.h:158) */
     double kernel_ms;         /* device time of the run's kernels (CUDA events) */
+    uint64_t phases;          /* delta-stepping phases (near iterations) summed over source tiles */
+    uint64_t expansions;      /* vertex expansions: one pass over a vertex's out-arcs */
+    uint64_t lane_expansions; /* (vertex, source) expansions; lane_expansions / expansions = sources per arc pass */
     /* optional outputs */
     uint64_t* hist;           /* hist_bins entries */
     double* src_sum;          /* per source: exactly rounded sum of distances */

@@ -27,7 +27,16 @@ struct RunOutputs {
     size_t bytes = 0;
 };
 
+// Device buffers of the DAG passes: per-vertex betweenness and per-arc gradients in 128-bit fixed point.
+struct DagOutputs {
+    unsigned long long* bc = nullptr;        // 2 * n
+    unsigned long long* grad_cpl = nullptr;  // 2 * m_user
+    unsigned long long* grad_eff = nullptr;  // 2 * m_user
+    unsigned long long* levels = nullptr;    // 1
+};
+
 int check_opts(const ngx_graph* g, const ngx_apsp_opts* opts);
+int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, double* rows, int tile_mode, DagOutputs* extra);
 int prepare_sources(const ngx_graph* g, const ngx_apsp_opts* opts, std::vector<int32_t>& sources);
 double pick_delta(const ngx_graph* g, int metric, double requested);
 int alloc_outputs(ngx_graph* g, int64_t num_sources, int64_t hist_bins, bool want_rows, RunOutputs& o);

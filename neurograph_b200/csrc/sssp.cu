@@ -19,8 +19,9 @@
 namespace ngx {
 
 namespace {
-constexpr int kBatchedUnroll = 8;
+constexpr int kBatchedUnroll = 4;
 constexpr int kPlainWarpsMax = 16;
+constexpr int kBatchedDefaultBlock = 384;
 }  // namespace
 
 int prepare_sources(const ngx_graph* g, const ngx_apsp_opts* opts, std::vector<int32_t>& sources) {
@@ -119,17 +120,36 @@ int device_error_status(int code) {
     }
 }
 
-// One persistent SSSP launch over `sources` (tile order). Leaves reduced outputs in `o`.
-int launch_sssp(ngx_graph* g, const ngx_apsp_opts* opts, const int32_t* d_sources, int64_t num_sources, int64_t hist_bins, double hist_max,
-                RunOutputs& o, float* kernel_ms) {
-    const bool batched = opts->mode == NGX_MODE_BATCHED;
+template <int kMode>
+const void* tile_kernel_for_block(int block) {
+    switch (block) {
+    case 256: return reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 256, 3>);
+    case 384: return reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 384, 2>);
+    case 512: return reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 512, 2>);
+    default: return nullptr;
+    }
+}
+
+// One persistent launch over `sources` (tile order): SSSP with the fused APSP epilogue, plus Brandes or the adjoint
+// when `tile_mode` asks for them (batched form only). Leaves reduced outputs in `o` and the DAG outputs in `extra`.
+int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const int32_t* d_sources, int64_t num_sources, int64_t hist_bins,
+                 double hist_max, RunOutputs& o, DagOutputs* extra, float* kernel_ms) {
+    const bool batched = opts->mode == NGX_MODE_BATCHED || tile_mode != kModeApsp;
     const int width = batched ? kTile : 1;
     const int64_t num_tiles = batched ? (num_sources + kTile - 1) / kTile : num_sources;
-    const int block = opts->block_threads > 0 ? opts->block_threads : (batched ? 512 : 512);
+    const int block = opts->block_threads > 0 ? opts->block_threads : (batched ? kBatchedDefaultBlock : 512);
     const size_t acc_bytes = static_cast<size_t>(2) * (batched ? kTile : kPlainWarpsMax) * kAccDigits * 8;
     const size_t smem = acc_bytes + static_cast<size_t>(hist_bins) * 4;
 
-    const void* kernel = batched ? reinterpret_cast<const void*>(&sssp_batched_kernel<kBatchedUnroll>) : reinterpret_cast<const void*>(&sssp_plain_kernel);
+    const void* kernel = reinterpret_cast<const void*>(&sssp_plain_kernel);
+    if (batched) {
+        kernel = tile_mode == kModeBrandes ? tile_kernel_for_block<kModeBrandes>(block)
+                 : tile_mode == kModeGrad  ? tile_kernel_for_block<kModeGrad>(block)
+                                           : tile_kernel_for_block<kModeApsp>(block);
+        if (kernel == nullptr) {
+            return fail(NGX_INVALID_ARGUMENT, "batched mode supports block_threads 256, 384 or 512");
+        }
+    }
     NGX_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     int per_sm = 0;
     NGX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem));
@@ -139,7 +159,7 @@ int launch_sssp(ngx_graph* g, const ngx_apsp_opts* opts, const int32_t* d_source
     if (opts->ctas_per_sm > 0) {
         per_sm = std::min(per_sm, opts->ctas_per_sm);
     }
-    const size_t slot_bytes = sssp_slot_bytes(g->n, width);
+    const size_t slot_bytes = sssp_slot_bytes(g->n, width) + (tile_mode != kModeApsp ? brandes_slot_bytes(g->n, tile_mode == kModeGrad) : 0);
     const size_t budget = workspace_budget(g);
     int64_t slots = std::min<int64_t>(num_tiles, static_cast<int64_t>(g->sm_count) * per_sm);
     slots = std::min<int64_t>(slots, static_cast<int64_t>(budget / slot_bytes));
@@ -170,6 +190,34 @@ int launch_sssp(ngx_graph* g, const ngx_apsp_opts* opts, const int32_t* d_source
     p.ws_queue = reinterpret_cast<int32_t*>(ws);
     ws += static_cast<size_t>(slots) * 2 * n * 4;
     p.ws_stamp = reinterpret_cast<uint32_t*>(ws);
+    ws += static_cast<size_t>(slots) * n * 4;
+    BrandesParams bp{};
+    if (tile_mode != kModeApsp) {
+        const size_t nt = static_cast<size_t>(n) * kTile;
+        ws = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(ws) + 255) & ~uintptr_t(255));
+        bp.rg = g->reverse_csr();
+        bp.ws_sigma = reinterpret_cast<double*>(ws);
+        ws += static_cast<size_t>(slots) * nt * 8;
+        bp.ws_delta = reinterpret_cast<double*>(ws);
+        ws += static_cast<size_t>(slots) * nt * 8;
+        if (tile_mode == kModeGrad) {
+            bp.ws_delta_g = reinterpret_cast<double*>(ws);
+            ws += static_cast<size_t>(slots) * nt * 8;
+        }
+        bp.ws_cnt = reinterpret_cast<uint32_t*>(ws);
+        ws += static_cast<size_t>(slots) * nt * 4;
+        bp.ws_lvl = reinterpret_cast<uint32_t*>(ws);
+        ws += static_cast<size_t>(slots) * nt * 4;
+        bp.ws_list = reinterpret_cast<int32_t*>(ws);
+        ws += static_cast<size_t>(slots) * nt * 4;
+        bp.ws_loff = reinterpret_cast<int32_t*>(ws);
+        if (extra != nullptr) {
+            bp.bc = extra->bc;
+            bp.grad_cpl = extra->grad_cpl;
+            bp.grad_eff = extra->grad_eff;
+            bp.levels = extra->levels;
+        }
+    }
     p.out.acc_sum = o.acc;
     p.out.acc_inv = o.acc + kAccDigits;
     p.out.counters = o.counters;
@@ -189,7 +237,13 @@ int launch_sssp(ngx_graph* g, const ngx_apsp_opts* opts, const int32_t* d_source
     NGX_CUDA_TRY(cudaEventCreate(&stop));
     cudaEventRecord(start, g->stream);
     if (batched) {
-        sssp_batched_kernel<kBatchedUnroll><<<static_cast<unsigned>(slots), block, smem, g->stream>>>(p);
+        void* args[] = { &p, &bp };
+        const cudaError_t launch = cudaLaunchKernel(kernel, dim3(static_cast<unsigned>(slots)), dim3(block), args, smem, g->stream);
+        if (launch != cudaSuccess) {
+            cudaEventDestroy(start);
+            cudaEventDestroy(stop);
+            return cuda_fail(launch, "sssp kernel launch");
+        }
     } else {
         sssp_plain_kernel<<<static_cast<unsigned>(slots), block, smem, g->stream>>>(p);
     }
@@ -231,7 +285,7 @@ int auto_hist_max(ngx_graph* g, const ngx_apsp_opts* opts, const std::vector<int
     ngx_apsp_opts sample_opts = *opts;
     sample_opts.mode = NGX_MODE_BATCHED;
     if (rc == NGX_OK) {
-        rc = launch_sssp(g, &sample_opts, d_sample, k, 0, 0.0, o, nullptr);
+        rc = launch_tiles(g, &sample_opts, kModeApsp, d_sample, k, 0, 0.0, o, nullptr, nullptr);
     }
     unsigned long long bits = 0;
     if (rc == NGX_OK && cudaMemcpy(&bits, o.counters + kDiameterBits, 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
@@ -261,6 +315,9 @@ int collect(ngx_graph* g, const RunOutputs& o, int64_t num_sources, int64_t hist
     r->traversed_arcs = counters[kTraversedArcs];
     r->hist_overflow = counters[kHistOverflow];
     r->hist_max = hist_max;
+    r->phases = counters[kIterations];
+    r->expansions = counters[kExpansions];
+    r->lane_expansions = counters[kLaneExpansions];
     r->cpl = r->sum_distances / static_cast<double>(r->reached_pairs);
     r->efficiency = r->sum_inverse / static_cast<double>(r->reached_pairs);
     const size_t s = static_cast<size_t>(num_sources);
@@ -284,9 +341,10 @@ void clear_result_totals(ngx_apsp_result* r) {
     r->hist_max = 0.0;
     r->cpl = r->efficiency = 0.0;
     r->kernel_ms = 0.0;
+    r->phases = r->expansions = r->lane_expansions = 0;
 }
 
-int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, double* rows) {
+int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, double* rows, int tile_mode, DagOutputs* extra) {
     if (const int rc = check_opts(g, opts); rc != NGX_OK) {
         return rc;
     }
@@ -318,7 +376,7 @@ int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, d
     int rc = alloc_outputs(g, num_sources, hist_bins, rows != nullptr, o);
     float ms = 0.0f;
     if (rc == NGX_OK) {
-        rc = launch_sssp(g, opts, d_sources, num_sources, hist_bins, hist_max, o, &ms);
+        rc = launch_tiles(g, opts, tile_mode, d_sources, num_sources, hist_bins, hist_max, o, extra, &ms);
     }
     if (rc == NGX_OK) {
         rc = collect(g, o, num_sources, hist_bins, hist_max, r);
@@ -342,7 +400,7 @@ using namespace ngx;
 
 extern "C" {
 
-int ngx_apsp(ngx_graph* graph, const ngx_apsp_opts* opts, ngx_apsp_result* result) { return run_apsp(graph, opts, result, nullptr); }
+int ngx_apsp(ngx_graph* graph, const ngx_apsp_opts* opts, ngx_apsp_result* result) { return run_apsp(graph, opts, result, nullptr, kModeApsp, nullptr); }
 
 int ngx_sssp_rows(ngx_graph* graph, const ngx_apsp_opts* opts, double* rows) {
     if (rows == nullptr) {
@@ -350,7 +408,7 @@ int ngx_sssp_rows(ngx_graph* graph, const ngx_apsp_opts* opts, double* rows) {
     }
     ngx_apsp_opts o = *opts;
     o.hist_bins = 0;
-    return run_apsp(graph, &o, nullptr, rows);
+    return run_apsp(graph, &o, nullptr, rows, kModeApsp, nullptr);
 }
 
 }  // extern "C"

@@ -30,6 +30,7 @@
 
 #include <cstdint>
 
+#include "brandes_kernels.cuh"
 #include "ngx_common.cuh"
 
 namespace ngx {
@@ -52,7 +53,17 @@ struct TileOutputs {
     double* rows;                   // num_sources x n distance rows (or nullptr)
 };
 
-enum Counter : int { kUnreachable = 0, kReachedPairs = 1, kTraversedArcs = 2, kHistOverflow = 3, kDiameterBits = 4, kIterations = 5, kCounterCount = 8 };
+enum Counter : int {
+    kUnreachable = 0,
+    kReachedPairs = 1,
+    kTraversedArcs = 2,
+    kHistOverflow = 3,
+    kDiameterBits = 4,
+    kIterations = 5,   // near iterations (phases) over all tiles
+    kExpansions = 6,   // vertex expansions (one warp pass over a vertex's arcs)
+    kLaneExpansions = 7,  // (vertex, source) expansions; kLaneExpansions / kExpansions = sources sharing one arc pass
+    kCounterCount = 8
+};
 
 struct SsspParams {
     DeviceCsr g;
@@ -100,20 +111,32 @@ struct TileShared {
     unsigned long long min_bits;
     unsigned long long iterations;
     unsigned long long overflow;
+    // Brandes / adjoint levels
+    unsigned level;
+    int lvl_start;
+    int lvl_len;
+    int next_len;
 };
 
 // ------------------------------------------------------------------------------------------ batched form
+// Expands vertex v for the k sources pending on it. The deg(v) x k (arc, source) pairs are spread over the 32 lanes:
+// pair p = 32 i + lane takes arc p / k and the (p % k)-th pending source, so no lane idles when few sources are
+// pending, and when all 32 are, every iteration reads one whole distance row d[x][0..31] (256 contiguous bytes).
 template <int kUnroll>
 __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, int lane, unsigned long long* __restrict__ dist, uint32_t* pend_cur,
                                                uint32_t* pend_nxt, uint32_t* far, int32_t* q_nxt, int* qlen_nxt, uint32_t* stamp, unsigned next_stamp,
-                                               double theta) {
+                                               double theta, unsigned long long& expansions, unsigned long long& lane_expansions) {
     const uint32_t amask = __ldcg(&pend_cur[v]);
     if (amask == 0) {
         return;
     }
     __syncwarp();
-    const bool act = (amask >> lane) & 1u;
-    const double dv = act ? __longlong_as_double(static_cast<long long>(__ldcg(&dist[static_cast<int64_t>(v) * kTile + lane]))) : 0.0;
+    const int k = __popc(amask);
+    expansions += 1;
+    lane_expansions += static_cast<unsigned long long>(k);
+    // lane r < k holds the r-th pending source and its distance to v
+    const int rank_src = lane < k ? static_cast<int>(__fns(amask, 0, lane + 1)) : 0;
+    const double rank_dv = __longlong_as_double(static_cast<long long>(__ldcg(&dist[static_cast<int64_t>(v) * kTile + rank_src])));
     if (lane == 0) {
         pend_cur[v] = 0u;
         if (__ldcg(&far[v]) & amask) {
@@ -121,61 +144,77 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, int la
         }
     }
     const int64_t beg = __ldg(&g.row_ptr[v]);
-    const int64_t end = __ldg(&g.row_ptr[v + 1]);
-    for (int64_t e0 = beg; e0 < end; e0 += 32) {
-        const int cnt = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
-        Arc a{ 0, 0, 0.0 };
-        if (lane < cnt) {
-            a = g.arcs[e0 + lane];
-        }
-        for (int j = 0; j < cnt; j += kUnroll) {
-            int x[kUnroll];
-            double nd[kUnroll];
-            unsigned long long cur[kUnroll];
+    const int deg = static_cast<int>(__ldg(&g.row_ptr[v + 1]) - beg);
+    const Arc* arcs = g.arcs + beg;
+    // position of this lane's first pair, and the per-iteration advance of 32 pairs
+    int a = lane / k;
+    int r = lane - a * k;
+    const int step_a = 32 / k;
+    const int step_r = 32 - step_a * k;
+    const int64_t total = static_cast<int64_t>(deg) * k;
+    for (int64_t p0 = 0; p0 < total; p0 += 32 * kUnroll) {
+        int x[kUnroll];
+        int src[kUnroll];
+        double nd[kUnroll];
+        unsigned long long cur[kUnroll];
+        bool valid[kUnroll];
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
-                const int jj = j + u;
-                const int from = jj < cnt ? jj : 0;
-                x[u] = __shfl_sync(kFullMask, a.col, from);
-                const double len = __shfl_sync(kFullMask, a.len, from);
-                nd[u] = __dadd_rn(dv, len);
-                cur[u] = (act && jj < cnt) ? __ldcg(&dist[static_cast<int64_t>(x[u]) * kTile + lane]) : 0ull;
+        for (int u = 0; u < kUnroll; ++u) {
+            valid[u] = a < deg;
+            src[u] = __shfl_sync(kFullMask, rank_src, r);
+            const double dvs = __shfl_sync(kFullMask, rank_dv, r);
+            x[u] = 0;
+            nd[u] = 0.0;
+            cur[u] = 0ull;
+            if (valid[u]) {
+                const Arc arc = arcs[a];
+                x[u] = arc.col;
+                nd[u] = __dadd_rn(dvs, arc.len);
+                cur[u] = __ldcg(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]]);
             }
+            a += step_a;
+            r += step_r;
+            if (r >= k) {
+                r -= k;
+                a += 1;
+            }
+        }
 #pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
-                const int jj = j + u;
-                bool improved = false;
-                if (act && jj < cnt) {
-                    const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd[u]));
-                    if (nb < cur[u]) {
-                        const unsigned long long old = atomicMin(&dist[static_cast<int64_t>(x[u]) * kTile + lane], nb);
-                        improved = nb < old;
+        for (int u = 0; u < kUnroll; ++u) {
+            bool push = false;
+            if (valid[u]) {
+                const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd[u]));
+                if (nb < cur[u]) {
+                    const unsigned long long old = atomicMin(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]], nb);
+                    if (nb < old) {
+                        const uint32_t bit = 1u << src[u];
+                        if (nd[u] < theta) {
+                            atomicOr(&pend_nxt[x[u]], bit);
+                            push = atomicExch(&stamp[x[u]], next_stamp) != next_stamp;
+                        } else {
+                            atomicOr(&far[x[u]], bit);
+                        }
                     }
                 }
-                const unsigned imask = __ballot_sync(kFullMask, improved);
-                if (imask != 0u) {
-                    const unsigned nmask = __ballot_sync(kFullMask, improved && nd[u] < theta);
-                    if (lane == 0) {
-                        const int xv = x[u];
-                        if (nmask != 0u) {
-                            atomicOr(&pend_nxt[xv], nmask);
-                            if (atomicExch(&stamp[xv], next_stamp) != next_stamp) {
-                                q_nxt[atomicAdd(qlen_nxt, 1)] = xv;
-                            }
-                        }
-                        const unsigned fmask = imask & ~nmask;
-                        if (fmask != 0u) {
-                            atomicOr(&far[xv], fmask);
-                        }
-                    }
+            }
+            const unsigned pmask = __ballot_sync(kFullMask, push);
+            if (pmask != 0u) {
+                int base = 0;
+                const int leader = __ffs(pmask) - 1;
+                if (lane == leader) {
+                    base = atomicAdd(qlen_nxt, __popc(pmask));
+                }
+                base = __shfl_sync(kFullMask, base, leader);
+                if (push) {
+                    q_nxt[base + __popc(pmask & lanemask_lt())] = x[u];
                 }
             }
         }
     }
 }
 
-template <int kUnroll>
-__global__ void __launch_bounds__(512, 2) sssp_batched_kernel(const SsspParams p) {
+template <int kMode, int kUnroll, int kBlock, int kMinBlocks>
+__global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspParams p, const BrandesParams b) {
     extern __shared__ __align__(16) unsigned long long smem[];
     unsigned long long* s_acc_sum = smem;                                // kTile * kAccDigits
     unsigned long long* s_acc_inv = smem + kTile * kAccDigits;          // kTile * kAccDigits
@@ -192,6 +231,7 @@ __global__ void __launch_bounds__(512, 2) sssp_batched_kernel(const SsspParams p
     const int nwarps = blockDim.x >> 5;
     const int64_t n = p.g.n;
     const int64_t slot = blockIdx.x;
+    unsigned long long expansions = 0, lane_expansions = 0;
 
     unsigned long long* dist = p.ws_dist + slot * n * kTile;
     uint32_t* pend0 = p.ws_pend + slot * 2 * n;
@@ -200,6 +240,32 @@ __global__ void __launch_bounds__(512, 2) sssp_batched_kernel(const SsspParams p
     int32_t* q0 = p.ws_queue + slot * 2 * n;
     int32_t* q1 = q0 + n;
     uint32_t* stamp = p.ws_stamp + slot * n;
+    const int64_t nt = n * kTile;
+    double* sigma = nullptr;
+    double* delta = nullptr;
+    double* delta_g = nullptr;
+    uint32_t* cnt = nullptr;
+    uint32_t* lvl = nullptr;
+    int32_t* list = nullptr;
+    int32_t* loff = nullptr;
+    if constexpr (kMode != kModeApsp) {
+        sigma = b.ws_sigma + slot * nt;
+        delta = b.ws_delta + slot * nt;
+        delta_g = kMode == kModeGrad ? b.ws_delta_g + slot * nt : nullptr;
+        cnt = b.ws_cnt + slot * nt;
+        lvl = b.ws_lvl + slot * nt;
+        list = b.ws_list + slot * nt;
+        loff = b.ws_loff + slot * (n + 2);
+        for (int64_t i = tid; i < nt; i += blockDim.x) {
+            sigma[i] = 0.0;
+            delta[i] = 0.0;
+            if constexpr (kMode == kModeGrad) {
+                delta_g[i] = 0.0;
+            }
+            cnt[i] = 0u;
+            lvl[i] = kNoLevel;
+        }
+    }
 
     for (int64_t i = tid; i < n * kTile; i += blockDim.x) {
         dist[i] = kInfBits;
@@ -272,7 +338,8 @@ __global__ void __launch_bounds__(512, 2) sssp_batched_kernel(const SsspParams p
                 const unsigned next_stamp = s.stamp + 1u;
                 const double theta = s.theta;
                 for (int i = warp; i < qlen; i += nwarps) {
-                    batched_expand<kUnroll>(p.g, __ldcg(&q_cur[i]), lane, dist, pend_cur, pend_nxt, far, q_nxt, &s.qlen[cur ^ 1], stamp, next_stamp, theta);
+                    batched_expand<kUnroll>(p.g, __ldcg(&q_cur[i]), lane, dist, pend_cur, pend_nxt, far, q_nxt, &s.qlen[cur ^ 1], stamp, next_stamp, theta,
+                                            expansions, lane_expansions);
                 }
                 __syncthreads();
                 if (tid == 0) {
@@ -364,6 +431,70 @@ __global__ void __launch_bounds__(512, 2) sssp_batched_kernel(const SsspParams p
             break;
         }
 
+        if constexpr (kMode != kModeApsp) {
+            // ------------------------------------------------------------ shortest-path DAG: counts, sigma, delta
+            brandes_count(b.rg, n, nsrc, s_src, dist, cnt, lane, warp, nwarps);
+            if (tid == 0) {
+                s.stamp += 1u;
+                s.level = 0u;
+                s.lvl_start = 0;
+                s.lvl_len = 0;
+                s.next_len = 0;
+                loff[0] = 0;
+            }
+            __syncthreads();
+            if (warp == 0) {
+                const int v = s_src[lane];
+                if (v >= 0) {
+                    const int64_t row = static_cast<int64_t>(v) * kTile + lane;
+                    lvl[row] = 0u;
+                    sigma[row] = 1.0;
+                    if (atomicExch(&stamp[v], s.stamp) != s.stamp) {
+                        list[atomicAdd(&s.lvl_len, 1)] = v;
+                    }
+                }
+            }
+            __syncthreads();
+            for (;;) {
+                const int start = s.lvl_start;
+                const int len = s.lvl_len;
+                if (len == 0) {
+                    break;
+                }
+                const unsigned level = s.level;
+                const unsigned level_stamp = s.stamp + 1u;
+                for (int i = warp; i < len; i += nwarps) {
+                    brandes_sigma_vertex(p.g, b.rg, __ldcg(&list[start + i]), level, nsrc, lane, dist, sigma, cnt, lvl, stamp, level_stamp,
+                                         list + start + len, &s.next_len);
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    s.lvl_start = start + len;
+                    s.lvl_len = s.next_len;
+                    s.next_len = 0;
+                    s.stamp = level_stamp;
+                    s.level = level + 1u;
+                    loff[level + 1u] = start + len;
+                }
+                __syncthreads();
+            }
+            // s.level is one past the last non-empty level; loff[s.level] is the end of the lists
+            const int levels = static_cast<int>(s.level);
+            const int lowest = kMode == kModeGrad ? 0 : 1;
+            for (int level = levels - 1; level >= lowest; --level) {
+                const int start = __ldcg(&loff[level]);
+                const int end = __ldcg(&loff[level + 1]);
+                for (int i = start + warp; i < end; i += nwarps) {
+                    brandes_delta_vertex<kMode>(p.g, __ldcg(&list[i]), static_cast<unsigned>(level), nsrc, lane, dist, sigma, delta, delta_g, lvl,
+                                                b.grad_cpl, b.grad_eff);
+                }
+                __syncthreads();
+            }
+            if (tid == 0 && b.levels != nullptr) {
+                atomicAdd(b.levels, static_cast<unsigned long long>(levels));
+            }
+        }
+
         // ------------------------------------------------------------ epilogue: fused APSP summaries, reset
         const int my_src = s_src[lane];
         const bool valid = lane < nsrc;
@@ -372,6 +503,24 @@ __global__ void __launch_bounds__(512, 2) sssp_batched_kernel(const SsspParams p
             unsigned long long* slot_ptr = &dist[v * kTile + lane];
             const unsigned long long bits = __ldcg(slot_ptr);
             *slot_ptr = kInfBits;
+            if constexpr (kMode != kModeApsp) {
+                const int64_t row = v * kTile + lane;
+                if constexpr (kMode == kModeBrandes) {
+                    // BrandesVariant.h:156: every settled vertex but the source gains its dependency
+                    const double dep = (valid && v != my_src) ? __ldcg(&delta[row]) : 0.0;
+                    const double total = warp_sum(dep);
+                    if (lane == 0 && total > 0.0) {
+                        fixed_add(&b.bc[2 * v], total);
+                    }
+                }
+                sigma[row] = 0.0;
+                delta[row] = 0.0;
+                if constexpr (kMode == kModeGrad) {
+                    delta_g[row] = 0.0;
+                }
+                cnt[row] = 0u;
+                lvl[row] = kNoLevel;
+            }
             if (!valid) {
                 continue;
             }
@@ -453,6 +602,10 @@ __global__ void __launch_bounds__(512, 2) sssp_batched_kernel(const SsspParams p
         }
         __syncthreads();
     }
+    if (lane == 0 && expansions != 0) {
+        atomicAdd(&p.out.counters[kExpansions], expansions);
+        atomicAdd(&p.out.counters[kLaneExpansions], lane_expansions);
+    }
 }
 
 // ------------------------------------------------------------------------------------------ plain form
@@ -486,6 +639,7 @@ __global__ void __launch_bounds__(512, 2) sssp_plain_kernel(const SsspParams p) 
     const int nwarps = blockDim.x >> 5;
     const int64_t n = p.g.n;
     const int64_t slot = blockIdx.x;
+    unsigned long long expansions = 0;
 
     unsigned long long* dist = p.ws_dist + slot * n;
     uint32_t* pend0 = p.ws_pend + slot * 2 * n;
@@ -561,6 +715,7 @@ __global__ void __launch_bounds__(512, 2) sssp_plain_kernel(const SsspParams p) 
                         continue;
                     }
                     const double dv = __longlong_as_double(static_cast<long long>(__ldcg(&dist[v])));
+                    expansions += 1;
                     if (lane == 0) {
                         pend_cur[v] = 0u;
                         far[v] = 0u;  // a near value supersedes any far mark; no far mark can be set while d[v] < theta
@@ -744,6 +899,10 @@ __global__ void __launch_bounds__(512, 2) sssp_plain_kernel(const SsspParams p) 
             s_acc_inv[i] = 0ull;
         }
         __syncthreads();
+    }
+    if (lane == 0 && expansions != 0) {
+        atomicAdd(&p.out.counters[kExpansions], expansions);
+        atomicAdd(&p.out.counters[kLaneExpansions], expansions);
     }
 }
 
