@@ -1,0 +1,380 @@
+"""Benchmark: all-sources APSP + Brandes throughput (GTEPS) on B200, batched form, with the reference CPU path beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ngx|reference]
+
+Workload (the batched single-graph configuration): a synthetic connectome with N = 100,000 vertices in the unit cube,
+out-degree Poisson(100) (about 1e7 arcs after merging repeated targets), spatial kernel exp(-d / 0.08), log-normal(0, 1)
+FP64 weights, generated from a fixed seed. One step = one batch of sources (a fixed seeded permutation of all
+vertices, consumed batch after batch) run through ngx_brandes: distances by batched delta-stepping, the fused APSP
+summaries (exact sums of d and 1/d, diameter, unreachable count, 1024-bin distance histogram, per-source outputs) and
+Brandes betweenness, in one persistent launch. GTEPS = traversed arcs (sum over sources of the out-degrees of the
+vertices they reach) / seconds.
+
+Timing: W untimed steps, then K steps between a barrier + synchronize on both sides; device time from CUDA events on
+the stream the library runs on (handed to it with ngx_graph_set_stream); max over ranks. The graph (320 MB of CSR and
+reverse CSR) and the per-CTA workspaces (GBs) are larger than L2, so no flush is needed between steps.
+e2e: the same metric through the C ABI from host buffers: every step creates the graph from the host CSR (H2D),
+runs, and copies the results (betweenness, per-source summaries, histogram) back (D2H); wall clock, synchronized.
+Under torchrun (N > 1) every rank runs its own disjoint batches (weak scaling); only the timing scalars are reduced.
+
+--impl reference: the reference's algorithm on the host cores. The reference's own build (oracle/_ref) reads int32
+weights only, so for this FP64-weight workload the CPU restatement of its Dijkstra and Brandes (oracle/ngx_oracle.c,
+bit-exact with the reference on integer weights) runs in one process per host core on disjoint sources.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {
+    "workload": "batched single graph: synthetic connectome N=100000, out-degree Poisson(100), kernel exp(-d/0.08), "
+                "log-normal(0,1) FP64 weights; APSP summaries + 1024-bin histogram + Brandes per source batch",
+    "n": 100000, "mean_degree": 100.0, "length_scale": 0.08, "weights": "lognormal(0,1)", "seed": 2,
+}
+HIST_BINS = 1024
+SLOTS_PER_WAVE = 296  # 148 SMs x 2 resident CTAs
+DEFAULT_SOURCES_PER_STEP = SLOTS_PER_WAVE * 32
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ngx", "reference"], default="ngx")
+    ap.add_argument("--sources-per-step", type=int, default=DEFAULT_SOURCES_PER_STEP)
+    ap.add_argument("--n", type=int, default=WORKLOAD["n"])
+    ap.add_argument("--degree", type=float, default=WORKLOAD["mean_degree"])
+    ap.add_argument("--delta", type=float, default=0.25)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_graph(n, degree):
+    from neurograph_b200 import synth
+
+    return synth.connectome(n, degree, WORKLOAD["length_scale"], weights="lognormal", mu=0.0, sigma=1.0, seed=WORKLOAD["seed"])
+
+
+def source_batches(n, per_step, count, rank, world):
+    perm = np.random.default_rng(12345).permutation(n)
+    out = []
+    for i in range(count):
+        start = ((i * world + rank) * per_step) % n
+        idx = (start + np.arange(per_step)) % n
+        out.append(np.ascontiguousarray(perm[idx], dtype=np.int64))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.file = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.proc = None
+        self.device_index = device_index
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                                          "-i", str(self.device_index)], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, sm_max, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                sm_max.append(float(r[2]))
+                power.append(float(r[3]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, r[5:9]):
+                if flag.strip().lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(sm_max), "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic_per_arc():
+    """DRAM bytes per traversed arc of the Brandes tile kernel, from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, "profiles", "tile_kernel_brandes_c2.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("dram_bytes_per_traversed_arc:"):
+                return float(line.split(":", 1)[1])
+    return None
+
+
+_WORKER = {}
+
+
+def cpu_worker_init(directory):
+    """Maps the CSR read-only (shared page cache across the worker processes)."""
+    sys.path.insert(0, ROOT)
+    import oracle
+
+    row_ptr = np.load(os.path.join(directory, "row_ptr.npy"), mmap_mode="r")
+    col = np.load(os.path.join(directory, "col.npy"), mmap_mode="r")
+    w = np.load(os.path.join(directory, "w.npy"), mmap_mode="r")
+    _WORKER["graph"] = oracle.Csr(int(row_ptr.size - 1), row_ptr, col, w)
+    _WORKER["oracle"] = oracle.Restatement()
+
+
+def cpu_worker(sources):
+    g, r = _WORKER["graph"], _WORKER["oracle"]
+    t0 = time.perf_counter()
+    a = r.apsp(g, sources=sources, bins=HIST_BINS, hist_max=64.0)
+    r.brandes(g, sources=sources)
+    return int(a["traversed_arcs"]), time.perf_counter() - t0
+
+
+def run_reference(args, rank, world):
+    """The reference arm: CPU restatement of the reference's Dijkstra + Brandes over all host cores."""
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    c = make_graph(args.n, args.degree)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    directory = tempfile.mkdtemp(prefix="ngx_ref_")
+    for name, arr in (("row_ptr", c.row_ptr), ("col", c.col), ("w", c.w)):
+        np.save(os.path.join(directory, f"{name}.npy"), arr)
+    batches = source_batches(c.n, cores, args.warmup + args.steps, 0, 1)
+    ctx = mp.get_context("spawn")
+    times, arcs = [], []
+    with ctx.Pool(cores, initializer=cpu_worker_init, initargs=(directory,)) as pool:
+        pool.map(cpu_worker, [np.zeros(0, np.int64)] * cores)  # start every worker and map the graph before timing
+        for i, batch in enumerate(batches):
+            t0 = time.perf_counter()
+            res = pool.map(cpu_worker, [batch[j:j + 1] for j in range(len(batch))], chunksize=1)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                times.append(dt)
+                arcs.append(sum(r[0] for r in res))
+    for name in ("row_ptr", "col", "w"):
+        os.unlink(os.path.join(directory, f"{name}.npy"))
+    os.rmdir(directory)
+    total = sum(times)
+    value = sum(arcs) / total / 1e9
+    line = {
+        "impl": "reference", "metric": "APSP+Brandes GTEPS (batched single graph)", "value": value, "unit": "GTEPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(WORKLOAD, sources_per_step=cores, parallelism=f"{cores} host processes x 1 thread"),
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": "port",
+                         "sample": f"{cores} sources per step (one per process), APSP summaries + histogram + Brandes, "
+                                   "CPU restatement of the reference Dijkstra/Brandes (the reference build reads int32 weights only)"},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_single_core(c, sources):
+    import oracle
+
+    g = oracle.Csr.from_arrays(c.n, c.row_ptr, c.col, c.w)
+    r = oracle.Restatement()
+    t0 = time.perf_counter()
+    a = r.apsp(g, sources=sources, bins=HIST_BINS, hist_max=64.0)
+    r.brandes(g, sources=sources)
+    dt = time.perf_counter() - t0
+    return {"value": a["traversed_arcs"] / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
+            "sample": f"{len(sources)} sources of the same graph, APSP summaries + histogram + Brandes, {dt:.1f} s, single thread; "
+                      "CPU restatement of the reference Dijkstra/Brandes (bit-exact with the reference on integer weights)"}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    import neurograph_b200 as ngx
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    t0 = time.perf_counter()
+    c = make_graph(args.n, args.degree)
+    log(f"[bench] graph n={c.n} m={c.m} generated in {time.perf_counter() - t0:.1f}s")
+    stream = torch.cuda.Stream()
+    g = ngx.Graph(c.n, c.row_ptr, c.col, c.w, device=local_rank)
+    g.set_stream(stream.cuda_stream)
+    batches = source_batches(c.n, args.sources_per_step, args.warmup + args.steps, rank, world)
+
+    # histogram bound: sampled eccentricity x 1.5 from the first warm-up step, fixed for the timed steps
+    hist_max = 0.0
+    launches = 0
+    for i in range(args.warmup):
+        bc, r = g.brandes(sources=batches[i], delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max, per_source=True)
+        hist_max = r.hist_max
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    arcs = 0
+    reached = 0
+    kernel_ms = 0.0
+    for i in range(args.warmup, args.warmup + args.steps):
+        bc, r = g.brandes(sources=batches[i], delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max, per_source=True)
+        arcs += r.traversed_arcs
+        reached += r.reached_pairs + len(batches[i])
+        kernel_ms += r.kernel_ms
+        launches += 1
+    ev1.record(stream)
+    barrier()
+    clock_info = clocks.stop()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    elapsed_max = max_over_ranks(elapsed)
+    arcs_total = sum_over_ranks(float(arcs))
+    value = arcs_total / elapsed_max / 1e9
+
+    # roofline of the dominant kernel (the Brandes tile kernel): algorithmic bytes per SURVEY 8(d) accounting:
+    # SSSP 20 B per traversed arc + 24 B per reached vertex, Brandes 56 B per arc + 32 B per vertex
+    alg_bytes = 76.0 * arcs + 56.0 * reached
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    traffic_per_arc = profiled_traffic_per_arc()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                "traffic": None if traffic_per_arc is None else traffic_per_arc * arcs / launches,
+                "algorithmic_bytes_per_launch": alg_bytes / launches,
+                "kernel": "tile_kernel<Brandes> (ngx_brandes)"}
+
+    # forms on the same graph: plain per-source GPU APSP vs batched APSP (one wave of sources each)
+    forms = {}
+    if rank == 0:
+        sample = batches[0][: SLOTS_PER_WAVE * 4]
+        rp = g.apsp(sources=sample, mode="plain", delta=0.1)
+        rb = g.apsp(sources=batches[0], delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max)
+        forms = {"plain_apsp_gteps": rp.gteps, "batched_apsp_gteps": rb.gteps, "batched_apsp_brandes_gteps": arcs / (kernel_ms / 1e3) / 1e9,
+                 "plain_sources": int(len(sample)), "batched_sources": int(len(batches[0]))}
+
+    # e2e through the C ABI from host buffers
+    e2e = None
+    if not args.no_e2e:
+        pinned = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in (("row_ptr", c.row_ptr), ("col", c.col), ("w", c.w))}
+        h2d = pinned["row_ptr"].nbytes + pinned["col"].nbytes + pinned["w"].nbytes + batches[0].nbytes
+        d2h = 0
+        barrier()
+        t1 = time.perf_counter()
+        e2e_arcs = 0
+        for i in range(args.warmup, args.warmup + args.steps):
+            with ngx.Graph(c.n, pinned["row_ptr"], pinned["col"], pinned["w"], device=local_rank) as ge:
+                bc, r = ge.brandes(sources=batches[i], delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max, per_source=True)
+            e2e_arcs += r.traversed_arcs
+            d2h = bc.nbytes + r.hist.nbytes + sum(a.nbytes for a in r.per_source.values())
+        barrier()
+        e2e_elapsed = max_over_ranks(time.perf_counter() - t1)
+        e2e = {"value": sum_over_ranks(float(e2e_arcs)) / e2e_elapsed / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "timing": "wall clock, synchronized, graph created from host CSR every step"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_single_core(c, batches[0][:2])
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": "APSP+Brandes GTEPS (batched single graph)", "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(WORKLOAD, n=c.n, arcs=c.m, sources_per_step=args.sources_per_step, delta=args.delta, hist_bins=HIST_BINS,
+                       hist_max=hist_max, parallelism=f"sources sharded over {world} GPU(s), no data-path collective",
+                       l2="graph (320 MB CSR + reverse CSR) and workspaces (GBs) exceed the 126 MB L2; no flush needed"),
+        "gpu_launches": launches,
+        "clocks": clock_info,
+        "roofline": roofline,
+        "forms": forms,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -124,6 +124,12 @@ NGX_API void ngx_graph_destroy(ngx_graph* graph);
 NGX_API int ngx_graph_size(const ngx_graph* graph, int64_t* n, int64_t* m);
 /* Asks an in-flight run on this graph to stop at its next phase boundary; the run returns NGX_ABORTED. */
 NGX_API int ngx_graph_request_abort(ngx_graph* graph);
+/*
+ * Runs the graph's work on `stream` (a cudaStream_t of the graph's device, owned by the caller, who keeps it alive
+ * while the graph uses it); NULL restores the graph's own stream. Lets a caller time or order the library's kernels
+ * with its own events.
+ */
+NGX_API int ngx_graph_set_stream(ngx_graph* graph, void* stream);
 /* Caps the device memory the graph's runs may use for workspaces (bytes; 0 = no cap beyond free memory). */
 NGX_API int ngx_graph_set_memory_budget(ngx_graph* graph, uint64_t bytes);
 

@@ -69,7 +69,7 @@ _LIB = None
 # Every symbol include/ngx_b200.h declares (checked by the CPU test suite against the built library).
 EXPORTED = [
     "ngx_status_string", "ngx_last_error", "ngx_version", "ngx_graph_create", "ngx_graph_destroy", "ngx_graph_size",
-    "ngx_graph_request_abort", "ngx_graph_set_memory_budget", "ngx_apsp", "ngx_sssp_rows", "ngx_brandes",
+    "ngx_graph_request_abort", "ngx_graph_set_stream", "ngx_graph_set_memory_budget", "ngx_apsp", "ngx_sssp_rows", "ngx_brandes",
     "ngx_apsp_grad",
 ]
 
@@ -90,6 +90,7 @@ def library() -> C.CDLL:
         lib.ngx_graph_size.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         lib.ngx_graph_request_abort.argtypes = [C.c_void_p]
         lib.ngx_graph_set_memory_budget.argtypes = [C.c_void_p, C.c_uint64]
+        lib.ngx_graph_set_stream.argtypes = [C.c_void_p, C.c_void_p]
         lib.ngx_apsp.argtypes = [C.c_void_p, C.POINTER(_Opts), C.POINTER(_Result)]
         lib.ngx_sssp_rows.argtypes = [C.c_void_p, C.POINTER(_Opts), C.c_void_p]
         if hasattr(lib, "ngx_brandes"):
@@ -167,6 +168,10 @@ class Graph:
 
     def request_abort(self) -> None:
         _check(library().ngx_graph_request_abort(self._handle))
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        """Issue the graph's work on a caller-owned cudaStream_t (e.g. torch.cuda.Stream().cuda_stream)."""
+        _check(library().ngx_graph_set_stream(self._handle, stream_handle))
 
     def set_memory_budget(self, nbytes: int) -> None:
         _check(library().ngx_graph_set_memory_budget(self._handle, int(nbytes)))

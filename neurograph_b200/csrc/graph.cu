@@ -83,8 +83,8 @@ void release(ngx_graph* g) {
     if (g->h_abort != nullptr) {
         cudaFreeHost(g->h_abort);
     }
-    if (g->stream != nullptr) {
-        cudaStreamDestroy(g->stream);
+    if (g->own_stream != nullptr) {
+        cudaStreamDestroy(g->own_stream);
     }
     delete g;
 }
@@ -196,12 +196,13 @@ int ngx_graph_create(const ngx_csr* csr, int device, ngx_graph** out) {
         return NGX_OK;
     };
 
-    if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess ||
+    if (cudaStreamCreateWithFlags(&g->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaHostAlloc(reinterpret_cast<void**>(&g->h_abort), sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
         cudaHostGetDevicePointer(reinterpret_cast<void**>(&g->d_abort), g->h_abort, 0) != cudaSuccess) {
         return finish(fail(NGX_CUDA_ERROR, "ngx_graph_create: stream or abort flag setup failed"));
     }
     *g->h_abort = 0;
+    g->stream = g->own_stream;
 
     const int64_t n = csr->n;
     // Host compaction: drop zero-weight arcs, keep the caller's arc index, precompute both metrics' lengths.
@@ -293,6 +294,16 @@ int ngx_graph_request_abort(ngx_graph* graph) {
         return fail(NGX_INVALID_ARGUMENT, "ngx_graph_request_abort: graph is NULL");
     }
     *reinterpret_cast<volatile int*>(graph->h_abort) = 1;
+    return NGX_OK;
+}
+
+int ngx_graph_set_stream(ngx_graph* graph, void* stream) {
+    if (graph == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_set_stream: graph is NULL");
+    }
+    NGX_CUDA_TRY(cudaSetDevice(graph->device));
+    NGX_CUDA_TRY(cudaStreamSynchronize(graph->stream));
+    graph->stream = stream != nullptr ? static_cast<cudaStream_t>(stream) : graph->own_stream;
     return NGX_OK;
 }
 

@@ -11,7 +11,8 @@
 struct ngx_graph {
     int device = 0;
     int sm_count = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;        // the stream all work of the graph is issued on
+    cudaStream_t own_stream = nullptr;    // created with the graph; `stream` points here unless the caller set one
 
     int64_t n = 0;
     int64_t m_user = 0;    // arcs in the caller's CSR (zero weights included)
