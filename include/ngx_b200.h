@@ -104,6 +104,8 @@ typedef struct {
     uint64_t phases;          /* delta-stepping phases (near iterations) summed over source tiles */
     uint64_t expansions;      /* vertex expansions: one pass over a vertex's out-arcs */
     uint64_t lane_expansions; /* (vertex, source) expansions; lane_expansions / expansions = sources per arc pass */
+    uint64_t dag_levels;      /* Kahn levels of the shortest-path DAGs summed over source tiles (Brandes / adjoint) */
+    uint64_t phase_cycles[5]; /* SM cycles summed over CTAs: distances, DAG counts, sigma, delta, summaries */
     /* optional outputs */
     uint64_t* hist;           /* hist_bins entries */
     double* src_sum;          /* per source: exactly rounded sum of distances */

@@ -39,7 +39,7 @@ int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_res
     unsigned long long* block = nullptr;
     NGX_CUDA_TRY(cudaMallocAsync(&block, words * 8, g->stream));
     NGX_CUDA_TRY(cudaMemsetAsync(block, 0, words * 8, g->stream));
-    extra.levels = block;
+    extra.sigma_inexact = reinterpret_cast<int*>(block);
     if (bc_words != 0) {
         extra.bc = block + 1;
     }
@@ -50,6 +50,24 @@ int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_res
     ngx_apsp_result scratch{};
     ngx_apsp_result* r = result != nullptr ? result : &scratch;
     int rc = run_apsp(g, &o, r, nullptr, tile_mode, &extra);
+    if (rc == NGX_OK) {
+        // sigma was pushed with atomics; if any path count reached 2^53 the sums may depend on the order of the
+        // atomics, so rerun with the order-defined pull form
+        int inexact = 0;
+        cudaError_t err = cudaMemcpyAsync(&inexact, extra.sigma_inexact, sizeof(int), cudaMemcpyDeviceToHost, g->stream);
+        if (err == cudaSuccess) {
+            err = cudaStreamSynchronize(g->stream);
+        }
+        if (err != cudaSuccess) {
+            rc = cuda_fail(err, "reading the sigma exactness flag");
+        } else if (inexact != 0) {
+            const double first_ms = r->kernel_ms;
+            extra.sigma_pull = 1;
+            NGX_CUDA_TRY(cudaMemsetAsync(block, 0, words * 8, g->stream));
+            rc = run_apsp(g, &o, r, nullptr, tile_mode, &extra);
+            r->kernel_ms += first_ms;
+        }
+    }
     if (rc == NGX_OK) {
         host_bc.resize(bc_words);
         host_cpl.resize(grad_words);

@@ -39,7 +39,9 @@ struct BrandesParams {
     unsigned long long* bc;         // 2 * n fixed point (Brandes), or nullptr
     unsigned long long* grad_cpl;   // 2 * m_user fixed point (adjoint), or nullptr
     unsigned long long* grad_eff;   // 2 * m_user fixed point (adjoint), or nullptr
-    unsigned long long* levels;     // total levels over all tiles (statistics)
+    unsigned long long* levels;     // unused (levels are counted in the run counters)
+    int* sigma_inexact;             // set when a pushed sigma sum reaches 2^53 (the host then reruns in pull form)
+    int sigma_pull;                 // 1: pull form for sigma
 };
 
 inline size_t brandes_slot_bytes(int64_t n, bool adjoint) {
@@ -98,82 +100,158 @@ __device__ __forceinline__ void brandes_count(const DeviceCsr& rg, int64_t n, in
     }
 }
 
-// Processes one level-L entry v of the sigma pass: pull sigma (L > 0), then release the DAG successors.
+// Pair-parallel walk over the deg x k (arc, ready source) pairs of one vertex, as in the SSSP expansion: pair
+// p = 32 i + lane takes arc p / k and the (p % k)-th ready source. Sums per source are gathered in arc order: in each
+// iteration the lanes holding rank r's pairs are l0, l0 + k, ... (increasing arcs), and lane r adds them in that order,
+// so every per-source sum runs over the arcs in CSR order, the same order for every run.
+struct PairWalk {
+    int k;         // ready sources
+    int a;         // this lane's arc (relative to the row)
+    int r;         // this lane's rank
+    int step_a;
+    int step_r;
+    __device__ __forceinline__ PairWalk(int k_, int lane) : k(k_) {
+        a = lane / k;
+        r = lane - a * k;
+        step_a = 32 / k;
+        step_r = 32 - step_a * k;
+    }
+    __device__ __forceinline__ void advance() {
+        a += step_a;
+        r += step_r;
+        if (r >= k) {
+            r -= k;
+            a += 1;
+        }
+    }
+};
+
+// Lane r (< k) receives the sum, in lane order, of `value` over the lanes whose pair has rank r in this iteration;
+// `first_rank` is the rank of lane 0's pair.
+__device__ __forceinline__ double gather_rank_sum(double value, int k, int first_rank, int lane) {
+    const int l0 = (lane - first_rank + 32 * k) % k;  // first lane whose rank equals this lane's index
+    const int rounds = (32 + k - 1) / k;
+    double sum = 0.0;
+    for (int q = 0; q < rounds; ++q) {
+        const int from = l0 + q * k;
+        const double t = __shfl_sync(0xFFFFFFFFu, value, from < 32 ? from : 0);
+        if (from < 32) {
+            sum += t;
+        }
+    }
+    return sum;
+}
+
+// sigma values are path counts: integers, summed exactly in FP64 (in any order) while below 2^53.
+constexpr double kSigmaExact = 9007199254740992.0;
+
+// Processes one level-L entry v of the sigma pass, then releases the DAG successors.
+// kPull: sigma[v] = sum over DAG in-arcs of sigma[u], gathered in reverse-CSR order (the order-defined form).
+// !kPull: sigma[v] is final on entry (pushed by its predecessors); v adds sigma[v] into each DAG successor with an
+//         atomic add. While every sum stays below 2^53 these integer sums are exact, so the result equals the pull
+//         form's bit for bit whatever the order; a sum reaching 2^53 raises *inexact and the host reruns in pull form.
+template <bool kPull, int kUnroll>
 __device__ __forceinline__ void brandes_sigma_vertex(const DeviceCsr& g, const DeviceCsr& rg, int v, uint32_t level, int nsrc, int lane,
                                                      const unsigned long long* dist, double* sigma, uint32_t* cnt, uint32_t* lvl, uint32_t* stamp,
-                                                     unsigned level_stamp, int32_t* next_list, int* next_len) {
-    const int64_t vrow = static_cast<int64_t>(v) * kTile + lane;
-    const bool ready = lane < nsrc && __ldcg(&lvl[vrow]) == level;
-    if (__ballot_sync(0xFFFFFFFFu, ready) == 0u) {
+                                                     unsigned level_stamp, int32_t* next_list, int* next_len, int* inexact) {
+    const int64_t vbase = static_cast<int64_t>(v) * kTile;
+    const bool ready = lane < nsrc && __ldcg(&lvl[vbase + lane]) == level;
+    const unsigned rmask = __ballot_sync(0xFFFFFFFFu, ready);
+    if (rmask == 0u) {
         return;
     }
-    const unsigned long long dv = __ldcg(&dist[vrow]);
-    if (level > 0) {
-        double sig = 0.0;
-        const int64_t beg = __ldg(&rg.row_ptr[v]);
-        const int64_t end = __ldg(&rg.row_ptr[v + 1]);
-        for (int64_t e0 = beg; e0 < end; e0 += 32) {
-            const int cntr = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
-            Arc a{ 0, 0, 0.0 };
-            if (lane < cntr) {
-                a = rg.arcs[e0 + lane];
-            }
-            for (int j = 0; j < cntr; j += 4) {
-                unsigned long long du[4];
-                int src[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int jj = j + u < cntr ? j + u : 0;
-                    src[u] = __shfl_sync(0xFFFFFFFFu, a.col, jj);
-                    du[u] = (ready && j + u < cntr) ? __ldcg(&dist[static_cast<int64_t>(src[u]) * kTile + lane]) : kInfBits;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const double len = __shfl_sync(0xFFFFFFFFu, a.len, j + u < cntr ? j + u : 0);
-                    if (du[u] != kInfBits && on_dag(du[u], len, dv)) {
-                        sig += __ldcg(&sigma[static_cast<int64_t>(src[u]) * kTile + lane]);
+    const int k = __popc(rmask);
+    const int rank_src = lane < k ? static_cast<int>(__fns(rmask, 0, lane + 1)) : 0;
+    const unsigned long long rank_dv = __ldcg(&dist[vbase + rank_src]);
+    double rank_sv = 0.0;
+    if constexpr (kPull) {
+        if (level > 0) {
+            const int64_t beg = __ldg(&rg.row_ptr[v]);
+            const int deg = static_cast<int>(__ldg(&rg.row_ptr[v + 1]) - beg);
+            const Arc* arcs = rg.arcs + beg;
+            PairWalk w(k, lane);
+            double acc = 0.0;
+            const int64_t total = static_cast<int64_t>(deg) * k;
+            for (int64_t p0 = 0; p0 < total; p0 += 32) {
+                const int s = __shfl_sync(0xFFFFFFFFu, rank_src, w.r);
+                const unsigned long long dvs = __shfl_sync(0xFFFFFFFFu, rank_dv, w.r);
+                double contrib = 0.0;
+                if (w.a < deg) {
+                    const Arc arc = arcs[w.a];
+                    const int64_t urow = static_cast<int64_t>(arc.col) * kTile + s;
+                    const unsigned long long du = __ldcg(&dist[urow]);
+                    if (du != kInfBits && on_dag(du, arc.len, dvs)) {
+                        contrib = __ldcg(&sigma[urow]);
                     }
                 }
+                acc += gather_rank_sum(contrib, k, static_cast<int>(p0 % k), lane);
+                w.advance();
             }
+            if (lane < k) {
+                sigma[vbase + rank_src] = acc;
+            }
+            rank_sv = acc;
+        } else {
+            rank_sv = __ldcg(&sigma[vbase + rank_src]);
         }
-        if (ready) {
-            sigma[vrow] = sig;
-        }
+    } else {
+        rank_sv = __ldcg(&sigma[vbase + rank_src]);
     }
     const int64_t beg = __ldg(&g.row_ptr[v]);
-    const int64_t end = __ldg(&g.row_ptr[v + 1]);
-    for (int64_t e0 = beg; e0 < end; e0 += 32) {
-        const int cntr = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
-        Arc a{ 0, 0, 0.0 };
-        if (lane < cntr) {
-            a = g.arcs[e0 + lane];
-        }
-        for (int j = 0; j < cntr; j += 4) {
-            unsigned long long dx[4];
-            int x[4];
-            double len[4];
+    const int deg = static_cast<int>(__ldg(&g.row_ptr[v + 1]) - beg);
+    const Arc* arcs = g.arcs + beg;
+    PairWalk w(k, lane);
+    const int64_t total = static_cast<int64_t>(deg) * k;
+    for (int64_t p0 = 0; p0 < total; p0 += 32 * kUnroll) {
+        int x[kUnroll];
+        int s[kUnroll];
+        double sv[kUnroll];
+        unsigned long long dvs[kUnroll], dx[kUnroll];
+        double len[kUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int jj = j + u < cntr ? j + u : 0;
-                x[u] = __shfl_sync(0xFFFFFFFFu, a.col, jj);
-                len[u] = __shfl_sync(0xFFFFFFFFu, a.len, jj);
-                dx[u] = (ready && j + u < cntr) ? __ldcg(&dist[static_cast<int64_t>(x[u]) * kTile + lane]) : kInfBits;
+        for (int u = 0; u < kUnroll; ++u) {
+            s[u] = __shfl_sync(0xFFFFFFFFu, rank_src, w.r);
+            dvs[u] = __shfl_sync(0xFFFFFFFFu, rank_dv, w.r);
+            sv[u] = __shfl_sync(0xFFFFFFFFu, rank_sv, w.r);
+            x[u] = 0;
+            len[u] = 0.0;
+            dx[u] = kInfBits;
+            if (w.a < deg) {
+                const Arc arc = arcs[w.a];
+                x[u] = arc.col;
+                len[u] = arc.len;
+                dx[u] = __ldcg(&dist[static_cast<int64_t>(x[u]) * kTile + s[u]]);
             }
+            w.advance();
+        }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                bool released = false;
-                if (dx[u] != kInfBits && on_dag(dv, len[u], dx[u])) {
-                    const int64_t xrow = static_cast<int64_t>(x[u]) * kTile + lane;
-                    if (atomicSub(&cnt[xrow], 1u) == 1u) {
-                        lvl[xrow] = level + 1u;
-                        released = true;
+        for (int u = 0; u < kUnroll; ++u) {
+            bool released = false;
+            if (dx[u] != kInfBits && on_dag(dvs[u], len[u], dx[u])) {
+                const int64_t xrow = static_cast<int64_t>(x[u]) * kTile + s[u];
+                if constexpr (!kPull) {
+                    const double before = atomicAdd(&sigma[xrow], sv[u]);
+                    if (before + sv[u] >= kSigmaExact) {
+                        atomicExch(inexact, 1);
                     }
                 }
-                const unsigned rmask = __ballot_sync(0xFFFFFFFFu, released);
-                if (rmask != 0u && lane == 0) {
-                    if (atomicExch(&stamp[x[u]], level_stamp) != level_stamp) {
-                        next_list[atomicAdd(next_len, 1)] = x[u];
-                    }
+                if (atomicSub(&cnt[xrow], 1u) == 1u) {
+                    lvl[xrow] = level + 1u;
+                    released = atomicExch(&stamp[x[u]], level_stamp) != level_stamp;
+                }
+            }
+            const unsigned pmask = __ballot_sync(0xFFFFFFFFu, released);
+            if (pmask != 0u) {
+                const int leader = __ffs(pmask) - 1;
+                int base = 0;
+                if (lane == leader) {
+                    base = atomicAdd(next_len, __popc(pmask));
+                }
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (released) {
+                    unsigned lt;
+                    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+                    next_list[base + __popc(pmask & lt)] = x[u];
                 }
             }
         }
@@ -181,73 +259,78 @@ __device__ __forceinline__ void brandes_sigma_vertex(const DeviceCsr& g, const D
 }
 
 // Processes one level-L entry v of the delta pass (pull over DAG out-arcs), emitting per-arc adjoint terms.
-template <int kMode>
+template <int kMode, int kUnroll>
 __device__ __forceinline__ void brandes_delta_vertex(const DeviceCsr& g, int v, uint32_t level, int nsrc, int lane, const unsigned long long* dist,
                                                      const double* sigma, double* delta, double* delta_g, const uint32_t* lvl,
                                                      unsigned long long* grad_cpl, unsigned long long* grad_eff) {
-    const int64_t vrow = static_cast<int64_t>(v) * kTile + lane;
-    const bool ready = lane < nsrc && __ldcg(&lvl[vrow]) == level;
-    if (__ballot_sync(0xFFFFFFFFu, ready) == 0u) {
+    const int64_t vbase = static_cast<int64_t>(v) * kTile;
+    const bool ready = lane < nsrc && __ldcg(&lvl[vbase + lane]) == level;
+    const unsigned rmask = __ballot_sync(0xFFFFFFFFu, ready);
+    if (rmask == 0u) {
         return;
     }
-    const unsigned long long dv = __ldcg(&dist[vrow]);
-    const double sv = ready ? __ldcg(&sigma[vrow]) : 0.0;
+    const int k = __popc(rmask);
+    const int rank_src = lane < k ? static_cast<int>(__fns(rmask, 0, lane + 1)) : 0;
+    const unsigned long long rank_dv = __ldcg(&dist[vbase + rank_src]);
+    const double rank_sv = __ldcg(&sigma[vbase + rank_src]);
+    const int64_t beg = __ldg(&g.row_ptr[v]);
+    const int deg = static_cast<int>(__ldg(&g.row_ptr[v + 1]) - beg);
+    const Arc* arcs = g.arcs + beg;
+    PairWalk w(k, lane);
     double acc = 0.0;
     double acc_g = 0.0;
-    const int64_t beg = __ldg(&g.row_ptr[v]);
-    const int64_t end = __ldg(&g.row_ptr[v + 1]);
-    for (int64_t e0 = beg; e0 < end; e0 += 32) {
-        const int cntr = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
-        Arc a{ 0, 0, 0.0 };
-        if (lane < cntr) {
-            a = g.arcs[e0 + lane];
-        }
-        for (int j = 0; j < cntr; j += 4) {
-            unsigned long long dx[4];
-            int x[4];
-            double len[4];
+    const int64_t total = static_cast<int64_t>(deg) * k;
+    for (int64_t p0 = 0; p0 < total; p0 += 32 * kUnroll) {
+        int s[kUnroll];
+        unsigned long long dvs[kUnroll], dx[kUnroll];
+        double sv[kUnroll], len[kUnroll];
+        int x[kUnroll], id[kUnroll];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int jj = j + u < cntr ? j + u : 0;
-                x[u] = __shfl_sync(0xFFFFFFFFu, a.col, jj);
-                len[u] = __shfl_sync(0xFFFFFFFFu, a.len, jj);
-                dx[u] = (ready && j + u < cntr) ? __ldcg(&dist[static_cast<int64_t>(x[u]) * kTile + lane]) : kInfBits;
+        for (int u = 0; u < kUnroll; ++u) {
+            s[u] = __shfl_sync(0xFFFFFFFFu, rank_src, w.r);
+            dvs[u] = __shfl_sync(0xFFFFFFFFu, rank_dv, w.r);
+            sv[u] = __shfl_sync(0xFFFFFFFFu, rank_sv, w.r);
+            x[u] = 0;
+            id[u] = 0;
+            len[u] = 0.0;
+            dx[u] = kInfBits;
+            if (w.a < deg) {
+                const Arc arc = arcs[w.a];
+                x[u] = arc.col;
+                id[u] = arc.id;
+                len[u] = arc.len;
+                dx[u] = __ldcg(&dist[static_cast<int64_t>(x[u]) * kTile + s[u]]);
             }
+            w.advance();
+        }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const bool dag = dx[u] != kInfBits && on_dag(dv, len[u], dx[u]);
-                const int64_t xrow = static_cast<int64_t>(x[u]) * kTile + lane;
+        for (int u = 0; u < kUnroll; ++u) {
+            double c = 0.0, cg = 0.0;
+            if (dx[u] != kInfBits && on_dag(dvs[u], len[u], dx[u])) {
+                const int64_t xrow = static_cast<int64_t>(x[u]) * kTile + s[u];
                 if constexpr (kMode == kModeBrandes) {
-                    if (dag) {
-                        acc += sv * ((1.0 + __ldcg(&delta[xrow])) / __ldcg(&sigma[xrow]));
-                    }
+                    c = sv[u] * ((1.0 + __ldcg(&delta[xrow])) / __ldcg(&sigma[xrow]));
                 } else {
-                    double c = 0.0, cg = 0.0;
-                    if (dag) {
-                        const double share = sv / __ldcg(&sigma[xrow]);
-                        const double inv = 1.0 / __longlong_as_double(static_cast<long long>(dx[u]));
-                        c = share * (1.0 + __ldcg(&delta[xrow]));
-                        cg = share * (inv * inv + __ldcg(&delta_g[xrow]));
-                        acc += c;
-                        acc_g += cg;
-                    }
-                    if (__ballot_sync(0xFFFFFFFFu, dag) != 0u) {
-                        const double sc = warp_sum(c);
-                        const double sg = warp_sum(cg);
-                        const int id = __shfl_sync(0xFFFFFFFFu, a.id, j + u < cntr ? j + u : 0);
-                        if (lane == 0) {
-                            fixed_add(&grad_cpl[2 * static_cast<int64_t>(id)], sc);
-                            fixed_add(&grad_eff[2 * static_cast<int64_t>(id)], sg);
-                        }
-                    }
+                    const double share = sv[u] / __ldcg(&sigma[xrow]);
+                    const double inv = 1.0 / __longlong_as_double(static_cast<long long>(dx[u]));
+                    c = share * (1.0 + __ldcg(&delta[xrow]));
+                    cg = share * (inv * inv + __ldcg(&delta_g[xrow]));
+                    // per (arc, source) term into the arc's 128-bit fixed-point sum: order-free, deterministic
+                    fixed_add(&grad_cpl[2 * static_cast<int64_t>(id[u])], c);
+                    fixed_add(&grad_eff[2 * static_cast<int64_t>(id[u])], cg);
                 }
+            }
+            const int first_rank = static_cast<int>((p0 + 32 * u) % k);
+            acc += gather_rank_sum(c, k, first_rank, lane);
+            if constexpr (kMode == kModeGrad) {
+                acc_g += gather_rank_sum(cg, k, first_rank, lane);
             }
         }
     }
-    if (ready) {
-        delta[vrow] = acc;
+    if (lane < k) {
+        delta[vbase + rank_src] = acc;
         if constexpr (kMode == kModeGrad) {
-            delta_g[vrow] = acc_g;
+            delta_g[vbase + rank_src] = acc_g;
         }
     }
 }

@@ -32,7 +32,9 @@ struct DagOutputs {
     unsigned long long* bc = nullptr;        // 2 * n
     unsigned long long* grad_cpl = nullptr;  // 2 * m_user
     unsigned long long* grad_eff = nullptr;  // 2 * m_user
-    unsigned long long* levels = nullptr;    // 1
+    unsigned long long* levels = nullptr;    // unused
+    int* sigma_inexact = nullptr;            // device flag: a pushed sigma sum reached 2^53
+    int sigma_pull = 0;                      // run the sigma pass in pull form
 };
 
 int check_opts(const ngx_graph* g, const ngx_apsp_opts* opts);

@@ -216,6 +216,8 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const i
             bp.grad_cpl = extra->grad_cpl;
             bp.grad_eff = extra->grad_eff;
             bp.levels = extra->levels;
+            bp.sigma_inexact = extra->sigma_inexact;
+            bp.sigma_pull = extra->sigma_pull;
         }
     }
     p.out.acc_sum = o.acc;
@@ -318,6 +320,10 @@ int collect(ngx_graph* g, const RunOutputs& o, int64_t num_sources, int64_t hist
     r->phases = counters[kIterations];
     r->expansions = counters[kExpansions];
     r->lane_expansions = counters[kLaneExpansions];
+    r->dag_levels = counters[kDagLevels];
+    for (int i = 0; i < 5; ++i) {
+        r->phase_cycles[i] = counters[kCyclesSssp + i];
+    }
     r->cpl = r->sum_distances / static_cast<double>(r->reached_pairs);
     r->efficiency = r->sum_inverse / static_cast<double>(r->reached_pairs);
     const size_t s = static_cast<size_t>(num_sources);
@@ -341,7 +347,10 @@ void clear_result_totals(ngx_apsp_result* r) {
     r->hist_max = 0.0;
     r->cpl = r->efficiency = 0.0;
     r->kernel_ms = 0.0;
-    r->phases = r->expansions = r->lane_expansions = 0;
+    r->phases = r->expansions = r->lane_expansions = r->dag_levels = 0;
+    for (int i = 0; i < 5; ++i) {
+        r->phase_cycles[i] = 0;
+    }
 }
 
 int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, double* rows, int tile_mode, DagOutputs* extra) {

@@ -62,7 +62,13 @@ enum Counter : int {
     kIterations = 5,   // near iterations (phases) over all tiles
     kExpansions = 6,   // vertex expansions (one warp pass over a vertex's arcs)
     kLaneExpansions = 7,  // (vertex, source) expansions; kLaneExpansions / kExpansions = sources sharing one arc pass
-    kCounterCount = 8
+    kCyclesSssp = 8,      // SM cycles spent per phase, summed over CTAs (thread 0 between barriers)
+    kCyclesCount = 9,
+    kCyclesSigma = 10,
+    kCyclesDelta = 11,
+    kCyclesEpilogue = 12,
+    kDagLevels = 13,      // Kahn levels of the shortest-path DAG, summed over tiles (Brandes / adjoint)
+    kCounterCount = 16
 };
 
 struct SsspParams {
@@ -324,6 +330,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         __syncthreads();
 
         // ------------------------------------------------------------ delta-stepping over the tile
+        long long t_phase = clock64();
         for (;;) {
             for (;;) {
                 const int cur = s.cur;
@@ -431,9 +438,20 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             break;
         }
 
+        if (tid == 0) {
+            const long long now = clock64();
+            atomicAdd(&p.out.counters[kCyclesSssp], static_cast<unsigned long long>(now - t_phase));
+            t_phase = now;
+        }
         if constexpr (kMode != kModeApsp) {
             // ------------------------------------------------------------ shortest-path DAG: counts, sigma, delta
             brandes_count(b.rg, n, nsrc, s_src, dist, cnt, lane, warp, nwarps);
+            __syncthreads();
+            if (tid == 0) {
+                const long long now = clock64();
+                atomicAdd(&p.out.counters[kCyclesCount], static_cast<unsigned long long>(now - t_phase));
+                t_phase = now;
+            }
             if (tid == 0) {
                 s.stamp += 1u;
                 s.level = 0u;
@@ -463,9 +481,16 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 }
                 const unsigned level = s.level;
                 const unsigned level_stamp = s.stamp + 1u;
-                for (int i = warp; i < len; i += nwarps) {
-                    brandes_sigma_vertex(p.g, b.rg, __ldcg(&list[start + i]), level, nsrc, lane, dist, sigma, cnt, lvl, stamp, level_stamp,
-                                         list + start + len, &s.next_len);
+                if (b.sigma_pull != 0) {
+                    for (int i = warp; i < len; i += nwarps) {
+                        brandes_sigma_vertex<true, 2>(p.g, b.rg, __ldcg(&list[start + i]), level, nsrc, lane, dist, sigma, cnt, lvl, stamp, level_stamp,
+                                                      list + start + len, &s.next_len, b.sigma_inexact);
+                    }
+                } else {
+                    for (int i = warp; i < len; i += nwarps) {
+                        brandes_sigma_vertex<false, 2>(p.g, b.rg, __ldcg(&list[start + i]), level, nsrc, lane, dist, sigma, cnt, lvl, stamp, level_stamp,
+                                                       list + start + len, &s.next_len, b.sigma_inexact);
+                    }
                 }
                 __syncthreads();
                 if (tid == 0) {
@@ -478,6 +503,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 }
                 __syncthreads();
             }
+            if (tid == 0) {
+                const long long now = clock64();
+                atomicAdd(&p.out.counters[kCyclesSigma], static_cast<unsigned long long>(now - t_phase));
+                t_phase = now;
+            }
             // s.level is one past the last non-empty level; loff[s.level] is the end of the lists
             const int levels = static_cast<int>(s.level);
             const int lowest = kMode == kModeGrad ? 0 : 1;
@@ -485,13 +515,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 const int start = __ldcg(&loff[level]);
                 const int end = __ldcg(&loff[level + 1]);
                 for (int i = start + warp; i < end; i += nwarps) {
-                    brandes_delta_vertex<kMode>(p.g, __ldcg(&list[i]), static_cast<unsigned>(level), nsrc, lane, dist, sigma, delta, delta_g, lvl,
-                                                b.grad_cpl, b.grad_eff);
+                    brandes_delta_vertex<kMode, 2>(p.g, __ldcg(&list[i]), static_cast<unsigned>(level), nsrc, lane, dist, sigma, delta, delta_g, lvl,
+                                                   b.grad_cpl, b.grad_eff);
                 }
                 __syncthreads();
             }
-            if (tid == 0 && b.levels != nullptr) {
-                atomicAdd(b.levels, static_cast<unsigned long long>(levels));
+            if (tid == 0) {
+                atomicAdd(&p.out.counters[kDagLevels], static_cast<unsigned long long>(levels));
+            }
+            if (tid == 0) {
+                const long long now = clock64();
+                atomicAdd(&p.out.counters[kCyclesDelta], static_cast<unsigned long long>(now - t_phase));
+                t_phase = now;
             }
         }
 
@@ -601,6 +636,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             smem[i] = 0ull;
         }
         __syncthreads();
+        if (tid == 0) {
+            atomicAdd(&p.out.counters[kCyclesEpilogue], static_cast<unsigned long long>(clock64() - t_phase));
+        }
     }
     if (lane == 0 && expansions != 0) {
         atomicAdd(&p.out.counters[kExpansions], expansions);

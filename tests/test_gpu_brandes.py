@@ -86,3 +86,27 @@ def test_inverse_metric_is_rejected():
         import ctypes as C
 
         assert ngx.library().ngx_brandes(gg._handle, C.byref(opts), bc.ctypes.data, C.byref(r)) == 6
+
+
+def test_path_counts_beyond_2_53_use_the_pull_form(restatement):
+    """A chain of 70 diamonds has 2^70 shortest paths: the atomic sigma push can no longer be exact, so the run must
+    fall back to the order-defined pull form and still agree with the oracle."""
+    diamonds = 70
+    n = 3 * diamonds + 1
+    src, dst = [], []
+    for i in range(diamonds):
+        hub, a, b, nxt = 3 * i, 3 * i + 1, 3 * i + 2, 3 * i + 3
+        src += [hub, hub, a, b]
+        dst += [a, b, nxt, nxt]
+    order = np.lexsort((dst, src))
+    src, dst = np.array(src)[order], np.array(dst)[order]
+    row_ptr = np.zeros(n + 1, np.int64)
+    np.add.at(row_ptr, src + 1, 1)
+    row_ptr = np.cumsum(row_ptr)
+    w = np.ones(src.size)
+    csr = oracle.Csr.from_arrays(n, row_ptr, dst, w)
+    with ngx.Graph(n, row_ptr, dst, w) as gg:
+        bc, _ = gg.brandes()
+        bc2, _ = gg.brandes()
+    assert_bc_close(bc, restatement.brandes(csr), "diamonds")
+    assert np.array_equal(bc, bc2)
