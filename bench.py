@@ -63,8 +63,11 @@ def parse():
     ap.add_argument("--n", type=int, default=WORKLOAD["n"])
     ap.add_argument("--degree", type=float, default=WORKLOAD["mean_degree"])
     ap.add_argument("--delta", type=float, default=0.25)
+    ap.add_argument("--mode", choices=["brandes", "apsp", "grad", "plain"], default="brandes",
+                    help="what one step runs: APSP+Brandes (the headline), APSP only, APSP+gradient, or the plain per-source form")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the plain/batched APSP comparison runs")
     return ap.parse_args()
 
 
@@ -282,12 +285,25 @@ def main():
     g.set_stream(stream.cuda_stream)
     batches = source_batches(c.n, args.sources_per_step, args.warmup + args.steps, rank, world)
 
+    def step(graph, sources, hist_max):
+        """One step of the selected mode; returns (result, host outputs)."""
+        if args.mode == "brandes":
+            bc, r = graph.brandes(sources=sources, delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max, per_source=True)
+            return r, [bc]
+        if args.mode == "grad":
+            dcpl, deff, r = graph.apsp_grad(sources=sources, delta=args.delta)
+            return r, [dcpl, deff]
+        mode = "plain" if args.mode == "plain" else "batched"
+        r = graph.apsp(sources=sources, mode=mode, delta=args.delta if mode == "batched" else 0.1, hist_bins=HIST_BINS, hist_max=hist_max,
+                       per_source=True)
+        return r, []
+
     # histogram bound: sampled eccentricity x 1.5 from the first warm-up step, fixed for the timed steps
     hist_max = 0.0
     launches = 0
     for i in range(args.warmup):
-        bc, r = g.brandes(sources=batches[i], delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max, per_source=True)
-        hist_max = r.hist_max
+        r, _ = step(g, batches[i], hist_max)
+        hist_max = r.hist_max if r.hist_max > 0 else hist_max
     clocks = ClockSampler(local_rank)
     clocks.start()
     barrier()
@@ -297,7 +313,7 @@ def main():
     reached = 0
     kernel_ms = 0.0
     for i in range(args.warmup, args.warmup + args.steps):
-        bc, r = g.brandes(sources=batches[i], delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max, per_source=True)
+        r, _ = step(g, batches[i], hist_max)
         arcs += r.traversed_arcs
         reached += r.reached_pairs + len(batches[i])
         kernel_ms += r.kernel_ms
@@ -312,7 +328,8 @@ def main():
 
     # roofline of the dominant kernel (the Brandes tile kernel): algorithmic bytes per SURVEY 8(d) accounting:
     # SSSP 20 B per traversed arc + 24 B per reached vertex, Brandes 56 B per arc + 32 B per vertex
-    alg_bytes = 76.0 * arcs + 56.0 * reached
+    per_arc, per_vertex = {"brandes": (76.0, 56.0), "grad": (104.0, 80.0), "apsp": (20.0, 24.0), "plain": (20.0, 24.0)}[args.mode]
+    alg_bytes = per_arc * arcs + per_vertex * reached
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
     traffic_per_arc = profiled_traffic_per_arc()
@@ -320,11 +337,12 @@ def main():
                 "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6.65 TB/s",
                 "traffic": None if traffic_per_arc is None else traffic_per_arc * arcs / launches,
                 "algorithmic_bytes_per_launch": alg_bytes / launches,
-                "kernel": "tile_kernel<Brandes> (ngx_brandes)"}
+                "kernel": {"brandes": "tile_kernel<Brandes> (ngx_brandes)", "grad": "tile_kernel<Grad> (ngx_apsp_grad)",
+                           "apsp": "tile_kernel<Apsp> (ngx_apsp)", "plain": "sssp_plain_kernel (ngx_apsp, plain form)"}[args.mode]}
 
     # forms on the same graph: plain per-source GPU APSP vs batched APSP (one wave of sources each)
     forms = {}
-    if rank == 0:
+    if rank == 0 and not args.no_forms:
         sample = batches[0][: SLOTS_PER_WAVE * 4]
         rp = g.apsp(sources=sample, mode="plain", delta=0.1)
         rb = g.apsp(sources=batches[0], delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max)
@@ -342,9 +360,10 @@ def main():
         e2e_arcs = 0
         for i in range(args.warmup, args.warmup + args.steps):
             with ngx.Graph(c.n, pinned["row_ptr"], pinned["col"], pinned["w"], device=local_rank) as ge:
-                bc, r = ge.brandes(sources=batches[i], delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max, per_source=True)
+                r, outs = step(ge, batches[i], hist_max)
             e2e_arcs += r.traversed_arcs
-            d2h = bc.nbytes + r.hist.nbytes + sum(a.nbytes for a in r.per_source.values())
+            d2h = sum(a.nbytes for a in outs) + (r.hist.nbytes if r.hist is not None else 0) + \
+                sum(a.nbytes for a in (r.per_source or {}).values())
         barrier()
         e2e_elapsed = max_over_ranks(time.perf_counter() - t1)
         e2e = {"value": sum_over_ranks(float(e2e_arcs)) / e2e_elapsed / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": int(h2d),
@@ -359,11 +378,13 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
+    metric = {"brandes": "APSP+Brandes GTEPS (batched single graph)", "apsp": "APSP GTEPS (batched single graph)",
+              "grad": "APSP+gradient GTEPS (batched single graph)", "plain": "APSP GTEPS (plain per-source form)"}[args.mode]
     line = {
-        "metric": "APSP+Brandes GTEPS (batched single graph)", "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+        "metric": metric, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(WORKLOAD, n=c.n, arcs=c.m, sources_per_step=args.sources_per_step, delta=args.delta, hist_bins=HIST_BINS,
+        "config": dict(WORKLOAD, n=c.n, arcs=c.m, mode=args.mode, sources_per_step=args.sources_per_step, delta=args.delta, hist_bins=HIST_BINS,
                        hist_max=hist_max, parallelism=f"sources sharded over {world} GPU(s), no data-path collective",
                        l2="graph (320 MB CSR + reverse CSR) and workspaces (GBs) exceed the 126 MB L2; no flush needed"),
         "gpu_launches": launches,

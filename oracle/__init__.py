@@ -27,6 +27,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATEMENT_SO = os.path.join(HERE, "libngx_oracle.so")
 REFERENCE_SO = os.path.join(HERE, "_ref", "libngx_ref.so")
 REFERENCE_GTESTS = os.path.join(HERE, "_ref", "ref_gtests")
+INTEGRATION_CHECK = os.path.join(HERE, "_ref", "integration_check")
 REFERENCE_SOURCES = os.environ.get("NGX_REFERENCE_DIR", "/root/reference")
 
 METRIC_REGULAR = 0
@@ -46,6 +47,8 @@ def build(reference: bool | None = None, quiet: bool = True) -> None:
         reference = os.path.isdir(os.path.join(REFERENCE_SOURCES, "source"))
     if reference:
         subprocess.run(["make", "-C", HERE, "-j8", "reference", f"REF={REFERENCE_SOURCES}"], check=True, stdout=out)
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "neurograph_b200", "lib", "libngx_b200.so")):
+            subprocess.run(["make", "-C", HERE, "integration", f"REF={REFERENCE_SOURCES}"], check=True, stdout=out)
 
 
 class _Graph(C.Structure):

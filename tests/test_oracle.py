@@ -200,3 +200,14 @@ def test_reference_pull_model_misses_shortest_paths():
     pull = rg.apsp_delta_stepping(3, 4)
     assert pull["cpl"] > dijkstra["cpl"]
     assert rg.apsp_delta_stepping(1000, 4)["cpl"] == dijkstra["cpl"]  # no heavy arcs: agrees
+
+
+@pytest.mark.skipif(not __import__("os").path.exists(oracle.REFERENCE_GTESTS), reason="reference gtests not built")
+def test_reference_own_hot_path_tests_pass_under_the_shim():
+    """The reference's own tests/apsp, tests/dijkstra, tests/delta_stepping and tests/centrality files, compiled from
+    its sources against the single-rank shims, pass: the shim build runs the reference faithfully."""
+    import subprocess
+
+    out = subprocess.run([oracle.REFERENCE_GTESTS], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout[-2000:]
+    assert "0 failed" in out.stdout
