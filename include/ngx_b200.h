@@ -105,6 +105,8 @@ typedef struct {
     uint64_t expansions;      /* vertex expansions: one pass over a vertex's out-arcs */
     uint64_t lane_expansions; /* (vertex, source) expansions; lane_expansions / expansions = sources per arc pass */
     uint64_t dag_levels;      /* Kahn levels of the shortest-path DAGs summed over source tiles (Brandes / adjoint) */
+    uint64_t dag_entries;     /* entries of those levels ((vertex, source) pairs, or vertices on the arc-scanning path) */
+    uint64_t dag_scan_tiles;  /* tiles whose DAG did not fit the successor lists and used the arc-scanning passes */
     uint64_t phase_cycles[5]; /* SM cycles summed over CTAs: distances, DAG counts, sigma, delta, summaries */
     /* optional outputs */
     uint64_t* hist;           /* hist_bins entries */

@@ -59,7 +59,8 @@ class _Result(C.Structure):
         ("unreachable", C.c_uint64), ("reached_pairs", C.c_uint64), ("traversed_arcs", C.c_uint64),
         ("hist_overflow", C.c_uint64), ("hist_max", C.c_double), ("cpl", C.c_double), ("efficiency", C.c_double),
         ("kernel_ms", C.c_double), ("phases", C.c_uint64), ("expansions", C.c_uint64), ("lane_expansions", C.c_uint64),
-        ("dag_levels", C.c_uint64), ("phase_cycles", C.c_uint64 * 5),
+        ("dag_levels", C.c_uint64), ("dag_entries", C.c_uint64), ("dag_scan_tiles", C.c_uint64),
+        ("phase_cycles", C.c_uint64 * 5),
         ("hist", C.c_void_p), ("src_sum", C.c_void_p), ("src_max", C.c_void_p), ("src_sum_inverse", C.c_void_p),
         ("src_unreachable", C.c_void_p), ("src_arcs", C.c_void_p),
     ]
@@ -126,6 +127,8 @@ class ApspResult:
     expansions: int = 0
     lane_expansions: int = 0
     dag_levels: int = 0
+    dag_entries: int = 0
+    dag_scan_tiles: int = 0
     phase_cycles: tuple = ()
     hist: np.ndarray | None = None
     per_source: dict | None = None
@@ -196,7 +199,7 @@ class Graph:
             cpl=r.cpl, efficiency=r.efficiency, diameter=r.diameter, unreachable=r.unreachable,
             reached_pairs=r.reached_pairs, traversed_arcs=r.traversed_arcs, sum_distances=r.sum_distances,
             sum_inverse=r.sum_inverse, hist_max=r.hist_max, hist_overflow=r.hist_overflow, kernel_ms=r.kernel_ms,
-            phases=r.phases, expansions=r.expansions, lane_expansions=r.lane_expansions, dag_levels=r.dag_levels,
+            phases=r.phases, expansions=r.expansions, lane_expansions=r.lane_expansions, dag_levels=r.dag_levels, dag_entries=r.dag_entries, dag_scan_tiles=r.dag_scan_tiles,
             phase_cycles=tuple(int(x) for x in r.phase_cycles), hist=hist, per_source=per,
         )
         if per is not None:

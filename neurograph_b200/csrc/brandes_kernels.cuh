@@ -28,7 +28,7 @@ enum TileMode : int { kModeApsp = 0, kModeBrandes = 1, kModeGrad = 2 };
 constexpr uint32_t kNoLevel = 0xFFFFFFFFu;
 
 struct BrandesParams {
-    DeviceCsr rg;                   // reverse CSR (in-arcs), regular lengths; Arc::col = source of the arc
+    DeviceCsr rg;                   // reverse CSR (in-arcs), regular lengths; Arc::col = source, Arc::id = forward stored index
     double* ws_sigma;               // slots * n * kTile
     double* ws_delta;               // slots * n * kTile
     double* ws_delta_g;             // slots * n * kTile (adjoint only)
@@ -36,6 +36,10 @@ struct BrandesParams {
     uint32_t* ws_lvl;               // slots * n * kTile
     int32_t* ws_list;               // slots * n * kTile: the vertices of each level, level after level
     int32_t* ws_loff;               // slots * (n + 2): start of each level in ws_list
+    uint32_t* ws_scnt;              // slots * n * kTile: DAG successors per (vertex, source), then fill positions
+    uint32_t* ws_soff;              // slots * (n * kTile + 1): start of each (vertex, source)'s successor list
+    uint32_t* ws_succ;              // slots * succ_capacity: successor lists (indices into the forward CSR)
+    int64_t succ_capacity;          // entries per slot; a tile with more DAG arcs uses the arc-scanning passes
     unsigned long long* bc;         // 2 * n fixed point (Brandes), or nullptr
     unsigned long long* grad_cpl;   // 2 * m_user fixed point (adjoint), or nullptr
     unsigned long long* grad_eff;   // 2 * m_user fixed point (adjoint), or nullptr
@@ -44,9 +48,12 @@ struct BrandesParams {
     int sigma_pull;                 // 1: pull form for sigma
 };
 
+constexpr int kSuccPerPair = 2;  // successor-list capacity, in DAG arcs per (vertex, source)
+
 inline size_t brandes_slot_bytes(int64_t n, bool adjoint) {
     const size_t nt = static_cast<size_t>(n) * kTile;
-    return nt * (8 + 8 + (adjoint ? 8 : 0) + 4 + 4 + 4) + static_cast<size_t>(n + 2) * 4 + 256;
+    return nt * (8 + 8 + (adjoint ? 8 : 0) + 4 + 4 + 4) + static_cast<size_t>(n + 2) * 4 +
+           nt * 4 + (nt + 1) * 4 + nt * kSuccPerPair * 4 + 1024;
 }
 
 __device__ __forceinline__ bool on_dag(unsigned long long du_bits, double len, unsigned long long dv_bits) {
@@ -331,6 +338,212 @@ __device__ __forceinline__ void brandes_delta_vertex(const DeviceCsr& g, int v, 
         delta[vbase + rank_src] = acc;
         if constexpr (kMode == kModeGrad) {
             delta_g[vbase + rank_src] = acc_g;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------ successor lists
+// The DAG of a tile is about one arc per (vertex, source) without ties, against deg arcs scanned per (vertex, source)
+// by the arc-scanning passes. The dense count pass (lane per source, coalesced distance rows) already visits every DAG
+// arc; it also counts successors per (vertex, source). A block-wide prefix sum gives each (vertex, source) its list,
+// a second dense pass fills the lists (forward-CSR arc indices), and each list is sorted so that every sum over it has
+// a fixed order. sigma and delta then touch only DAG arcs.
+
+// cnt[v][s] = DAG predecessors; scnt[u][s] += 1 for each DAG arc u -> v (warp per vertex, lane per source).
+__device__ __forceinline__ void dag_count(const DeviceCsr& rg, int64_t n, int nsrc, const int* s_src, const unsigned long long* dist, uint32_t* cnt,
+                                          uint32_t* scnt, int lane, int warp, int nwarps) {
+    for (int64_t v = warp; v < n; v += nwarps) {
+        const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
+        const bool active = lane < nsrc && dv != kInfBits && v != s_src[lane];
+        uint32_t c = 0;
+        if (__ballot_sync(0xFFFFFFFFu, active) != 0u) {
+            const int64_t beg = __ldg(&rg.row_ptr[v]);
+            const int64_t end = __ldg(&rg.row_ptr[v + 1]);
+            for (int64_t e0 = beg; e0 < end; e0 += 32) {
+                const int cntr = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
+                Arc a{ 0, 0, 0.0 };
+                if (lane < cntr) {
+                    a = rg.arcs[e0 + lane];
+                }
+                for (int j = 0; j < cntr; j += 4) {
+                    unsigned long long du[4];
+                    double len[4];
+                    int src[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int jj = j + u < cntr ? j + u : 0;
+                        src[u] = __shfl_sync(0xFFFFFFFFu, a.col, jj);
+                        len[u] = __shfl_sync(0xFFFFFFFFu, a.len, jj);
+                        du[u] = (active && j + u < cntr) ? __ldcg(&dist[static_cast<int64_t>(src[u]) * kTile + lane]) : kInfBits;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        if (du[u] != kInfBits && on_dag(du[u], len[u], dv)) {
+                            ++c;
+                            atomicAdd(&scnt[static_cast<int64_t>(src[u]) * kTile + lane], 1u);
+                        }
+                    }
+                }
+            }
+        }
+        cnt[v * kTile + lane] = c;
+    }
+}
+
+// Exclusive prefix sum of in[0..len) into out[0..len] (out[len] = total) by one CTA; returns the total to every thread.
+__device__ __forceinline__ unsigned long long block_exclusive_scan(const uint32_t* in, uint32_t* out, int64_t len, unsigned long long* s_part) {
+    const int tid = threadIdx.x;
+    const int nthreads = blockDim.x;
+    const int64_t chunk = (len + nthreads - 1) / nthreads;
+    const int64_t beg = tid * chunk < len ? tid * chunk : len;
+    const int64_t end = beg + chunk < len ? beg + chunk : len;
+    unsigned long long sum = 0;
+    for (int64_t i = beg; i < end; ++i) {
+        sum += __ldcg(&in[i]);
+    }
+    s_part[tid] = sum;
+    __syncthreads();
+    if (tid == 0) {
+        unsigned long long run = 0;
+        for (int t = 0; t < nthreads; ++t) {
+            const unsigned long long x = s_part[t];
+            s_part[t] = run;
+            run += x;
+        }
+        s_part[nthreads] = run;
+    }
+    __syncthreads();
+    unsigned long long run = s_part[tid];
+    for (int64_t i = beg; i < end; ++i) {
+        const uint32_t x = __ldcg(&in[i]);
+        out[i] = static_cast<uint32_t>(run);
+        run += x;
+    }
+    const unsigned long long total = s_part[nthreads];
+    if (tid == 0) {
+        out[len] = static_cast<uint32_t>(total);
+    }
+    __syncthreads();
+    return total;
+}
+
+// Fills the successor lists: for each DAG arc u -> v (forward index in the reverse record), appended to (u, s).
+__device__ __forceinline__ void dag_fill(const DeviceCsr& rg, int64_t n, int nsrc, const int* s_src, const unsigned long long* dist, const uint32_t* soff,
+                                         uint32_t* sfill, uint32_t* succ, int lane, int warp, int nwarps) {
+    for (int64_t v = warp; v < n; v += nwarps) {
+        const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
+        const bool active = lane < nsrc && dv != kInfBits && v != s_src[lane];
+        if (__ballot_sync(0xFFFFFFFFu, active) == 0u) {
+            continue;
+        }
+        const int64_t beg = __ldg(&rg.row_ptr[v]);
+        const int64_t end = __ldg(&rg.row_ptr[v + 1]);
+        for (int64_t e0 = beg; e0 < end; e0 += 32) {
+            const int cntr = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
+            Arc a{ 0, 0, 0.0 };
+            if (lane < cntr) {
+                a = rg.arcs[e0 + lane];
+            }
+            for (int j = 0; j < cntr; j += 4) {
+                unsigned long long du[4];
+                double len[4];
+                int src[4], fwd[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int jj = j + u < cntr ? j + u : 0;
+                    src[u] = __shfl_sync(0xFFFFFFFFu, a.col, jj);
+                    fwd[u] = __shfl_sync(0xFFFFFFFFu, a.id, jj);
+                    len[u] = __shfl_sync(0xFFFFFFFFu, a.len, jj);
+                    du[u] = (active && j + u < cntr) ? __ldcg(&dist[static_cast<int64_t>(src[u]) * kTile + lane]) : kInfBits;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (du[u] != kInfBits && on_dag(du[u], len[u], dv)) {
+                        const int64_t urow = static_cast<int64_t>(src[u]) * kTile + lane;
+                        const uint32_t pos = atomicAdd(&sfill[urow], 1u);
+                        succ[__ldcg(&soff[urow]) + pos] = static_cast<uint32_t>(fwd[u]);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Sorts each successor list by forward arc index (the fill order depends on timing; the sums must not).
+__device__ __forceinline__ void dag_sort(const uint32_t* soff, uint32_t* succ, int64_t nt) {
+    for (int64_t i = threadIdx.x; i < nt; i += blockDim.x) {
+        const uint32_t beg = __ldcg(&soff[i]);
+        const uint32_t end = __ldcg(&soff[i + 1]);
+        for (uint32_t a = beg + 1; a < end; ++a) {
+            const uint32_t key = succ[a];
+            uint32_t b = a;
+            while (b > beg && succ[b - 1] > key) {
+                succ[b] = succ[b - 1];
+                --b;
+            }
+            succ[b] = key;
+        }
+    }
+}
+
+// sigma over one level of (vertex, source) entries (entry = v * 32 + s): push sigma[v][s] into the DAG successors
+// (exact integer sums, see brandes_sigma_vertex) and release those whose last predecessor this was.
+__device__ __forceinline__ void dag_sigma_level(const DeviceCsr& g, const int32_t* entries, int len, uint32_t level, double* sigma, uint32_t* cnt,
+                                                uint32_t* lvl, const uint32_t* soff, const uint32_t* succ, int32_t* next_list, int* next_len,
+                                                int* inexact) {
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        const uint32_t entry = static_cast<uint32_t>(__ldcg(&entries[i]));
+        const int64_t row = static_cast<int64_t>(entry >> 5) * kTile + (entry & 31u);
+        const double sv = __ldcg(&sigma[row]);
+        const uint32_t beg = __ldcg(&soff[row]);
+        const uint32_t end = __ldcg(&soff[row + 1]);
+        for (uint32_t j = beg; j < end; ++j) {
+            const Arc arc = g.arcs[__ldcg(&succ[j])];
+            const int64_t xrow = static_cast<int64_t>(arc.col) * kTile + (entry & 31u);
+            const double before = atomicAdd(&sigma[xrow], sv);
+            if (before + sv >= kSigmaExact) {
+                atomicExch(inexact, 1);
+            }
+            if (atomicSub(&cnt[xrow], 1u) == 1u) {
+                lvl[xrow] = level + 1u;
+                next_list[atomicAdd(next_len, 1)] = static_cast<int32_t>((static_cast<uint32_t>(arc.col) << 5) | (entry & 31u));
+            }
+        }
+    }
+}
+
+// delta (and the adjoint terms) over one level of (vertex, source) entries: pull over the sorted successor list.
+template <int kMode>
+__device__ __forceinline__ void dag_delta_level(const DeviceCsr& g, const int32_t* entries, int len, const unsigned long long* dist, const double* sigma,
+                                                double* delta, double* delta_g, const uint32_t* soff, const uint32_t* succ, unsigned long long* grad_cpl,
+                                                unsigned long long* grad_eff) {
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+        const uint32_t entry = static_cast<uint32_t>(__ldcg(&entries[i]));
+        const uint32_t s = entry & 31u;
+        const int64_t row = static_cast<int64_t>(entry >> 5) * kTile + s;
+        const double sv = __ldcg(&sigma[row]);
+        const uint32_t beg = __ldcg(&soff[row]);
+        const uint32_t end = __ldcg(&soff[row + 1]);
+        double acc = 0.0, acc_g = 0.0;
+        for (uint32_t j = beg; j < end; ++j) {
+            const Arc arc = g.arcs[__ldcg(&succ[j])];
+            const int64_t xrow = static_cast<int64_t>(arc.col) * kTile + s;
+            if constexpr (kMode == kModeBrandes) {
+                acc += sv * ((1.0 + __ldcg(&delta[xrow])) / __ldcg(&sigma[xrow]));
+            } else {
+                const double share = sv / __ldcg(&sigma[xrow]);
+                const double inv = 1.0 / __longlong_as_double(static_cast<long long>(__ldcg(&dist[xrow])));
+                const double c = share * (1.0 + __ldcg(&delta[xrow]));
+                const double cg = share * (inv * inv + __ldcg(&delta_g[xrow]));
+                acc += c;
+                acc_g += cg;
+                fixed_add(&grad_cpl[2 * static_cast<int64_t>(arc.id)], c);
+                fixed_add(&grad_eff[2 * static_cast<int64_t>(arc.id)], cg);
+            }
+        }
+        delta[row] = acc;
+        if constexpr (kMode == kModeGrad) {
+            delta_g[row] = acc_g;
         }
     }
 }

@@ -251,7 +251,8 @@ int ngx_graph_create(const ngx_csr* csr, int device, ngx_graph** out) {
     for (int64_t u = 0; u < n; ++u) {
         for (int64_t e = row_ptr[static_cast<size_t>(u)]; e < row_ptr[static_cast<size_t>(u) + 1]; ++e) {
             const Arc& a = regular[static_cast<size_t>(e)];
-            rarcs[static_cast<size_t>(fill[static_cast<size_t>(a.col)]++)] = Arc{ static_cast<int32_t>(u), a.id, a.len };
+            // the reverse record keeps the arc's index in the stored forward CSR (its caller index is arcs[e].id)
+            rarcs[static_cast<size_t>(fill[static_cast<size_t>(a.col)]++)] = Arc{ static_cast<int32_t>(u), static_cast<int32_t>(e), a.len };
         }
     }
 

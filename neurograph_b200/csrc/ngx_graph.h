@@ -22,7 +22,7 @@ struct ngx_graph {
     int64_t* d_row_ptr = nullptr;
     ngx::Arc* d_arcs_regular = nullptr;
     ngx::Arc* d_arcs_inverse = nullptr;
-    // Reverse CSR (in-arcs) with regular lengths; Arc::col is the arc's source, Arc::id its caller index.
+    // Reverse CSR (in-arcs) with regular lengths; Arc::col is the arc's source, Arc::id its index in the stored forward CSR.
     int64_t* d_rrow_ptr = nullptr;
     ngx::Arc* d_rarcs = nullptr;
 

@@ -211,6 +211,14 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const i
         bp.ws_list = reinterpret_cast<int32_t*>(ws);
         ws += static_cast<size_t>(slots) * nt * 4;
         bp.ws_loff = reinterpret_cast<int32_t*>(ws);
+        ws += static_cast<size_t>(slots) * static_cast<size_t>(n + 2) * 4;
+        bp.ws_scnt = reinterpret_cast<uint32_t*>(ws);
+        ws += static_cast<size_t>(slots) * nt * 4;
+        bp.ws_soff = reinterpret_cast<uint32_t*>(ws);
+        ws += static_cast<size_t>(slots) * (nt + 1) * 4;
+        // list entries pack (vertex << 5 | source) into 32 bits; larger graphs use the arc-scanning passes
+        bp.succ_capacity = n < (int64_t(1) << 26) ? static_cast<int64_t>(nt) * kSuccPerPair : 0;
+        bp.ws_succ = reinterpret_cast<uint32_t*>(ws);
         if (extra != nullptr) {
             bp.bc = extra->bc;
             bp.grad_cpl = extra->grad_cpl;
@@ -321,6 +329,8 @@ int collect(ngx_graph* g, const RunOutputs& o, int64_t num_sources, int64_t hist
     r->expansions = counters[kExpansions];
     r->lane_expansions = counters[kLaneExpansions];
     r->dag_levels = counters[kDagLevels];
+    r->dag_entries = counters[kDagEntries];
+    r->dag_scan_tiles = counters[kDagScanTiles];
     for (int i = 0; i < 5; ++i) {
         r->phase_cycles[i] = counters[kCyclesSssp + i];
     }
@@ -347,7 +357,7 @@ void clear_result_totals(ngx_apsp_result* r) {
     r->hist_max = 0.0;
     r->cpl = r->efficiency = 0.0;
     r->kernel_ms = 0.0;
-    r->phases = r->expansions = r->lane_expansions = r->dag_levels = 0;
+    r->phases = r->expansions = r->lane_expansions = r->dag_levels = r->dag_entries = r->dag_scan_tiles = 0;
     for (int i = 0; i < 5; ++i) {
         r->phase_cycles[i] = 0;
     }

@@ -68,6 +68,8 @@ enum Counter : int {
     kCyclesDelta = 11,
     kCyclesEpilogue = 12,
     kDagLevels = 13,      // Kahn levels of the shortest-path DAG, summed over tiles (Brandes / adjoint)
+    kDagEntries = 14,     // (vertex, level) entries of the Kahn level lists, summed over tiles
+    kDagScanTiles = 15,   // tiles whose DAG overflowed the successor lists (arc-scanning passes used)
     kCounterCount = 16
 };
 
@@ -254,7 +256,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     uint32_t* lvl = nullptr;
     int32_t* list = nullptr;
     int32_t* loff = nullptr;
+    uint32_t* scnt = nullptr;
+    uint32_t* soff = nullptr;
+    uint32_t* succ = nullptr;
+    __shared__ unsigned long long s_part[kBlock + 1];
     if constexpr (kMode != kModeApsp) {
+        scnt = b.ws_scnt + slot * nt;
+        soff = b.ws_soff + slot * (nt + 1);
+        succ = b.ws_succ + slot * b.succ_capacity;
+        for (int64_t i = tid; i < nt; i += blockDim.x) {
+            scnt[i] = 0u;
+        }
         sigma = b.ws_sigma + slot * nt;
         delta = b.ws_delta + slot * nt;
         delta_g = kMode == kModeGrad ? b.ws_delta_g + slot * nt : nullptr;
@@ -445,13 +457,88 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         }
         if constexpr (kMode != kModeApsp) {
             // ------------------------------------------------------------ shortest-path DAG: counts, sigma, delta
-            brandes_count(b.rg, n, nsrc, s_src, dist, cnt, lane, warp, nwarps);
+            dag_count(b.rg, n, nsrc, s_src, dist, cnt, scnt, lane, warp, nwarps);
             __syncthreads();
+            const unsigned long long dag_arcs = block_exclusive_scan(scnt, soff, nt, s_part);
+            const bool use_lists = dag_arcs <= static_cast<unsigned long long>(b.succ_capacity);
+            for (int64_t i = tid; i < nt; i += blockDim.x) {
+                scnt[i] = 0u;
+            }
+            __syncthreads();
+            if (use_lists) {
+                dag_fill(b.rg, n, nsrc, s_src, dist, soff, scnt, succ, lane, warp, nwarps);
+                __syncthreads();
+                dag_sort(soff, succ, nt);
+                __syncthreads();
+            }
             if (tid == 0) {
                 const long long now = clock64();
                 atomicAdd(&p.out.counters[kCyclesCount], static_cast<unsigned long long>(now - t_phase));
                 t_phase = now;
+                if (!use_lists) {
+                    atomicAdd(&p.out.counters[kDagScanTiles], 1ull);
+                }
             }
+          if (use_lists) {
+            // --- sigma and delta over the successor lists, one (vertex, source) entry per thread
+            if (tid == 0) {
+                s.level = 0u;
+                s.lvl_start = 0;
+                s.lvl_len = 0;
+                s.next_len = 0;
+                loff[0] = 0;
+            }
+            __syncthreads();
+            if (warp == 0) {
+                const int v = s_src[lane];
+                if (v >= 0) {
+                    const int64_t row = static_cast<int64_t>(v) * kTile + lane;
+                    lvl[row] = 0u;
+                    sigma[row] = 1.0;
+                    list[atomicAdd(&s.lvl_len, 1)] = static_cast<int32_t>((static_cast<uint32_t>(v) << 5) | static_cast<uint32_t>(lane));
+                }
+            }
+            __syncthreads();
+            for (;;) {
+                const int start = s.lvl_start;
+                const int len = s.lvl_len;
+                if (len == 0) {
+                    break;
+                }
+                const unsigned level = s.level;
+                dag_sigma_level(p.g, list + start, len, level, sigma, cnt, lvl, soff, succ, list + start + len, &s.next_len, b.sigma_inexact);
+                __syncthreads();
+                if (tid == 0) {
+                    s.lvl_start = start + len;
+                    s.lvl_len = s.next_len;
+                    s.next_len = 0;
+                    s.level = level + 1u;
+                    loff[level + 1u] = start + len;
+                }
+                __syncthreads();
+            }
+            if (tid == 0) {
+                const long long now = clock64();
+                atomicAdd(&p.out.counters[kCyclesSigma], static_cast<unsigned long long>(now - t_phase));
+                t_phase = now;
+            }
+            const int levels = static_cast<int>(s.level);
+            const int lowest = kMode == kModeGrad ? 0 : 1;
+            for (int level = levels - 1; level >= lowest; --level) {
+                const int start = __ldcg(&loff[level]);
+                const int end = __ldcg(&loff[level + 1]);
+                dag_delta_level<kMode>(p.g, list + start, end - start, dist, sigma, delta, delta_g, soff, succ, b.grad_cpl, b.grad_eff);
+                __syncthreads();
+            }
+            if (tid == 0) {
+                atomicAdd(&p.out.counters[kDagLevels], static_cast<unsigned long long>(levels));
+                atomicAdd(&p.out.counters[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
+                const long long now = clock64();
+                atomicAdd(&p.out.counters[kCyclesDelta], static_cast<unsigned long long>(now - t_phase));
+                t_phase = now;
+            }
+          } else {
+            // --- too many DAG arcs for the lists (many ties): the arc-scanning passes, one vertex per warp
             if (tid == 0) {
                 s.stamp += 1u;
                 s.level = 0u;
@@ -522,12 +609,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             }
             if (tid == 0) {
                 atomicAdd(&p.out.counters[kDagLevels], static_cast<unsigned long long>(levels));
+                atomicAdd(&p.out.counters[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
             }
             if (tid == 0) {
                 const long long now = clock64();
                 atomicAdd(&p.out.counters[kCyclesDelta], static_cast<unsigned long long>(now - t_phase));
                 t_phase = now;
             }
+          }
         }
 
         // ------------------------------------------------------------ epilogue: fused APSP summaries, reset
@@ -555,6 +644,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 }
                 cnt[row] = 0u;
                 lvl[row] = kNoLevel;
+                scnt[row] = 0u;
             }
             if (!valid) {
                 continue;

@@ -68,6 +68,15 @@ int main(int argc, char** argv) {
         const bool bc_ok = std::fabs(bc_gpu - bc_ref) <= 1e-12 * std::fmax(1.0, std::fabs(bc_ref));
         std::printf("%-40s apsp %s  inverse %s  betweenness %s (%.17g vs %.17g)\n", name, apsp_ok ? "ok" : "MISMATCH", inv_ok ? "ok" : "MISMATCH",
                     bc_ok ? "ok" : "MISMATCH", bc_gpu, bc_ref);
+        if (!apsp_ok || !inv_ok) {
+            std::printf("  regular: gpu cpl %.17g eff %.17g dia %llu unreach %llu clusters %zu | ref cpl %.17g eff %.17g dia %llu unreach %llu clusters %zu\n",
+                        gpu.average_shortest_path_length, gpu.average_efficiency, static_cast<unsigned long long>(gpu.diameter),
+                        static_cast<unsigned long long>(gpu.number_disconnected_pairs), gpu.cluster_sizes.size(), ref.average_shortest_path_length,
+                        ref.average_efficiency, static_cast<unsigned long long>(ref.diameter), static_cast<unsigned long long>(ref.number_disconnected_pairs),
+                        ref.cluster_sizes.size());
+            std::printf("  inverse: gpu cpl %.17g eff %.17g dia %.17g | ref cpl %.17g eff %.17g dia %.17g\n", gpu_inv.average_shortest_path_length,
+                        gpu_inv.average_efficiency, gpu_inv.diameter, ref_inv.average_shortest_path_length, ref_inv.average_efficiency, ref_inv.diameter);
+        }
         failures += apsp_ok && inv_ok && bc_ok ? 0 : 1;
     }
     mpiPP::MPIWrapper::finalize();

@@ -110,3 +110,26 @@ def test_path_counts_beyond_2_53_use_the_pull_form(restatement):
         bc2, _ = gg.brandes()
     assert_bc_close(bc, restatement.brandes(csr), "diamonds")
     assert np.array_equal(bc, bc2)
+
+
+def test_dense_ties_use_the_arc_scanning_passes(restatement):
+    """Unit weights on a dense graph give many equal-length predecessors: the DAG overflows the successor lists and
+    the arc-scanning passes run; results still match the oracle."""
+    c = synth.random_graph(300, 40, weights="unit", seed=12)
+    csr = oracle.Csr.from_arrays(c.n, c.row_ptr, c.col, c.w)
+    with ngx.Graph(c.n, c.row_ptr, c.col, c.w) as gg:
+        bc, res = gg.brandes()
+        dcpl, deff, _ = gg.apsp_grad()
+    assert res.dag_scan_tiles > 0
+    assert_bc_close(bc, restatement.brandes(csr), "dense ties")
+    want_cpl, want_eff, _ = restatement.apsp_grad(csr)
+    assert np.allclose(dcpl, want_cpl, rtol=1e-12, atol=1e-15) and np.allclose(deff, want_eff, rtol=1e-12, atol=1e-15)
+
+
+def test_sparse_graphs_use_the_successor_lists(restatement):
+    c = synth.connectome(1200, 10, 0.2, weights="lognormal", seed=13, use_gpu=False)
+    csr = oracle.Csr.from_arrays(c.n, c.row_ptr, c.col, c.w)
+    with ngx.Graph(c.n, c.row_ptr, c.col, c.w) as gg:
+        bc, res = gg.brandes()
+    assert res.dag_scan_tiles == 0
+    assert_bc_close(bc, restatement.brandes(csr), "lists")
