@@ -156,6 +156,50 @@ NGX_API int ngx_brandes(ngx_graph* graph, const ngx_apsp_opts* opts, double* bc,
  */
 NGX_API int ngx_apsp_grad(ngx_graph* graph, const ngx_apsp_opts* opts, double* dcpl, double* deff, ngx_apsp_result* result);
 
+/* ------------------------------------------------------------------------------------------------------------------
+ * Batches: many independent graphs of uneven sizes in one handle and one persistent launch, fed by a device queue of
+ * (graph, source tile) work items in longest-first order. No reference counterpart: the reference processes one
+ * graph per run (neurograph.cpp:139-416); the batch runs that loop's APSP / betweenness for every graph at once.
+ */
+typedef enum { NGX_TASK_APSP = 0, NGX_TASK_BRANDES = 1, NGX_TASK_GRAD = 2 } ngx_task;
+
+#define NGX_SIZE_CLASSES 32 /* graphs are grouped by floor(log2(n)) for the tuned bucket widths */
+
+typedef struct {
+    int task;               /* ngx_task: APSP summaries; + Brandes betweenness; + CPL / efficiency gradient */
+    int metric;             /* ngx_metric (APSP only; betweenness and the gradient use |w|) */
+    double delta_scale;     /* bucket width = delta_scale x the graph's mean arc length; <= 0: its size class's tuned
+                               scale (1.0 until ngx_batch_autotune has run) */
+    int block_threads;      /* 0 = default */
+    int64_t hist_bins;      /* distance histogram bins per graph; 0 = none */
+    double hist_max;        /* histogram bound, the same for all graphs; must be > 0 when hist_bins > 0 */
+    int use_cuda_graph;     /* capture the run (output reset + launch) and replay it while these options are unchanged */
+    uint64_t max_iterations;/* cap on phases per source tile; 0 = 4 * n + 64 of the largest graph */
+} ngx_batch_opts;
+
+/* Validates and uploads `count` CSRs into one handle. Vertex and arc numbering stays per graph in every output. */
+NGX_API int ngx_batch_create(const ngx_csr* graphs, int64_t count, int device, ngx_graph** out);
+
+/*
+ * All-sources run of every graph of a batch handle. results: `count` entries (per-graph summaries; their optional
+ * per-source / histogram pointers are honoured). bc: sum of n entries (graph after graph) or NULL, for NGX_TASK_BRANDES.
+ * dcpl, deff: sum of m entries (graph after graph) or NULL, for NGX_TASK_GRAD.
+ */
+NGX_API int ngx_batch_run(ngx_graph* batch, const ngx_batch_opts* opts, ngx_apsp_result* results, double* bc, double* dcpl, double* deff);
+
+/*
+ * Picks the bucket width scale of every size class present in the batch: for each class, the median-size graph's first
+ * wave of source tiles runs with scales 1/8 .. 4 and the fastest (traversed arcs per second) is kept in the handle.
+ * class_scales (optional, NGX_SIZE_CLASSES entries) receives the result (0 for classes without graphs).
+ */
+NGX_API int ngx_batch_autotune(ngx_graph* batch, int task, double* class_scales);
+
+/*
+ * Replaces the weights of a graph or batch handle in place (same arcs, caller order, sum of m entries). A weight may
+ * not change between zero and non-zero (that changes the arc set; create a new handle instead).
+ */
+NGX_API int ngx_graph_update_weights(ngx_graph* graph, const double* w);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,6 +13,8 @@ Mapping to the reference (paths relative to the reference project):
 * ``Graph.brandes()``            BetweennessCentrality::compute_average_betweenness_centrality with the Brandes
                                  variant (source/metrics/paths/BetweennessCentrality.h:46-80)
 * ``Graph.apsp_grad()``          new: gradient of CPL and global efficiency w.r.t. every arc length
+* ``Batch(...)``                 new: many graphs in one handle and one persistent launch (the per-graph loop of
+                                 source/neurograph.cpp:139-416 run for every graph at once)
 """
 
 from __future__ import annotations
@@ -30,6 +32,8 @@ NGX_OK = 0
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARGUMENT", 2: "OUT_OF_MEMORY", 3: "CUDA_ERROR", 4: "TIMEOUT", 5: "ABORTED", 6: "UNSUPPORTED"}
 METRICS = {"regular": 0, "inverse": 1}
 MODES = {"batched": 0, "plain": 1}
+TASKS = {"apsp": 0, "brandes": 1, "grad": 2}
+SIZE_CLASSES = 32
 TILE = 32
 
 
@@ -53,6 +57,13 @@ class _Opts(C.Structure):
     ]
 
 
+class _BatchOpts(C.Structure):
+    _fields_ = [
+        ("task", C.c_int), ("metric", C.c_int), ("delta_scale", C.c_double), ("block_threads", C.c_int),
+        ("hist_bins", C.c_int64), ("hist_max", C.c_double), ("use_cuda_graph", C.c_int), ("max_iterations", C.c_uint64),
+    ]
+
+
 class _Result(C.Structure):
     _fields_ = [
         ("sum_distances", C.c_double), ("sum_inverse", C.c_double), ("diameter", C.c_double),
@@ -72,7 +83,7 @@ _LIB = None
 EXPORTED = [
     "ngx_status_string", "ngx_last_error", "ngx_version", "ngx_graph_create", "ngx_graph_destroy", "ngx_graph_size",
     "ngx_graph_request_abort", "ngx_graph_set_stream", "ngx_graph_set_memory_budget", "ngx_apsp", "ngx_sssp_rows", "ngx_brandes",
-    "ngx_apsp_grad",
+    "ngx_apsp_grad", "ngx_batch_create", "ngx_batch_run", "ngx_batch_autotune", "ngx_graph_update_weights",
 ]
 
 
@@ -99,6 +110,10 @@ def library() -> C.CDLL:
             lib.ngx_brandes.argtypes = [C.c_void_p, C.POINTER(_Opts), C.c_void_p, C.POINTER(_Result)]
         if hasattr(lib, "ngx_apsp_grad"):
             lib.ngx_apsp_grad.argtypes = [C.c_void_p, C.POINTER(_Opts), C.c_void_p, C.c_void_p, C.POINTER(_Result)]
+        lib.ngx_batch_create.argtypes = [C.POINTER(_Csr), C.c_int64, C.c_int, C.POINTER(C.c_void_p)]
+        lib.ngx_batch_run.argtypes = [C.c_void_p, C.POINTER(_BatchOpts), C.POINTER(_Result), C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.ngx_batch_autotune.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        lib.ngx_graph_update_weights.argtypes = [C.c_void_p, C.c_void_p]
         _LIB = lib
     return _LIB
 
@@ -182,6 +197,14 @@ class Graph:
     def set_memory_budget(self, nbytes: int) -> None:
         _check(library().ngx_graph_set_memory_budget(self._handle, int(nbytes)))
 
+    def update_weights(self, w) -> None:
+        """Replaces the arc weights in place (same arcs; no weight may change between zero and non-zero)."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        if w.size != self.m:
+            raise ValueError(f"expected {self.m} weights, got {w.size}")
+        _check(library().ngx_graph_update_weights(self._handle, w.ctypes.data if self.m else None))
+        self.w = w
+
     def _opts(self, sources, metric, mode, delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations):
         srcs = None if sources is None else np.ascontiguousarray(sources, dtype=np.int64)
         opts = _Opts(
@@ -251,6 +274,99 @@ class Graph:
         deff = np.zeros(max(self.m, 1), np.float64)
         _check(library().ngx_apsp_grad(self._handle, C.byref(opts), dcpl.ctypes.data, deff.ctypes.data, C.byref(r)))
         return dcpl[: self.m], deff[: self.m], self._result(r, hist, per, k)
+
+
+class Batch:
+    """Many independent graphs resident on one GPU in one handle; every run covers all sources of all graphs.
+
+    ``graphs`` is a sequence of ``(n, row_ptr, col, w)``. Results, betweenness and gradients keep per-graph numbering.
+    """
+
+    def __init__(self, graphs, device: int = 0):
+        lib = library()
+        self.graphs = [(int(n), np.ascontiguousarray(rp, dtype=np.int64), np.ascontiguousarray(c, dtype=np.int32),
+                        np.ascontiguousarray(w, dtype=np.float64)) for n, rp, c, w in graphs]
+        self.ns = [g[0] for g in self.graphs]
+        self.ms = [int(g[2].size) for g in self.graphs]
+        csrs = (_Csr * max(1, len(self.graphs)))()
+        for i, (n, rp, c, w) in enumerate(self.graphs):
+            csrs[i] = _Csr(n, c.size, rp.ctypes.data, c.ctypes.data if c.size else None, w.ctypes.data if c.size else None)
+        handle = C.c_void_p()
+        _check(lib.ngx_batch_create(csrs, len(self.graphs), int(device), C.byref(handle)))
+        self._handle = handle
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            library().ngx_graph_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        _check(library().ngx_graph_set_stream(self._handle, stream_handle))
+
+    def run(self, task="apsp", metric="regular", delta_scale=0.0, hist_bins=0, hist_max=0.0, per_source=False,
+            use_cuda_graph=False, block_threads=0, max_iterations=0):
+        """Runs `task` for every graph. Returns (results, extra): a list of ApspResult and, per graph, the betweenness
+        vector (task "brandes"), the (dcpl, deff) pair (task "grad") or None."""
+        t = TASKS[task] if isinstance(task, str) else int(task)
+        opts = _BatchOpts(t, METRICS[metric] if isinstance(metric, str) else int(metric), float(delta_scale),
+                          int(block_threads), int(hist_bins), float(hist_max), int(bool(use_cuda_graph)), int(max_iterations))
+        count = len(self.graphs)
+        structs = (_Result * max(1, count))()
+        keep = []
+        for i, n in enumerate(self.ns):
+            r, hist, per = Graph._result_struct(hist_bins, per_source, n)
+            structs[i] = r
+            keep.append((hist, per))
+        n_total, m_total = sum(self.ns), sum(self.ms)
+        bc = np.zeros(max(1, n_total)) if t == 1 else None
+        dcpl = np.zeros(max(1, m_total)) if t == 2 else None
+        deff = np.zeros(max(1, m_total)) if t == 2 else None
+        _check(library().ngx_batch_run(self._handle, C.byref(opts), structs,
+                                       None if bc is None else bc.ctypes.data,
+                                       None if dcpl is None else dcpl.ctypes.data,
+                                       None if deff is None else deff.ctypes.data))
+        results, extras = [], []
+        v_off = a_off = 0
+        for i, n in enumerate(self.ns):
+            hist, per = keep[i]
+            view = Graph.__new__(Graph)
+            view.n = n
+            results.append(Graph._result(view, structs[i], hist, per, n))
+            m = self.ms[i]
+            if bc is not None:
+                extras.append(bc[v_off:v_off + n].copy())
+            elif dcpl is not None:
+                extras.append((dcpl[a_off:a_off + m].copy(), deff[a_off:a_off + m].copy()))
+            else:
+                extras.append(None)
+            v_off += n
+            a_off += m
+        return results, extras
+
+    def autotune(self, task="apsp") -> np.ndarray:
+        """Tunes the bucket width per size class (floor(log2 n)); returns the chosen scales (0 = class empty)."""
+        scales = np.zeros(SIZE_CLASSES)
+        _check(library().ngx_batch_autotune(self._handle, TASKS[task] if isinstance(task, str) else int(task), scales.ctypes.data))
+        return scales
+
+    def update_weights(self, weights) -> None:
+        """Replaces all graphs' weights in place: one array per graph, caller arc order."""
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(w, dtype=np.float64) for w in weights]) if weights else np.zeros(0))
+        if flat.size != sum(self.ms):
+            raise ValueError("weights do not match the batch's arcs")
+        _check(library().ngx_graph_update_weights(self._handle, flat.ctypes.data if flat.size else None))
 
 
 def version() -> str:

@@ -23,8 +23,6 @@
 
 namespace ngx {
 
-enum TileMode : int { kModeApsp = 0, kModeBrandes = 1, kModeGrad = 2 };
-
 constexpr uint32_t kNoLevel = 0xFFFFFFFFu;
 
 struct BrandesParams {

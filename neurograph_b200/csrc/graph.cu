@@ -55,6 +55,12 @@ int ensure_workspace(ngx_graph* g, size_t bytes) {
     }
     if (g->d_workspace != nullptr) {
         NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        if (g->graph_exec != nullptr) {
+            // a captured batch run refers to the old workspace
+            cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g->graph_exec));
+            g->graph_exec = nullptr;
+            g->graph_key = 0;
+        }
         NGX_CUDA_TRY(cudaFree(g->d_workspace));
         g->d_workspace = nullptr;
         g->workspace_bytes = 0;
@@ -80,6 +86,11 @@ void release(ngx_graph* g) {
     cudaFree(g->d_rrow_ptr);
     cudaFree(g->d_rarcs);
     cudaFree(g->d_workspace);
+    cudaFree(g->d_items);
+    cudaFree(g->d_persistent);
+    if (g->graph_exec != nullptr) {
+        cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g->graph_exec));
+    }
     if (g->h_abort != nullptr) {
         cudaFreeHost(g->h_abort);
     }
@@ -128,6 +139,171 @@ int validate(const ngx_csr* csr) {
 }
 
 }  // namespace
+
+int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** out) {
+    if (out == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: out is NULL");
+    }
+    *out = nullptr;
+    if (csrs == nullptr || count <= 0) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: no graphs");
+    }
+    int64_t n_total = 0, m_total = 0;
+    for (int64_t i = 0; i < count; ++i) {
+        if (const int rc = validate(&csrs[i]); rc != NGX_OK) {
+            return count > 1 ? fail(rc, "graph " + std::to_string(i) + ": " + ngx_last_error()) : rc;
+        }
+        n_total += csrs[i].n;
+        m_total += csrs[i].m;
+    }
+    if (n_total >= (int64_t(1) << 31) - 1 || m_total >= (int64_t(1) << 31) - 1) {
+        return fail(NGX_UNSUPPORTED, "ngx_graph_create: total vertices and arcs must be below 2^31 - 1");
+    }
+    int device_count = 0;
+    NGX_CUDA_TRY(cudaGetDeviceCount(&device_count));
+    if (device < 0 || device >= device_count) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: no CUDA device " + std::to_string(device));
+    }
+    NGX_CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop{};
+    NGX_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        return fail(NGX_UNSUPPORTED, std::string("ngx_graph_create: the kernels are built for sm_100a (B200); device is ") + prop.name);
+    }
+
+    auto* g = new (std::nothrow) ngx_graph{};
+    if (g == nullptr) {
+        return fail(NGX_OUT_OF_MEMORY, "ngx_graph_create: host allocation failed");
+    }
+    g->device = device;
+    g->sm_count = prop.multiProcessorCount;
+    g->n_total = n_total;
+    g->m_user = m_total;
+
+    const auto finish = [&](int rc) -> int {
+        if (rc != NGX_OK) {
+            release(g);
+            return rc;
+        }
+        *out = g;
+        return NGX_OK;
+    };
+
+    if (cudaStreamCreateWithFlags(&g->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaHostAlloc(reinterpret_cast<void**>(&g->h_abort), sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(reinterpret_cast<void**>(&g->d_abort), g->h_abort, 0) != cudaSuccess) {
+        return finish(fail(NGX_CUDA_ERROR, "ngx_graph_create: stream or abort flag setup failed"));
+    }
+    *g->h_abort = 0;
+    g->stream = g->own_stream;
+
+    // Host compaction, graph after graph: drop zero-weight arcs, keep each arc's caller index (graphs numbered
+    // consecutively), precompute both metrics' lengths. Row offsets are global arc indices; targets stay graph-local.
+    std::vector<int64_t> row_ptr;
+    std::vector<int64_t> rrow_ptr;
+    std::vector<Arc> regular;
+    std::vector<Arc> inverse;
+    row_ptr.reserve(static_cast<size_t>(n_total + count));
+    rrow_ptr.reserve(static_cast<size_t>(n_total + count));
+    regular.reserve(static_cast<size_t>(m_total));
+    inverse.reserve(static_cast<size_t>(m_total));
+    std::vector<Arc> rarcs(static_cast<size_t>(m_total));
+    g->stored_of_user.assign(static_cast<size_t>(m_total), -1);
+    double sum_regular = 0.0, sum_inverse = 0.0;
+    double min_regular = INFINITY, max_regular = 0.0;
+    int64_t user_arc_off = 0, vertex_off = 0;
+    g->parts.resize(static_cast<size_t>(count));
+    for (int64_t gi = 0; gi < count; ++gi) {
+        const ngx_csr* csr = &csrs[gi];
+        const int64_t n = csr->n;
+        GraphPart& part = g->parts[static_cast<size_t>(gi)];
+        part.n = n;
+        part.m_user = csr->m;
+        part.row_off = static_cast<int64_t>(row_ptr.size());
+        part.user_arc_off = user_arc_off;
+        part.vertex_off = vertex_off;
+        const int64_t first_arc = static_cast<int64_t>(regular.size());
+        std::vector<int64_t> in_degree(static_cast<size_t>(n) + 1, 0);
+        double part_regular = 0.0, part_inverse = 0.0;
+        row_ptr.push_back(first_arc);
+        for (int64_t u = 0; u < n; ++u) {
+            for (int64_t e = csr->row_ptr[u]; e < csr->row_ptr[u + 1]; ++e) {
+                const double a = std::fabs(csr->w[e]);
+                if (a == 0.0) {
+                    continue;
+                }
+                const int32_t v = csr->col[e];
+                const int32_t id = static_cast<int32_t>(user_arc_off + e);
+                g->stored_of_user[static_cast<size_t>(id)] = static_cast<int32_t>(regular.size());
+                regular.push_back(Arc{ v, id, a });
+                inverse.push_back(Arc{ v, id, 1.0 / a });
+                part_regular += a;
+                part_inverse += 1.0 / a;
+                min_regular = std::min(min_regular, a);
+                max_regular = std::max(max_regular, a);
+                in_degree[static_cast<size_t>(v) + 1] += 1;
+            }
+            row_ptr.push_back(static_cast<int64_t>(regular.size()));
+            g->max_out_degree = std::max(g->max_out_degree, row_ptr.back() - row_ptr[row_ptr.size() - 2]);
+        }
+        part.m_stored = static_cast<int64_t>(regular.size()) - first_arc;
+        if (part.m_stored > 0) {
+            part.mean_len_regular = part_regular / static_cast<double>(part.m_stored);
+            part.mean_len_inverse = part_inverse / static_cast<double>(part.m_stored);
+        }
+        sum_regular += part_regular;
+        sum_inverse += part_inverse;
+        // reverse CSR of this graph by counting sort over targets; within a target, ascending source order
+        const size_t rbase = rrow_ptr.size();
+        rrow_ptr.push_back(first_arc);
+        for (int64_t v = 0; v < n; ++v) {
+            rrow_ptr.push_back(rrow_ptr.back() + in_degree[static_cast<size_t>(v) + 1]);
+        }
+        std::vector<int64_t> fill(rrow_ptr.begin() + static_cast<std::ptrdiff_t>(rbase), rrow_ptr.end() - 1);
+        for (int64_t u = 0; u < n; ++u) {
+            for (int64_t e = row_ptr[static_cast<size_t>(part.row_off + u)]; e < row_ptr[static_cast<size_t>(part.row_off + u + 1)]; ++e) {
+                const Arc& a = regular[static_cast<size_t>(e)];
+                // the reverse record keeps the arc's index in the stored forward CSR (its caller index is arcs[e].id)
+                rarcs[static_cast<size_t>(fill[static_cast<size_t>(a.col)]++)] = Arc{ static_cast<int32_t>(u), static_cast<int32_t>(e), a.len };
+            }
+        }
+        g->n = std::max(g->n, n);
+        user_arc_off += csr->m;
+        vertex_off += n;
+    }
+    const int64_t m = static_cast<int64_t>(regular.size());
+    rarcs.resize(static_cast<size_t>(m));
+    g->m_stored = m;
+    if (m > 0) {
+        g->mean_len_regular = sum_regular / static_cast<double>(m);
+        g->mean_len_inverse = sum_inverse / static_cast<double>(m);
+        g->min_len_regular = min_regular;
+        g->max_len_regular = max_regular;
+    }
+
+    const auto upload = [&](auto** dst, const auto& src) -> int {
+        using T = std::remove_reference_t<decltype(src[0])>;
+        const size_t bytes = std::max<size_t>(1, src.size()) * sizeof(T);
+        NGX_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(dst), bytes));
+        if (!src.empty()) {
+            NGX_CUDA_TRY(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, g->stream));
+        }
+        return NGX_OK;
+    };
+    int rc = upload(&g->d_row_ptr, row_ptr);
+    if (rc == NGX_OK) rc = upload(&g->d_arcs_regular, regular);
+    if (rc == NGX_OK) rc = upload(&g->d_arcs_inverse, inverse);
+    if (rc == NGX_OK) rc = upload(&g->d_rrow_ptr, rrow_ptr);
+    if (rc == NGX_OK) rc = upload(&g->d_rarcs, rarcs);
+    if (rc == NGX_OK) {
+        const cudaError_t err = cudaStreamSynchronize(g->stream);
+        if (err != cudaSuccess) {
+            rc = cuda_fail(err, "ngx_graph_create: upload");
+        }
+    }
+    return finish(rc);
+}
+
 }  // namespace ngx
 
 using namespace ngx;
@@ -159,124 +335,10 @@ const char* ngx_version(void) {
 }
 
 int ngx_graph_create(const ngx_csr* csr, int device, ngx_graph** out) {
-    if (out == nullptr) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: out is NULL");
+    if (csr == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: csr is NULL");
     }
-    *out = nullptr;
-    if (const int rc = validate(csr); rc != NGX_OK) {
-        return rc;
-    }
-    int device_count = 0;
-    NGX_CUDA_TRY(cudaGetDeviceCount(&device_count));
-    if (device < 0 || device >= device_count) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: no CUDA device " + std::to_string(device));
-    }
-    NGX_CUDA_TRY(cudaSetDevice(device));
-    cudaDeviceProp prop{};
-    NGX_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
-    if (prop.major != 10) {
-        return fail(NGX_UNSUPPORTED, std::string("ngx_graph_create: the kernels are built for sm_100a (B200); device is ") + prop.name);
-    }
-
-    auto* g = new (std::nothrow) ngx_graph{};
-    if (g == nullptr) {
-        return fail(NGX_OUT_OF_MEMORY, "ngx_graph_create: host allocation failed");
-    }
-    g->device = device;
-    g->sm_count = prop.multiProcessorCount;
-    g->n = csr->n;
-    g->m_user = csr->m;
-
-    const auto finish = [&](int rc) -> int {
-        if (rc != NGX_OK) {
-            release(g);
-            return rc;
-        }
-        *out = g;
-        return NGX_OK;
-    };
-
-    if (cudaStreamCreateWithFlags(&g->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaHostAlloc(reinterpret_cast<void**>(&g->h_abort), sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
-        cudaHostGetDevicePointer(reinterpret_cast<void**>(&g->d_abort), g->h_abort, 0) != cudaSuccess) {
-        return finish(fail(NGX_CUDA_ERROR, "ngx_graph_create: stream or abort flag setup failed"));
-    }
-    *g->h_abort = 0;
-    g->stream = g->own_stream;
-
-    const int64_t n = csr->n;
-    // Host compaction: drop zero-weight arcs, keep the caller's arc index, precompute both metrics' lengths.
-    std::vector<int64_t> row_ptr(static_cast<size_t>(n) + 1, 0);
-    std::vector<Arc> regular;
-    std::vector<Arc> inverse;
-    regular.reserve(static_cast<size_t>(csr->m));
-    inverse.reserve(static_cast<size_t>(csr->m));
-    std::vector<int64_t> in_degree(static_cast<size_t>(n) + 1, 0);
-    double sum_regular = 0.0, sum_inverse = 0.0;
-    double min_regular = INFINITY, max_regular = 0.0;
-    for (int64_t u = 0; u < n; ++u) {
-        for (int64_t e = csr->row_ptr[u]; e < csr->row_ptr[u + 1]; ++e) {
-            const double a = std::fabs(csr->w[e]);
-            if (a == 0.0) {
-                continue;
-            }
-            const int32_t v = csr->col[e];
-            regular.push_back(Arc{ v, static_cast<int32_t>(e), a });
-            inverse.push_back(Arc{ v, static_cast<int32_t>(e), 1.0 / a });
-            sum_regular += a;
-            sum_inverse += 1.0 / a;
-            min_regular = std::min(min_regular, a);
-            max_regular = std::max(max_regular, a);
-            in_degree[static_cast<size_t>(v) + 1] += 1;
-        }
-        row_ptr[static_cast<size_t>(u) + 1] = static_cast<int64_t>(regular.size());
-        g->max_out_degree = std::max(g->max_out_degree, row_ptr[static_cast<size_t>(u) + 1] - row_ptr[static_cast<size_t>(u)]);
-    }
-    const int64_t m = static_cast<int64_t>(regular.size());
-    g->m_stored = m;
-    if (m > 0) {
-        g->mean_len_regular = sum_regular / static_cast<double>(m);
-        g->mean_len_inverse = sum_inverse / static_cast<double>(m);
-        g->min_len_regular = min_regular;
-        g->max_len_regular = max_regular;
-    }
-
-    // Reverse CSR by counting sort over targets; within a target, in-arcs keep ascending source order.
-    std::vector<int64_t> rrow_ptr(static_cast<size_t>(n) + 1, 0);
-    for (int64_t v = 0; v < n; ++v) {
-        rrow_ptr[static_cast<size_t>(v) + 1] = rrow_ptr[static_cast<size_t>(v)] + in_degree[static_cast<size_t>(v) + 1];
-    }
-    std::vector<Arc> rarcs(static_cast<size_t>(m));
-    std::vector<int64_t> fill(rrow_ptr.begin(), rrow_ptr.end() - 1);
-    for (int64_t u = 0; u < n; ++u) {
-        for (int64_t e = row_ptr[static_cast<size_t>(u)]; e < row_ptr[static_cast<size_t>(u) + 1]; ++e) {
-            const Arc& a = regular[static_cast<size_t>(e)];
-            // the reverse record keeps the arc's index in the stored forward CSR (its caller index is arcs[e].id)
-            rarcs[static_cast<size_t>(fill[static_cast<size_t>(a.col)]++)] = Arc{ static_cast<int32_t>(u), static_cast<int32_t>(e), a.len };
-        }
-    }
-
-    const auto upload = [&](auto** dst, const auto& src) -> int {
-        using T = std::remove_reference_t<decltype(src[0])>;
-        const size_t bytes = std::max<size_t>(1, src.size()) * sizeof(T);
-        NGX_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(dst), bytes));
-        if (!src.empty()) {
-            NGX_CUDA_TRY(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, g->stream));
-        }
-        return NGX_OK;
-    };
-    int rc = upload(&g->d_row_ptr, row_ptr);
-    if (rc == NGX_OK) rc = upload(&g->d_arcs_regular, regular);
-    if (rc == NGX_OK) rc = upload(&g->d_arcs_inverse, inverse);
-    if (rc == NGX_OK) rc = upload(&g->d_rrow_ptr, rrow_ptr);
-    if (rc == NGX_OK) rc = upload(&g->d_rarcs, rarcs);
-    if (rc == NGX_OK) {
-        const cudaError_t err = cudaStreamSynchronize(g->stream);
-        if (err != cudaSuccess) {
-            rc = cuda_fail(err, "ngx_graph_create: upload");
-        }
-    }
-    return finish(rc);
+    return create_graphs(csr, 1, device, out);
 }
 
 void ngx_graph_destroy(ngx_graph* graph) { release(graph); }
@@ -285,7 +347,7 @@ int ngx_graph_size(const ngx_graph* graph, int64_t* n, int64_t* m) {
     if (graph == nullptr) {
         return fail(NGX_INVALID_ARGUMENT, "ngx_graph_size: graph is NULL");
     }
-    if (n != nullptr) *n = graph->n;
+    if (n != nullptr) *n = graph->n_total;
     if (m != nullptr) *m = graph->m_user;
     return NGX_OK;
 }

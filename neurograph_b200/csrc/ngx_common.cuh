@@ -30,6 +30,48 @@ struct DeviceCsr {
     const Arc* arcs;         // m
 };
 
+// One graph of a batch: its slice of the concatenated CSR arrays, its sources and outputs. A single-graph run is a
+// batch of one.
+struct GraphDesc {
+    int64_t n;            // vertices (local ids 0..n-1)
+    int64_t m;            // stored arcs
+    int64_t row_off;      // start of the graph's n + 1 row offsets (forward and reverse CSR); values are global arc indices
+    int64_t src_off;      // start of the graph's sources in `sources` and in the per-source outputs
+    int64_t num_sources;
+    int64_t bc_off;       // start of the graph's vertices in the betweenness output
+    double delta;         // bucket width
+};
+
+// A unit of work of the persistent kernel: one tile of up to 32 sources of one graph.
+struct WorkItem {
+    int32_t graph;
+    int32_t tile;
+};
+
+// What a tile computes after its distances are final.
+enum TileMode : int { kModeApsp = 0, kModeBrandes = 1, kModeGrad = 2 };
+
+// Per-graph launch counters (unsigned 64-bit words, kCounterCount per graph).
+enum Counter : int {
+    kUnreachable = 0,
+    kReachedPairs = 1,
+    kTraversedArcs = 2,
+    kHistOverflow = 3,
+    kDiameterBits = 4,
+    kIterations = 5,   // near iterations (phases) over all tiles
+    kExpansions = 6,   // vertex expansions (one warp pass over a vertex's arcs)
+    kLaneExpansions = 7,  // (vertex, source) expansions; kLaneExpansions / kExpansions = sources sharing one arc pass
+    kCyclesSssp = 8,      // SM cycles spent per phase, summed over CTAs (thread 0 between barriers)
+    kCyclesCount = 9,
+    kCyclesSigma = 10,
+    kCyclesDelta = 11,
+    kCyclesEpilogue = 12,
+    kDagLevels = 13,      // Kahn levels of the shortest-path DAG, summed over tiles (Brandes / adjoint)
+    kDagEntries = 14,     // (vertex, level) entries of the Kahn level lists, summed over tiles
+    kDagScanTiles = 15,   // tiles whose DAG overflowed the successor lists (arc-scanning passes used)
+    kCounterCount = 16
+};
+
 // Error codes written by kernels into a device flag (first writer wins).
 enum DeviceError : int { kDevOk = 0, kDevTimeout = 1, kDevAborted = 2 };
 

@@ -8,15 +8,34 @@
 
 #include "ngx_common.cuh"
 
+namespace ngx {
+// Host view of one graph of a handle (a single-graph handle holds one; a batch handle holds many, concatenated).
+struct GraphPart {
+    int64_t n = 0;
+    int64_t m_user = 0;         // the caller's arcs (zero weights included)
+    int64_t m_stored = 0;       // device arcs (zero weights dropped)
+    int64_t row_off = 0;        // start of its n + 1 row offsets in the concatenated row_ptr arrays
+    int64_t user_arc_off = 0;   // start of its caller arcs in the concatenated arc numbering (gradients)
+    int64_t vertex_off = 0;     // start of its vertices in concatenated per-vertex outputs (betweenness)
+    double mean_len_regular = 1.0;
+    double mean_len_inverse = 1.0;
+};
+}  // namespace ngx
+
 struct ngx_graph {
     int device = 0;
     int sm_count = 0;
     cudaStream_t stream = nullptr;        // the stream all work of the graph is issued on
     cudaStream_t own_stream = nullptr;    // created with the graph; `stream` points here unless the caller set one
 
-    int64_t n = 0;
-    int64_t m_user = 0;    // arcs in the caller's CSR (zero weights included)
+    int64_t n = 0;         // vertices of the largest graph (workspace slots are sized for it)
+    int64_t n_total = 0;   // vertices of all graphs
+    int64_t m_user = 0;    // arcs in the caller's CSRs (zero weights included)
     int64_t m_stored = 0;  // arcs on the device (zero weights dropped)
+    std::vector<ngx::GraphPart> parts;  // one per graph
+    // batch work items (graph, tile) in scheduling order, on the device; built by ngx_batch_create
+    void* d_items = nullptr;
+    int64_t num_items = 0;
 
     // Forward CSR over stored arcs; two arc arrays, one per metric (|w| and 1/|w|).
     int64_t* d_row_ptr = nullptr;
@@ -42,6 +61,17 @@ struct ngx_graph {
     void* d_workspace = nullptr;
     size_t workspace_bytes = 0;
 
+    // CUDA graph of the last batch run (kernel + output resets), replayed while the run's configuration is unchanged
+    void* graph_exec = nullptr;  // cudaGraphExec_t
+    uint64_t graph_key = 0;
+    void* d_persistent = nullptr;  // output buffers the captured graph writes
+    size_t persistent_bytes = 0;
+
+    // bucket width per size class (floor(log2 n)), as a multiple of each graph's mean arc length (ngx_batch_autotune)
+    double class_scale[64] = {};
+    // stored forward index of each caller arc (-1 for zero weights), for ngx_graph_update_weights
+    std::vector<int32_t> stored_of_user;
+
     ngx::DeviceCsr csr(int metric) const {
         return ngx::DeviceCsr{ n, m_stored, d_row_ptr, metric == NGX_METRIC_INVERSE ? d_arcs_inverse : d_arcs_regular };
     }
@@ -49,6 +79,9 @@ struct ngx_graph {
 };
 
 namespace ngx {
+
+// Validates and uploads `count` CSRs into one handle (concatenated device CSR + reverse CSR).
+int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** out);
 
 // Grows the graph's cached workspace to at least `bytes`.
 int ensure_workspace(ngx_graph* g, size_t bytes);

@@ -15,16 +15,32 @@ constexpr int64_t kMaxHistBins = 16384;
 
 // Device buffers of one run's reduced outputs, carved from one allocation.
 struct RunOutputs {
-    unsigned long long* acc = nullptr;       // 2 * kAccDigits: exact sums of d and of 1/d
-    unsigned long long* counters = nullptr;  // kCounterCount
-    unsigned long long* hist = nullptr;
+    unsigned long long* acc = nullptr;       // per graph 2 * kAccDigits: exact sums of d and of 1/d
+    unsigned long long* counters = nullptr;  // per graph kCounterCount
+    unsigned long long* hist = nullptr;      // per graph hist_bins
+    GraphDesc* graphs = nullptr;             // the run's graph table
+    int32_t* sources = nullptr;              // all graphs' sources, graph after graph
     double* src_f64 = nullptr;               // 3 * S: per-source sum, max, inverse sum
     unsigned long long* src_u64 = nullptr;   // 2 * S: per-source unreachable, traversed arcs
     double* rows = nullptr;                  // S * n distance rows, when requested
     int* error = nullptr;
     unsigned long long* tile_counter = nullptr;
     void* block = nullptr;
+    bool owned = true;                       // false: the graph's persistent buffer (CUDA graph replays)
     size_t bytes = 0;
+    size_t zeroed_bytes = 0;                 // leading bytes (accumulators, counters, flags) reset before each run
+    int64_t num_graphs = 0;
+    int64_t num_sources = 0;
+};
+
+// What one launch covers: a graph table and sources already in the outputs block, and the work items.
+struct TileJob {
+    int64_t num_graphs = 1;
+    int64_t num_items = 0;             // (graph, tile) work items
+    const WorkItem* d_items = nullptr; // nullptr: tile t of graph 0
+    int64_t num_sources = 0;
+    int64_t n_max = 0;                 // largest graph (workspace slot size)
+    double plain_delta = 1.0;          // bucket width of the plain form (single graph)
 };
 
 // Device buffers of the DAG passes: per-vertex betweenness and per-arc gradients in 128-bit fixed point.
@@ -40,12 +56,15 @@ struct DagOutputs {
 int check_opts(const ngx_graph* g, const ngx_apsp_opts* opts);
 int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, double* rows, int tile_mode, DagOutputs* extra);
 int prepare_sources(const ngx_graph* g, const ngx_apsp_opts* opts, std::vector<int32_t>& sources);
-double pick_delta(const ngx_graph* g, int metric, double requested);
-int alloc_outputs(ngx_graph* g, int64_t num_sources, int64_t hist_bins, bool want_rows, RunOutputs& o);
+double pick_delta(double mean_len, double requested, double scale);
+int alloc_outputs(ngx_graph* g, int64_t num_graphs, int64_t num_sources, int64_t hist_bins, bool want_rows, RunOutputs& o, bool persistent);
 void free_outputs(ngx_graph* g, RunOutputs& o);
 int device_error_status(int code);
-int auto_hist_max(ngx_graph* g, const ngx_apsp_opts* opts, const std::vector<int32_t>& sources, double* out);
-int collect(ngx_graph* g, const RunOutputs& o, int64_t num_sources, int64_t hist_bins, double hist_max, ngx_apsp_result* r);
+int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const TileJob& job, int64_t hist_bins, double hist_max, RunOutputs& o,
+                 DagOutputs* extra, float* kernel_ms, bool synchronous);
+int read_totals(ngx_graph* g, const RunOutputs& o, std::vector<unsigned long long>& acc, std::vector<unsigned long long>& counters);
+int collect_graph(ngx_graph* g, const RunOutputs& o, const unsigned long long* acc_all, const unsigned long long* counters_all, int64_t gi,
+                  int64_t src_off, int64_t num_sources, int64_t hist_bins, double hist_max, ngx_apsp_result* r);
 void clear_result_totals(ngx_apsp_result* r);
 
 }  // namespace ngx

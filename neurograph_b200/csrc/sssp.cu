@@ -1,7 +1,8 @@
-// Host side of the all-sources APSP run: source tiling, workspace sizing, launch, result reduction.
+// Host side of the tile runs: source tiling, workspace sizing, launch, result reduction.
 //
 // Replaces AllPairsShortestPath::compute_apsp_impl's per-source loop (source/metrics/paths/AllPairsShortestPath.h:110-163)
-// and compute_apsp_impl_delta_stepping (:197-247) with one persistent launch over all source tiles.
+// and compute_apsp_impl_delta_stepping (:197-247) with one persistent launch over all source tiles, of one graph or of
+// a batch of graphs.
 
 #include <cuda_runtime.h>
 
@@ -22,6 +23,8 @@ namespace {
 constexpr int kBatchedUnroll = 4;
 constexpr int kPlainWarpsMax = 16;
 constexpr int kBatchedDefaultBlock = 384;
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 }  // namespace
 
 int prepare_sources(const ngx_graph* g, const ngx_apsp_opts* opts, std::vector<int32_t>& sources) {
@@ -46,12 +49,12 @@ int prepare_sources(const ngx_graph* g, const ngx_apsp_opts* opts, std::vector<i
     return NGX_OK;
 }
 
-double pick_delta(const ngx_graph* g, int metric, double requested) {
+double pick_delta(double mean_len, double requested, double scale) {
     if (requested > 0.0 && std::isfinite(requested)) {
         return requested;
     }
-    const double mean = metric == NGX_METRIC_INVERSE ? g->mean_len_inverse : g->mean_len_regular;
-    return mean > 0.0 && std::isfinite(mean) ? mean : 1.0;
+    const double base = mean_len > 0.0 && std::isfinite(mean_len) ? mean_len : 1.0;
+    return base * (scale > 0.0 ? scale : 1.0);
 }
 
 int check_opts(const ngx_graph* g, const ngx_apsp_opts* opts) {
@@ -73,42 +76,64 @@ int check_opts(const ngx_graph* g, const ngx_apsp_opts* opts) {
     return NGX_OK;
 }
 
-int alloc_outputs(ngx_graph* g, int64_t num_sources, int64_t hist_bins, bool want_rows, RunOutputs& o) {
+int alloc_outputs(ngx_graph* g, int64_t num_graphs, int64_t num_sources, int64_t hist_bins, bool want_rows, RunOutputs& o, bool persistent) {
     const size_t s = static_cast<size_t>(num_sources);
+    const size_t gcount = static_cast<size_t>(num_graphs);
     size_t off = 0;
     const auto take = [&](size_t bytes) {
         const size_t at = off;
-        off += (bytes + 255) & ~size_t(255);
+        off += align256(bytes);
         return at;
     };
-    const size_t a_acc = take(2 * kAccDigits * 8);
-    const size_t a_cnt = take(kCounterCount * 8);
+    const size_t a_acc = take(gcount * 2 * kAccDigits * 8);
+    const size_t a_cnt = take(gcount * kCounterCount * 8);
     const size_t a_err = take(8);
     const size_t a_tile = take(8);
-    const size_t a_hist = take(static_cast<size_t>(std::max<int64_t>(hist_bins, 1)) * 8);
+    const size_t a_hist = take(gcount * static_cast<size_t>(std::max<int64_t>(hist_bins, 1)) * 8);
+    const size_t zeroed = off;  // everything above starts at zero
+    const size_t a_graphs = take(gcount * sizeof(GraphDesc));
+    const size_t a_sources = take(std::max<size_t>(s, 1) * 4);
     const size_t a_f64 = take(3 * s * 8);
     const size_t a_u64 = take(2 * s * 8);
     const size_t a_rows = want_rows ? take(s * static_cast<size_t>(g->n) * 8) : 0;
-    NGX_CUDA_TRY(cudaMallocAsync(&o.block, off, g->stream));
+    if (persistent) {
+        if (off > g->persistent_bytes) {
+            NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            cudaFree(g->d_persistent);
+            g->d_persistent = nullptr;
+            g->persistent_bytes = 0;
+            NGX_CUDA_TRY(cudaMalloc(&g->d_persistent, off));
+            g->persistent_bytes = off;
+        }
+        o.block = g->d_persistent;
+        o.owned = false;
+    } else {
+        NGX_CUDA_TRY(cudaMallocAsync(&o.block, off, g->stream));
+        o.owned = true;
+    }
     o.bytes = off;
+    o.zeroed_bytes = zeroed;
     char* b = static_cast<char*>(o.block);
     o.acc = reinterpret_cast<unsigned long long*>(b + a_acc);
     o.counters = reinterpret_cast<unsigned long long*>(b + a_cnt);
     o.error = reinterpret_cast<int*>(b + a_err);
     o.tile_counter = reinterpret_cast<unsigned long long*>(b + a_tile);
     o.hist = reinterpret_cast<unsigned long long*>(b + a_hist);
+    o.graphs = reinterpret_cast<GraphDesc*>(b + a_graphs);
+    o.sources = reinterpret_cast<int32_t*>(b + a_sources);
     o.src_f64 = reinterpret_cast<double*>(b + a_f64);
     o.src_u64 = reinterpret_cast<unsigned long long*>(b + a_u64);
     o.rows = want_rows ? reinterpret_cast<double*>(b + a_rows) : nullptr;
-    NGX_CUDA_TRY(cudaMemsetAsync(o.block, 0, a_f64, g->stream));
+    o.num_graphs = num_graphs;
+    o.num_sources = num_sources;
     return NGX_OK;
 }
 
 void free_outputs(ngx_graph* g, RunOutputs& o) {
-    if (o.block != nullptr) {
+    if (o.block != nullptr && o.owned) {
         cudaFreeAsync(o.block, g->stream);
-        o.block = nullptr;
     }
+    o.block = nullptr;
 }
 
 int device_error_status(int code) {
@@ -130,16 +155,20 @@ const void* tile_kernel_for_block(int block) {
     }
 }
 
-// One persistent launch over `sources` (tile order): SSSP with the fused APSP epilogue, plus Brandes or the adjoint
-// when `tile_mode` asks for them (batched form only). Leaves reduced outputs in `o` and the DAG outputs in `extra`.
-int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const int32_t* d_sources, int64_t num_sources, int64_t hist_bins,
-                 double hist_max, RunOutputs& o, DagOutputs* extra, float* kernel_ms) {
+int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const TileJob& job, int64_t hist_bins, double hist_max, RunOutputs& o,
+                 DagOutputs* extra, float* kernel_ms, bool synchronous) {
     const bool batched = opts->mode == NGX_MODE_BATCHED || tile_mode != kModeApsp;
     const int width = batched ? kTile : 1;
-    const int64_t num_tiles = batched ? (num_sources + kTile - 1) / kTile : num_sources;
+    const int64_t num_tiles = batched ? job.num_items : job.num_sources;
     const int block = opts->block_threads > 0 ? opts->block_threads : (batched ? kBatchedDefaultBlock : 512);
     const size_t acc_bytes = static_cast<size_t>(2) * (batched ? kTile : kPlainWarpsMax) * kAccDigits * 8;
     const size_t smem = acc_bytes + static_cast<size_t>(hist_bins) * 4;
+    if (!batched && job.num_graphs != 1) {
+        return fail(NGX_UNSUPPORTED, "the plain form runs one graph at a time");
+    }
+    if (num_tiles == 0) {
+        return NGX_OK;
+    }
 
     const void* kernel = reinterpret_cast<const void*>(&sssp_plain_kernel);
     if (batched) {
@@ -159,7 +188,8 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const i
     if (opts->ctas_per_sm > 0) {
         per_sm = std::min(per_sm, opts->ctas_per_sm);
     }
-    const size_t slot_bytes = sssp_slot_bytes(g->n, width) + (tile_mode != kModeApsp ? brandes_slot_bytes(g->n, tile_mode == kModeGrad) : 0);
+    const int64_t n = job.n_max;
+    const size_t slot_bytes = sssp_slot_bytes(n, width) + (tile_mode != kModeApsp ? brandes_slot_bytes(n, tile_mode == kModeGrad) : 0);
     const size_t budget = workspace_budget(g);
     int64_t slots = std::min<int64_t>(num_tiles, static_cast<int64_t>(g->sm_count) * per_sm);
     slots = std::min<int64_t>(slots, static_cast<int64_t>(budget / slot_bytes));
@@ -169,14 +199,16 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const i
     if (const int rc = ensure_workspace(g, static_cast<size_t>(slots) * slot_bytes); rc != NGX_OK) {
         return rc;
     }
-    const int64_t n = g->n;
     char* ws = static_cast<char*>(g->d_workspace);
     SsspParams p{};
     p.g = g->csr(opts->metric);
-    p.sources = d_sources;
-    p.num_sources = num_sources;
+    p.g.n = n;
+    p.sources = o.sources;
+    p.num_sources = job.num_sources;
     p.num_tiles = num_tiles;
-    p.delta = pick_delta(g, opts->metric, opts->delta);
+    p.delta = job.plain_delta;
+    p.graphs = o.graphs;
+    p.items = job.d_items;
     p.max_iterations = opts->max_iterations > 0 ? opts->max_iterations : static_cast<unsigned long long>(4 * n + 64);
     p.tile_counter = o.tile_counter;
     p.error = o.error;
@@ -236,28 +268,29 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const i
     p.out.hist_max = hist_max;
     p.out.hist_width = hist_bins > 0 ? hist_max / static_cast<double>(hist_bins) : 0.0;
     p.out.src_sum = o.src_f64;
-    p.out.src_max = o.src_f64 + num_sources;
-    p.out.src_inv = o.src_f64 + 2 * num_sources;
+    p.out.src_max = o.src_f64 + job.num_sources;
+    p.out.src_inv = o.src_f64 + 2 * job.num_sources;
     p.out.src_unreach = o.src_u64;
-    p.out.src_arcs = o.src_u64 + num_sources;
+    p.out.src_arcs = o.src_u64 + job.num_sources;
     p.out.rows = o.rows;
 
-    cudaEvent_t start, stop;
-    NGX_CUDA_TRY(cudaEventCreate(&start));
-    NGX_CUDA_TRY(cudaEventCreate(&stop));
-    cudaEventRecord(start, g->stream);
+    cudaEvent_t start = nullptr, stop = nullptr;
+    if (synchronous) {
+        NGX_CUDA_TRY(cudaEventCreate(&start));
+        NGX_CUDA_TRY(cudaEventCreate(&stop));
+        cudaEventRecord(start, g->stream);
+    }
+    cudaError_t err = cudaSuccess;
     if (batched) {
         void* args[] = { &p, &bp };
-        const cudaError_t launch = cudaLaunchKernel(kernel, dim3(static_cast<unsigned>(slots)), dim3(block), args, smem, g->stream);
-        if (launch != cudaSuccess) {
-            cudaEventDestroy(start);
-            cudaEventDestroy(stop);
-            return cuda_fail(launch, "sssp kernel launch");
-        }
+        err = cudaLaunchKernel(kernel, dim3(static_cast<unsigned>(slots)), dim3(block), args, smem, g->stream);
     } else {
         sssp_plain_kernel<<<static_cast<unsigned>(slots), block, smem, g->stream>>>(p);
+        err = cudaGetLastError();
     }
-    cudaError_t err = cudaGetLastError();
+    if (!synchronous) {
+        return err == cudaSuccess ? NGX_OK : cuda_fail(err, "tile kernel launch");
+    }
     cudaEventRecord(stop, g->stream);
     if (err == cudaSuccess) {
         err = cudaEventSynchronize(stop);
@@ -269,7 +302,7 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const i
     cudaEventDestroy(start);
     cudaEventDestroy(stop);
     if (err != cudaSuccess) {
-        return cuda_fail(err, "sssp kernel");
+        return cuda_fail(err, "tile kernel");
     }
     if (kernel_ms != nullptr) {
         *kernel_ms += ms;
@@ -279,42 +312,24 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const i
     return device_error_status(code);
 }
 
-// Histogram bound when the caller gives none: 1.5 x the largest eccentricity of up to one tile of sources spread
-// over the requested list (plus the overflow count for anything beyond it).
-int auto_hist_max(ngx_graph* g, const ngx_apsp_opts* opts, const std::vector<int32_t>& sources, double* out) {
-    const int64_t k = std::min<int64_t>(kTile, static_cast<int64_t>(sources.size()));
-    std::vector<int32_t> sample(static_cast<size_t>(k));
-    for (int64_t i = 0; i < k; ++i) {
-        sample[static_cast<size_t>(i)] = sources[static_cast<size_t>(i * static_cast<int64_t>(sources.size()) / k)];
+void clear_result_totals(ngx_apsp_result* r) {
+    r->sum_distances = r->sum_inverse = r->diameter = 0.0;
+    r->unreachable = r->reached_pairs = r->traversed_arcs = r->hist_overflow = 0;
+    r->hist_max = 0.0;
+    r->cpl = r->efficiency = 0.0;
+    r->kernel_ms = 0.0;
+    r->phases = r->expansions = r->lane_expansions = r->dag_levels = r->dag_entries = r->dag_scan_tiles = 0;
+    for (int i = 0; i < 5; ++i) {
+        r->phase_cycles[i] = 0;
     }
-    int32_t* d_sample = nullptr;
-    NGX_CUDA_TRY(cudaMallocAsync(&d_sample, sizeof(int32_t) * static_cast<size_t>(k), g->stream));
-    NGX_CUDA_TRY(cudaMemcpyAsync(d_sample, sample.data(), sizeof(int32_t) * static_cast<size_t>(k), cudaMemcpyHostToDevice, g->stream));
-    RunOutputs o;
-    int rc = alloc_outputs(g, k, 0, false, o);
-    ngx_apsp_opts sample_opts = *opts;
-    sample_opts.mode = NGX_MODE_BATCHED;
-    if (rc == NGX_OK) {
-        rc = launch_tiles(g, &sample_opts, kModeApsp, d_sample, k, 0, 0.0, o, nullptr, nullptr);
-    }
-    unsigned long long bits = 0;
-    if (rc == NGX_OK && cudaMemcpy(&bits, o.counters + kDiameterBits, 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
-        rc = fail(NGX_CUDA_ERROR, "copying the sampled eccentricity");
-    }
-    free_outputs(g, o);
-    cudaFreeAsync(d_sample, g->stream);
-    double ecc = 0.0;
-    std::memcpy(&ecc, &bits, sizeof(double));
-    *out = ecc > 0.0 ? 1.5 * ecc : 1.0;
-    return rc;
 }
 
-int collect(ngx_graph* g, const RunOutputs& o, int64_t num_sources, int64_t hist_bins, double hist_max, ngx_apsp_result* r) {
+// Reduces graph `gi`'s accumulators and counters (host copies) into a result; copies its optional device outputs.
+int collect_graph(ngx_graph* g, const RunOutputs& o, const unsigned long long* acc_all, const unsigned long long* counters_all, int64_t gi,
+                  int64_t src_off, int64_t num_sources, int64_t hist_bins, double hist_max, ngx_apsp_result* r) {
     unsigned long long acc[2 * kAccDigits];
-    unsigned long long counters[kCounterCount];
-    NGX_CUDA_TRY(cudaMemcpyAsync(acc, o.acc, sizeof(acc), cudaMemcpyDeviceToHost, g->stream));
-    NGX_CUDA_TRY(cudaMemcpyAsync(counters, o.counters, sizeof(counters), cudaMemcpyDeviceToHost, g->stream));
-    NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    std::memcpy(acc, acc_all + gi * 2 * kAccDigits, sizeof(acc));
+    const unsigned long long* counters = counters_all + gi * kCounterCount;
     acc_normalize(acc);
     acc_normalize(acc + kAccDigits);
     r->sum_distances = acc_round_normalized(acc);
@@ -334,38 +349,92 @@ int collect(ngx_graph* g, const RunOutputs& o, int64_t num_sources, int64_t hist
     for (int i = 0; i < 5; ++i) {
         r->phase_cycles[i] = counters[kCyclesSssp + i];
     }
+    // AllPairsShortestPath.h:154-158: both averages are over the R reached ordered pairs (0 / 0 gives NaN, as there)
     r->cpl = r->sum_distances / static_cast<double>(r->reached_pairs);
     r->efficiency = r->sum_inverse / static_cast<double>(r->reached_pairs);
     const size_t s = static_cast<size_t>(num_sources);
+    const size_t total = static_cast<size_t>(o.num_sources);
+    const size_t at = static_cast<size_t>(src_off);
     if (r->hist != nullptr && hist_bins > 0) {
-        NGX_CUDA_TRY(cudaMemcpyAsync(r->hist, o.hist, static_cast<size_t>(hist_bins) * 8, cudaMemcpyDeviceToHost, g->stream));
+        NGX_CUDA_TRY(cudaMemcpyAsync(r->hist, o.hist + gi * hist_bins, static_cast<size_t>(hist_bins) * 8, cudaMemcpyDeviceToHost, g->stream));
     }
     if (s > 0) {
-        if (r->src_sum != nullptr) NGX_CUDA_TRY(cudaMemcpyAsync(r->src_sum, o.src_f64, s * 8, cudaMemcpyDeviceToHost, g->stream));
-        if (r->src_max != nullptr) NGX_CUDA_TRY(cudaMemcpyAsync(r->src_max, o.src_f64 + s, s * 8, cudaMemcpyDeviceToHost, g->stream));
-        if (r->src_sum_inverse != nullptr) NGX_CUDA_TRY(cudaMemcpyAsync(r->src_sum_inverse, o.src_f64 + 2 * s, s * 8, cudaMemcpyDeviceToHost, g->stream));
-        if (r->src_unreachable != nullptr) NGX_CUDA_TRY(cudaMemcpyAsync(r->src_unreachable, o.src_u64, s * 8, cudaMemcpyDeviceToHost, g->stream));
-        if (r->src_arcs != nullptr) NGX_CUDA_TRY(cudaMemcpyAsync(r->src_arcs, o.src_u64 + s, s * 8, cudaMemcpyDeviceToHost, g->stream));
+        if (r->src_sum != nullptr) NGX_CUDA_TRY(cudaMemcpyAsync(r->src_sum, o.src_f64 + at, s * 8, cudaMemcpyDeviceToHost, g->stream));
+        if (r->src_max != nullptr) NGX_CUDA_TRY(cudaMemcpyAsync(r->src_max, o.src_f64 + total + at, s * 8, cudaMemcpyDeviceToHost, g->stream));
+        if (r->src_sum_inverse != nullptr) {
+            NGX_CUDA_TRY(cudaMemcpyAsync(r->src_sum_inverse, o.src_f64 + 2 * total + at, s * 8, cudaMemcpyDeviceToHost, g->stream));
+        }
+        if (r->src_unreachable != nullptr) NGX_CUDA_TRY(cudaMemcpyAsync(r->src_unreachable, o.src_u64 + at, s * 8, cudaMemcpyDeviceToHost, g->stream));
+        if (r->src_arcs != nullptr) NGX_CUDA_TRY(cudaMemcpyAsync(r->src_arcs, o.src_u64 + total + at, s * 8, cudaMemcpyDeviceToHost, g->stream));
     }
+    return NGX_OK;
+}
+
+int read_totals(ngx_graph* g, const RunOutputs& o, std::vector<unsigned long long>& acc, std::vector<unsigned long long>& counters) {
+    acc.resize(static_cast<size_t>(o.num_graphs) * 2 * kAccDigits);
+    counters.resize(static_cast<size_t>(o.num_graphs) * kCounterCount);
+    NGX_CUDA_TRY(cudaMemcpyAsync(acc.data(), o.acc, acc.size() * 8, cudaMemcpyDeviceToHost, g->stream));
+    NGX_CUDA_TRY(cudaMemcpyAsync(counters.data(), o.counters, counters.size() * 8, cudaMemcpyDeviceToHost, g->stream));
     NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
     return NGX_OK;
 }
 
-void clear_result_totals(ngx_apsp_result* r) {
-    r->sum_distances = r->sum_inverse = r->diameter = 0.0;
-    r->unreachable = r->reached_pairs = r->traversed_arcs = r->hist_overflow = 0;
-    r->hist_max = 0.0;
-    r->cpl = r->efficiency = 0.0;
-    r->kernel_ms = 0.0;
-    r->phases = r->expansions = r->lane_expansions = r->dag_levels = r->dag_entries = r->dag_scan_tiles = 0;
-    for (int i = 0; i < 5; ++i) {
-        r->phase_cycles[i] = 0;
+// One single-graph run of `sources` (graph 0 of the handle).
+int run_sources(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const std::vector<int32_t>& sources, int64_t hist_bins, double hist_max,
+                bool want_rows, DagOutputs* extra, RunOutputs& o, float* ms) {
+    const int64_t num_sources = static_cast<int64_t>(sources.size());
+    if (const int rc = alloc_outputs(g, 1, num_sources, hist_bins, want_rows, o, false); rc != NGX_OK) {
+        return rc;
     }
+    const GraphPart& part = g->parts[0];
+    const double delta = pick_delta(opts->metric == NGX_METRIC_INVERSE ? part.mean_len_inverse : part.mean_len_regular, opts->delta, 1.0);
+    const GraphDesc desc{ part.n, part.m_stored, part.row_off, 0, num_sources, part.vertex_off, delta };
+    NGX_CUDA_TRY(cudaMemsetAsync(o.block, 0, o.zeroed_bytes, g->stream));
+    NGX_CUDA_TRY(cudaMemcpyAsync(o.graphs, &desc, sizeof(desc), cudaMemcpyHostToDevice, g->stream));
+    NGX_CUDA_TRY(cudaMemcpyAsync(o.sources, sources.data(), sizeof(int32_t) * sources.size(), cudaMemcpyHostToDevice, g->stream));
+    TileJob job;
+    job.num_graphs = 1;
+    job.num_items = (num_sources + kTile - 1) / kTile;
+    job.d_items = nullptr;
+    job.num_sources = num_sources;
+    job.n_max = part.n;
+    job.plain_delta = delta;
+    return launch_tiles(g, opts, tile_mode, job, hist_bins, hist_max, o, extra, ms, true);
+}
+
+// Histogram bound when the caller gives none: 1.5 x the largest eccentricity of up to one tile of sources spread
+// over the requested list (plus the overflow count for anything beyond it).
+int auto_hist_max(ngx_graph* g, const ngx_apsp_opts* opts, const std::vector<int32_t>& sources, double* out) {
+    const int64_t k = std::min<int64_t>(kTile, static_cast<int64_t>(sources.size()));
+    std::vector<int32_t> sample(static_cast<size_t>(k));
+    for (int64_t i = 0; i < k; ++i) {
+        sample[static_cast<size_t>(i)] = sources[static_cast<size_t>(i * static_cast<int64_t>(sources.size()) / k)];
+    }
+    ngx_apsp_opts sample_opts = *opts;
+    sample_opts.mode = NGX_MODE_BATCHED;
+    RunOutputs o;
+    int rc = run_sources(g, &sample_opts, kModeApsp, sample, 0, 0.0, false, nullptr, o, nullptr);
+    unsigned long long bits = 0;
+    if (rc == NGX_OK) {
+        std::vector<unsigned long long> acc, counters;
+        rc = read_totals(g, o, acc, counters);
+        if (rc == NGX_OK) {
+            bits = counters[kDiameterBits];
+        }
+    }
+    free_outputs(g, o);
+    double ecc = 0.0;
+    std::memcpy(&ecc, &bits, sizeof(double));
+    *out = ecc > 0.0 ? 1.5 * ecc : 1.0;
+    return rc;
 }
 
 int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, double* rows, int tile_mode, DagOutputs* extra) {
     if (const int rc = check_opts(g, opts); rc != NGX_OK) {
         return rc;
+    }
+    if (g->parts.size() != 1) {
+        return fail(NGX_INVALID_ARGUMENT, "this handle holds a batch of graphs: use ngx_batch_run");
     }
     NGX_CUDA_TRY(cudaSetDevice(g->device));
     *g->h_abort = 0;
@@ -388,27 +457,26 @@ int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, d
             return rc;
         }
     }
-    int32_t* d_sources = nullptr;
-    NGX_CUDA_TRY(cudaMallocAsync(&d_sources, sizeof(int32_t) * sources.size(), g->stream));
-    NGX_CUDA_TRY(cudaMemcpyAsync(d_sources, sources.data(), sizeof(int32_t) * sources.size(), cudaMemcpyHostToDevice, g->stream));
     RunOutputs o;
-    int rc = alloc_outputs(g, num_sources, hist_bins, rows != nullptr, o);
     float ms = 0.0f;
+    int rc = run_sources(g, opts, tile_mode, sources, hist_bins, hist_max, rows != nullptr, extra, o, &ms);
     if (rc == NGX_OK) {
-        rc = launch_tiles(g, opts, tile_mode, d_sources, num_sources, hist_bins, hist_max, o, extra, &ms);
-    }
-    if (rc == NGX_OK) {
-        rc = collect(g, o, num_sources, hist_bins, hist_max, r);
+        std::vector<unsigned long long> acc, counters;
+        rc = read_totals(g, o, acc, counters);
+        if (rc == NGX_OK) {
+            rc = collect_graph(g, o, acc.data(), counters.data(), 0, 0, num_sources, hist_bins, hist_max, r);
+        }
         r->kernel_ms = ms;
     }
     if (rc == NGX_OK && rows != nullptr) {
-        const cudaError_t err = cudaMemcpy(rows, o.rows, static_cast<size_t>(num_sources) * static_cast<size_t>(g->n) * 8, cudaMemcpyDeviceToHost);
+        const cudaError_t err = cudaMemcpyAsync(rows, o.rows, static_cast<size_t>(num_sources) * static_cast<size_t>(g->n) * 8, cudaMemcpyDeviceToHost,
+                                                g->stream);
         if (err != cudaSuccess) {
             rc = cuda_fail(err, "copying distance rows");
         }
     }
+    cudaStreamSynchronize(g->stream);
     free_outputs(g, o);
-    cudaFreeAsync(d_sources, g->stream);
     cudaStreamSynchronize(g->stream);
     return rc;
 }
@@ -422,8 +490,8 @@ extern "C" {
 int ngx_apsp(ngx_graph* graph, const ngx_apsp_opts* opts, ngx_apsp_result* result) { return run_apsp(graph, opts, result, nullptr, kModeApsp, nullptr); }
 
 int ngx_sssp_rows(ngx_graph* graph, const ngx_apsp_opts* opts, double* rows) {
-    if (rows == nullptr) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_sssp_rows: rows is NULL");
+    if (rows == nullptr || opts == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_sssp_rows: opts or rows is NULL");
     }
     ngx_apsp_opts o = *opts;
     o.hist_bins = 0;

@@ -38,10 +38,10 @@ namespace ngx {
 constexpr unsigned kFullMask = 0xFFFFFFFFu;
 
 struct TileOutputs {
-    unsigned long long* acc_sum;    // kAccDigits: exact sum of distances over all sources
-    unsigned long long* acc_inv;    // kAccDigits: exact sum of 1/d
-    unsigned long long* counters;   // see Counter
-    unsigned long long* hist;       // hist_bins (or nullptr)
+    unsigned long long* acc_sum;    // per graph: kAccDigits words of the exact sum of distances, then kAccDigits for 1/d
+    unsigned long long* acc_inv;    // unused by the tile kernel (acc_sum + kAccDigits of each graph)
+    unsigned long long* counters;   // per graph: kCounterCount words (see Counter)
+    unsigned long long* hist;       // per graph: hist_bins words (or nullptr)
     int hist_bins;
     double hist_width;
     double hist_max;
@@ -53,32 +53,15 @@ struct TileOutputs {
     double* rows;                   // num_sources x n distance rows (or nullptr)
 };
 
-enum Counter : int {
-    kUnreachable = 0,
-    kReachedPairs = 1,
-    kTraversedArcs = 2,
-    kHistOverflow = 3,
-    kDiameterBits = 4,
-    kIterations = 5,   // near iterations (phases) over all tiles
-    kExpansions = 6,   // vertex expansions (one warp pass over a vertex's arcs)
-    kLaneExpansions = 7,  // (vertex, source) expansions; kLaneExpansions / kExpansions = sources sharing one arc pass
-    kCyclesSssp = 8,      // SM cycles spent per phase, summed over CTAs (thread 0 between barriers)
-    kCyclesCount = 9,
-    kCyclesSigma = 10,
-    kCyclesDelta = 11,
-    kCyclesEpilogue = 12,
-    kDagLevels = 13,      // Kahn levels of the shortest-path DAG, summed over tiles (Brandes / adjoint)
-    kDagEntries = 14,     // (vertex, level) entries of the Kahn level lists, summed over tiles
-    kDagScanTiles = 15,   // tiles whose DAG overflowed the successor lists (arc-scanning passes used)
-    kCounterCount = 16
-};
 
 struct SsspParams {
-    DeviceCsr g;
-    const int32_t* sources;        // tile order
+    DeviceCsr g;                   // concatenated CSR: row_ptr over all graphs' rows, arcs with graph-local targets; g.n = largest n
+    const int32_t* sources;        // tile order (graph-local ids)
     int64_t num_sources;
-    int64_t num_tiles;
+    int64_t num_tiles;             // work items
     double delta;
+    const GraphDesc* graphs;       // batch table (tile kernel)
+    const WorkItem* items;         // work items in scheduling order, or nullptr: tile t of graph 0
     unsigned long long max_iterations;  // per tile
     unsigned long long* tile_counter;
     int* error;
@@ -237,18 +220,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     const int lane = tid & 31;
     const int warp = tid >> 5;
     const int nwarps = blockDim.x >> 5;
-    const int64_t n = p.g.n;
+    const int64_t n_slot = p.g.n;  // every slot holds the largest graph of the batch
     const int64_t slot = blockIdx.x;
     unsigned long long expansions = 0, lane_expansions = 0;
 
-    unsigned long long* dist = p.ws_dist + slot * n * kTile;
-    uint32_t* pend0 = p.ws_pend + slot * 2 * n;
-    uint32_t* pend1 = pend0 + n;
-    uint32_t* far = p.ws_far + slot * n;
-    int32_t* q0 = p.ws_queue + slot * 2 * n;
-    int32_t* q1 = q0 + n;
-    uint32_t* stamp = p.ws_stamp + slot * n;
-    const int64_t nt = n * kTile;
+    unsigned long long* dist = p.ws_dist + slot * n_slot * kTile;
+    uint32_t* pend0 = p.ws_pend + slot * 2 * n_slot;
+    uint32_t* pend1 = pend0 + n_slot;
+    uint32_t* far = p.ws_far + slot * n_slot;
+    int32_t* q0 = p.ws_queue + slot * 2 * n_slot;
+    int32_t* q1 = q0 + n_slot;
+    uint32_t* stamp = p.ws_stamp + slot * n_slot;
+    const int64_t nt_slot = n_slot * kTile;
     double* sigma = nullptr;
     double* delta = nullptr;
     double* delta_g = nullptr;
@@ -261,20 +244,20 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     uint32_t* succ = nullptr;
     __shared__ unsigned long long s_part[kBlock + 1];
     if constexpr (kMode != kModeApsp) {
-        scnt = b.ws_scnt + slot * nt;
-        soff = b.ws_soff + slot * (nt + 1);
+        scnt = b.ws_scnt + slot * nt_slot;
+        soff = b.ws_soff + slot * (nt_slot + 1);
         succ = b.ws_succ + slot * b.succ_capacity;
-        for (int64_t i = tid; i < nt; i += blockDim.x) {
+        for (int64_t i = tid; i < nt_slot; i += blockDim.x) {
             scnt[i] = 0u;
         }
-        sigma = b.ws_sigma + slot * nt;
-        delta = b.ws_delta + slot * nt;
-        delta_g = kMode == kModeGrad ? b.ws_delta_g + slot * nt : nullptr;
-        cnt = b.ws_cnt + slot * nt;
-        lvl = b.ws_lvl + slot * nt;
-        list = b.ws_list + slot * nt;
-        loff = b.ws_loff + slot * (n + 2);
-        for (int64_t i = tid; i < nt; i += blockDim.x) {
+        sigma = b.ws_sigma + slot * nt_slot;
+        delta = b.ws_delta + slot * nt_slot;
+        delta_g = kMode == kModeGrad ? b.ws_delta_g + slot * nt_slot : nullptr;
+        cnt = b.ws_cnt + slot * nt_slot;
+        lvl = b.ws_lvl + slot * nt_slot;
+        list = b.ws_list + slot * nt_slot;
+        loff = b.ws_loff + slot * (n_slot + 2);
+        for (int64_t i = tid; i < nt_slot; i += blockDim.x) {
             sigma[i] = 0.0;
             delta[i] = 0.0;
             if constexpr (kMode == kModeGrad) {
@@ -285,10 +268,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         }
     }
 
-    for (int64_t i = tid; i < n * kTile; i += blockDim.x) {
+    for (int64_t i = tid; i < nt_slot; i += blockDim.x) {
         dist[i] = kInfBits;
     }
-    for (int64_t i = tid; i < n; i += blockDim.x) {
+    for (int64_t i = tid; i < n_slot; i += blockDim.x) {
         pend0[i] = 0u;
         pend1[i] = 0u;
         far[i] = 0u;
@@ -312,7 +295,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             s.qlen[0] = 0;
             s.qlen[1] = 0;
             s.cur = 0;
-            s.theta = p.delta;
             s.iterations = 0;
             s.overflow = 0;
         }
@@ -320,8 +302,24 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         if (s.stop != 0 || s.tile >= p.num_tiles) {
             break;
         }
-        const int64_t base = s.tile * kTile;
-        const int nsrc = static_cast<int>(p.num_sources - base < kTile ? p.num_sources - base : kTile);
+        // ---- the work item: tile `item.tile` of graph `item.graph`
+        const WorkItem item = p.items != nullptr ? p.items[s.tile] : WorkItem{ 0, static_cast<int32_t>(s.tile) };
+        const GraphDesc gd = p.graphs[item.graph];
+        const int64_t n = gd.n;
+        const int64_t nt = n * kTile;
+        const DeviceCsr g{ gd.n, gd.m, p.g.row_ptr + gd.row_off, p.g.arcs };
+        const DeviceCsr rg{ gd.n, gd.m, b.rg.row_ptr + gd.row_off, b.rg.arcs };
+        unsigned long long* const cnts = p.out.counters + static_cast<int64_t>(item.graph) * kCounterCount;
+        unsigned long long* const acc_sum_g = p.out.acc_sum + static_cast<int64_t>(item.graph) * 2 * kAccDigits;
+        unsigned long long* const acc_inv_g = acc_sum_g + kAccDigits;
+        unsigned long long* const hist_g = p.out.hist != nullptr ? p.out.hist + static_cast<int64_t>(item.graph) * p.out.hist_bins : nullptr;
+        unsigned long long* const bc_g = b.bc != nullptr ? b.bc + 2 * gd.bc_off : nullptr;
+        const int64_t tile_first = static_cast<int64_t>(item.tile) * kTile;
+        const int64_t base = gd.src_off + tile_first;
+        const int nsrc = static_cast<int>(gd.num_sources - tile_first < kTile ? gd.num_sources - tile_first : kTile);
+        if (tid == 0) {
+            s.theta = gd.delta;
+        }
         if (tid < kTile) {
             s_src[tid] = tid < nsrc ? p.sources[base + tid] : -1;
             s_unreach[tid] = 0ull;
@@ -357,7 +355,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 const unsigned next_stamp = s.stamp + 1u;
                 const double theta = s.theta;
                 for (int i = warp; i < qlen; i += nwarps) {
-                    batched_expand<kUnroll>(p.g, __ldcg(&q_cur[i]), lane, dist, pend_cur, pend_nxt, far, q_nxt, &s.qlen[cur ^ 1], stamp, next_stamp, theta,
+                    batched_expand<kUnroll>(g, __ldcg(&q_cur[i]), lane, dist, pend_cur, pend_nxt, far, q_nxt, &s.qlen[cur ^ 1], stamp, next_stamp, theta,
                                             expansions, lane_expansions);
                 }
                 __syncthreads();
@@ -414,7 +412,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             if (s.min_bits == kInfBits) {
                 break;  // nothing pending: the tile's distances are final
             }
-            const double theta = next_theta(__longlong_as_double(static_cast<long long>(s.min_bits)), p.delta);
+            const double theta = next_theta(__longlong_as_double(static_cast<long long>(s.min_bits)), gd.delta);
             // pass 2: move the pairs below the new bound into the near queue of the next iteration
             const int cur = s.cur;
             uint32_t* pend_cur = cur ? pend1 : pend0;
@@ -452,12 +450,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
 
         if (tid == 0) {
             const long long now = clock64();
-            atomicAdd(&p.out.counters[kCyclesSssp], static_cast<unsigned long long>(now - t_phase));
+            atomicAdd(&cnts[kCyclesSssp], static_cast<unsigned long long>(now - t_phase));
             t_phase = now;
         }
         if constexpr (kMode != kModeApsp) {
             // ------------------------------------------------------------ shortest-path DAG: counts, sigma, delta
-            dag_count(b.rg, n, nsrc, s_src, dist, cnt, scnt, lane, warp, nwarps);
+            dag_count(rg, n, nsrc, s_src, dist, cnt, scnt, lane, warp, nwarps);
             __syncthreads();
             const unsigned long long dag_arcs = block_exclusive_scan(scnt, soff, nt, s_part);
             const bool use_lists = dag_arcs <= static_cast<unsigned long long>(b.succ_capacity);
@@ -466,17 +464,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             }
             __syncthreads();
             if (use_lists) {
-                dag_fill(b.rg, n, nsrc, s_src, dist, soff, scnt, succ, lane, warp, nwarps);
+                dag_fill(rg, n, nsrc, s_src, dist, soff, scnt, succ, lane, warp, nwarps);
                 __syncthreads();
                 dag_sort(soff, succ, nt);
                 __syncthreads();
             }
             if (tid == 0) {
                 const long long now = clock64();
-                atomicAdd(&p.out.counters[kCyclesCount], static_cast<unsigned long long>(now - t_phase));
+                atomicAdd(&cnts[kCyclesCount], static_cast<unsigned long long>(now - t_phase));
                 t_phase = now;
                 if (!use_lists) {
-                    atomicAdd(&p.out.counters[kDagScanTiles], 1ull);
+                    atomicAdd(&cnts[kDagScanTiles], 1ull);
                 }
             }
           if (use_lists) {
@@ -506,7 +504,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                     break;
                 }
                 const unsigned level = s.level;
-                dag_sigma_level(p.g, list + start, len, level, sigma, cnt, lvl, soff, succ, list + start + len, &s.next_len, b.sigma_inexact);
+                dag_sigma_level(g, list + start, len, level, sigma, cnt, lvl, soff, succ, list + start + len, &s.next_len, b.sigma_inexact);
                 __syncthreads();
                 if (tid == 0) {
                     s.lvl_start = start + len;
@@ -519,7 +517,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             }
             if (tid == 0) {
                 const long long now = clock64();
-                atomicAdd(&p.out.counters[kCyclesSigma], static_cast<unsigned long long>(now - t_phase));
+                atomicAdd(&cnts[kCyclesSigma], static_cast<unsigned long long>(now - t_phase));
                 t_phase = now;
             }
             const int levels = static_cast<int>(s.level);
@@ -527,14 +525,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             for (int level = levels - 1; level >= lowest; --level) {
                 const int start = __ldcg(&loff[level]);
                 const int end = __ldcg(&loff[level + 1]);
-                dag_delta_level<kMode>(p.g, list + start, end - start, dist, sigma, delta, delta_g, soff, succ, b.grad_cpl, b.grad_eff);
+                dag_delta_level<kMode>(g, list + start, end - start, dist, sigma, delta, delta_g, soff, succ, b.grad_cpl, b.grad_eff);
                 __syncthreads();
             }
             if (tid == 0) {
-                atomicAdd(&p.out.counters[kDagLevels], static_cast<unsigned long long>(levels));
-                atomicAdd(&p.out.counters[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
+                atomicAdd(&cnts[kDagLevels], static_cast<unsigned long long>(levels));
+                atomicAdd(&cnts[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
                 const long long now = clock64();
-                atomicAdd(&p.out.counters[kCyclesDelta], static_cast<unsigned long long>(now - t_phase));
+                atomicAdd(&cnts[kCyclesDelta], static_cast<unsigned long long>(now - t_phase));
                 t_phase = now;
             }
           } else {
@@ -570,12 +568,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 const unsigned level_stamp = s.stamp + 1u;
                 if (b.sigma_pull != 0) {
                     for (int i = warp; i < len; i += nwarps) {
-                        brandes_sigma_vertex<true, 2>(p.g, b.rg, __ldcg(&list[start + i]), level, nsrc, lane, dist, sigma, cnt, lvl, stamp, level_stamp,
+                        brandes_sigma_vertex<true, 2>(g, rg, __ldcg(&list[start + i]), level, nsrc, lane, dist, sigma, cnt, lvl, stamp, level_stamp,
                                                       list + start + len, &s.next_len, b.sigma_inexact);
                     }
                 } else {
                     for (int i = warp; i < len; i += nwarps) {
-                        brandes_sigma_vertex<false, 2>(p.g, b.rg, __ldcg(&list[start + i]), level, nsrc, lane, dist, sigma, cnt, lvl, stamp, level_stamp,
+                        brandes_sigma_vertex<false, 2>(g, rg, __ldcg(&list[start + i]), level, nsrc, lane, dist, sigma, cnt, lvl, stamp, level_stamp,
                                                        list + start + len, &s.next_len, b.sigma_inexact);
                     }
                 }
@@ -592,7 +590,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             }
             if (tid == 0) {
                 const long long now = clock64();
-                atomicAdd(&p.out.counters[kCyclesSigma], static_cast<unsigned long long>(now - t_phase));
+                atomicAdd(&cnts[kCyclesSigma], static_cast<unsigned long long>(now - t_phase));
                 t_phase = now;
             }
             // s.level is one past the last non-empty level; loff[s.level] is the end of the lists
@@ -602,18 +600,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 const int start = __ldcg(&loff[level]);
                 const int end = __ldcg(&loff[level + 1]);
                 for (int i = start + warp; i < end; i += nwarps) {
-                    brandes_delta_vertex<kMode, 2>(p.g, __ldcg(&list[i]), static_cast<unsigned>(level), nsrc, lane, dist, sigma, delta, delta_g, lvl,
+                    brandes_delta_vertex<kMode, 2>(g, __ldcg(&list[i]), static_cast<unsigned>(level), nsrc, lane, dist, sigma, delta, delta_g, lvl,
                                                    b.grad_cpl, b.grad_eff);
                 }
                 __syncthreads();
             }
             if (tid == 0) {
-                atomicAdd(&p.out.counters[kDagLevels], static_cast<unsigned long long>(levels));
-                atomicAdd(&p.out.counters[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
+                atomicAdd(&cnts[kDagLevels], static_cast<unsigned long long>(levels));
+                atomicAdd(&cnts[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
             }
             if (tid == 0) {
                 const long long now = clock64();
-                atomicAdd(&p.out.counters[kCyclesDelta], static_cast<unsigned long long>(now - t_phase));
+                atomicAdd(&cnts[kCyclesDelta], static_cast<unsigned long long>(now - t_phase));
                 t_phase = now;
             }
           }
@@ -634,7 +632,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                     const double dep = (valid && v != my_src) ? __ldcg(&delta[row]) : 0.0;
                     const double total = warp_sum(dep);
                     if (lane == 0 && total > 0.0) {
-                        fixed_add(&b.bc[2 * v], total);
+                        fixed_add(&bc_g[2 * v], total);
                     }
                 }
                 sigma[row] = 0.0;
@@ -657,7 +655,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 ++unreach;
                 continue;
             }
-            arcs += static_cast<unsigned long long>(__ldg(&p.g.row_ptr[v + 1]) - __ldg(&p.g.row_ptr[v]));
+            arcs += static_cast<unsigned long long>(__ldg(&g.row_ptr[v + 1]) - __ldg(&g.row_ptr[v]));
             mx = bits > mx ? bits : mx;
             acc_add_shared(&s_acc_sum[lane * kAccDigits], d);
             if (bits != 0ull) {
@@ -696,10 +694,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             if (p.out.src_unreach != nullptr) p.out.src_unreach[pos] = s_unreach[tid];
             if (p.out.src_arcs != nullptr) p.out.src_arcs[pos] = s_arcs[tid];
             const unsigned long long reached = static_cast<unsigned long long>(n) - s_unreach[tid];
-            atomicAdd(&p.out.counters[kUnreachable], s_unreach[tid]);
-            atomicAdd(&p.out.counters[kReachedPairs], reached - 1ull);
-            atomicAdd(&p.out.counters[kTraversedArcs], s_arcs[tid]);
-            atomicMax(&p.out.counters[kDiameterBits], s_max[tid]);
+            atomicAdd(&cnts[kUnreachable], s_unreach[tid]);
+            atomicAdd(&cnts[kReachedPairs], reached - 1ull);
+            atomicAdd(&cnts[kTraversedArcs], s_arcs[tid]);
+            atomicMax(&cnts[kDiameterBits], s_max[tid]);
         }
         __syncthreads();
         for (int i = tid; i < kAccDigits; i += blockDim.x) {
@@ -708,18 +706,18 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 t_sum += s_acc_sum[k * kAccDigits + i];
                 t_inv += s_acc_inv[k * kAccDigits + i];
             }
-            if (t_sum != 0) atomicAdd(&p.out.acc_sum[i], t_sum);
-            if (t_inv != 0) atomicAdd(&p.out.acc_inv[i], t_inv);
+            if (t_sum != 0) atomicAdd(&acc_sum_g[i], t_sum);
+            if (t_inv != 0) atomicAdd(&acc_inv_g[i], t_inv);
         }
         for (int i = tid; i < p.out.hist_bins; i += blockDim.x) {
             if (s_hist[i] != 0u) {
-                atomicAdd(&p.out.hist[i], static_cast<unsigned long long>(s_hist[i]));
+                atomicAdd(&hist_g[i], static_cast<unsigned long long>(s_hist[i]));
                 s_hist[i] = 0u;
             }
         }
         if (tid == 0) {
-            if (s.overflow != 0) atomicAdd(&p.out.counters[kHistOverflow], s.overflow);
-            atomicAdd(&p.out.counters[kIterations], s.iterations);
+            if (s.overflow != 0) atomicAdd(&cnts[kHistOverflow], s.overflow);
+            atomicAdd(&cnts[kIterations], s.iterations);
         }
         __syncthreads();
         for (int i = tid; i < 2 * kTile * kAccDigits; i += blockDim.x) {
@@ -727,10 +725,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         }
         __syncthreads();
         if (tid == 0) {
-            atomicAdd(&p.out.counters[kCyclesEpilogue], static_cast<unsigned long long>(clock64() - t_phase));
+            atomicAdd(&cnts[kCyclesEpilogue], static_cast<unsigned long long>(clock64() - t_phase));
         }
     }
     if (lane == 0 && expansions != 0) {
+        // whole-launch totals, kept in the first graph's counters
         atomicAdd(&p.out.counters[kExpansions], expansions);
         atomicAdd(&p.out.counters[kLaneExpansions], lane_expansions);
     }
