@@ -157,6 +157,25 @@ NGX_API int ngx_brandes(ngx_graph* graph, const ngx_apsp_opts* opts, double* bc,
 NGX_API int ngx_apsp_grad(ngx_graph* graph, const ngx_apsp_opts* opts, double* dcpl, double* deff, ngx_apsp_result* result);
 
 /* ------------------------------------------------------------------------------------------------------------------
+ * APSP without device allocation. No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory while they run: a process whose caching allocator already holds
+ * nearly all of the GPU (a cudaMalloc there fails or empties the cache), or a loop with a latency bound (cudaFree
+ * synchronizes the device). Same inputs, outputs and results as ngx_apsp in the batched form, but every device
+ * buffer comes from one fixed array of NGX_NOALLOC_SCRATCH_BYTES per device inside the library, and nothing is
+ * allocated. Limits, rejected with NGX_INVALID_ARGUMENT: n <= NGX_NOALLOC_MAX_VERTICES, num_sources <=
+ * NGX_NOALLOC_MAX_SOURCES, hist_max > 0 whenever hist_bins > 0 (no automatic bound); the plain form is rejected with
+ * NGX_UNSUPPORTED. kernel_ms is not measured (0). The first call on each device resolves the array's address
+ * (cudaGetSymbolAddress, which may load the library's device code): make that first call before any stream capture
+ * begins. Calls that overlap on the same device share the array and race: serialize them.
+ */
+#define NGX_NOALLOC_SCRATCH_BYTES (32u << 20)
+#define NGX_NOALLOC_MAX_VERTICES 32768
+#define NGX_NOALLOC_MAX_SOURCES 32768
+
+NGX_API int ngx_apsp_noalloc(ngx_graph* graph, const ngx_apsp_opts* opts, ngx_apsp_result* result);
+
+/* ------------------------------------------------------------------------------------------------------------------
  * Batches: many independent graphs of uneven sizes in one handle and one persistent launch, fed by a device queue of
  * (graph, source tile) work items in longest-first order. No reference counterpart: the reference processes one
  * graph per run (neurograph.cpp:139-416); the batch runs that loop's APSP / betweenness for every graph at once.

@@ -83,7 +83,7 @@ _LIB = None
 EXPORTED = [
     "ngx_status_string", "ngx_last_error", "ngx_version", "ngx_graph_create", "ngx_graph_destroy", "ngx_graph_size",
     "ngx_graph_request_abort", "ngx_graph_set_stream", "ngx_graph_set_memory_budget", "ngx_apsp", "ngx_sssp_rows", "ngx_brandes",
-    "ngx_apsp_grad", "ngx_batch_create", "ngx_batch_run", "ngx_batch_autotune", "ngx_graph_update_weights",
+    "ngx_apsp_grad", "ngx_batch_create", "ngx_batch_run", "ngx_batch_autotune", "ngx_graph_update_weights", "ngx_apsp_noalloc",
 ]
 
 
@@ -114,6 +114,7 @@ def library() -> C.CDLL:
         lib.ngx_batch_run.argtypes = [C.c_void_p, C.POINTER(_BatchOpts), C.POINTER(_Result), C.c_void_p, C.c_void_p, C.c_void_p]
         lib.ngx_batch_autotune.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         lib.ngx_graph_update_weights.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ngx_apsp_noalloc.argtypes = [C.c_void_p, C.POINTER(_Opts), C.POINTER(_Result)]
         _LIB = lib
     return _LIB
 
@@ -251,6 +252,15 @@ class Graph:
         opts, srcs, k = self._opts(sources, metric, mode, delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations)
         r, hist, per = self._result_struct(hist_bins, per_source, k)
         _check(library().ngx_apsp(self._handle, C.byref(opts), C.byref(r)))
+        return self._result(r, hist, per, k)
+
+    def apsp_noalloc(self, sources=None, metric="regular", delta=0.0, hist_bins=0, hist_max=0.0, per_source=False,
+                     block_threads=0, ctas_per_sm=0, max_iterations=0) -> ApspResult:
+        """ngx_apsp_noalloc: apsp() in the batched form with no device allocation (graphs of up to 32768 vertices;
+        hist_max is required with hist_bins). Calls on one device must not overlap."""
+        opts, srcs, k = self._opts(sources, metric, "batched", delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations)
+        r, hist, per = self._result_struct(hist_bins, per_source, k)
+        _check(library().ngx_apsp_noalloc(self._handle, C.byref(opts), C.byref(r)))
         return self._result(r, hist, per, k)
 
     def sssp_rows(self, sources, metric="regular", mode="batched", delta=0.0) -> np.ndarray:

@@ -62,6 +62,8 @@ void free_outputs(ngx_graph* g, RunOutputs& o);
 int device_error_status(int code);
 int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const TileJob& job, int64_t hist_bins, double hist_max, RunOutputs& o,
                  DagOutputs* extra, float* kernel_ms, bool synchronous);
+int launch_apsp_in_workspace(ngx_graph* g, const ngx_apsp_opts* opts, const TileJob& job, int64_t hist_bins, double hist_max, RunOutputs& o, void* ws,
+                             size_t ws_bytes);
 int read_totals(ngx_graph* g, const RunOutputs& o, std::vector<unsigned long long>& acc, std::vector<unsigned long long>& counters);
 int collect_graph(ngx_graph* g, const RunOutputs& o, const unsigned long long* acc_all, const unsigned long long* counters_all, int64_t gi,
                   int64_t src_off, int64_t num_sources, int64_t hist_bins, double hist_max, ngx_apsp_result* r);

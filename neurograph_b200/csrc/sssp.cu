@@ -312,6 +312,81 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
     return device_error_status(code);
 }
 
+// Launches the batched APSP tile kernel on the graph's stream with its workspace carved from `ws` (`ws_bytes` bytes,
+// 256-byte aligned) instead of the handle's workspace: nothing is allocated. Per-source outputs are written only where
+// `o` has them. Returns after the launch; the caller synchronizes.
+int launch_apsp_in_workspace(ngx_graph* g, const ngx_apsp_opts* opts, const TileJob& job, int64_t hist_bins, double hist_max, RunOutputs& o, void* ws,
+                             size_t ws_bytes) {
+    const int block = opts->block_threads > 0 ? opts->block_threads : kBatchedDefaultBlock;
+    const void* kernel = tile_kernel_for_block<kModeApsp>(block);
+    if (kernel == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "batched mode supports block_threads 256, 384 or 512");
+    }
+    if (job.num_items == 0) {
+        return NGX_OK;
+    }
+    const size_t smem = static_cast<size_t>(2) * kTile * kAccDigits * 8 + static_cast<size_t>(hist_bins) * 4;
+    NGX_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    int per_sm = 0;
+    NGX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem));
+    if (per_sm <= 0) {
+        return fail(NGX_UNSUPPORTED, "kernel does not fit on an SM with this block size and histogram");
+    }
+    if (opts->ctas_per_sm > 0) {
+        per_sm = std::min(per_sm, opts->ctas_per_sm);
+    }
+    const int64_t n = job.n_max;
+    const size_t slot_bytes = sssp_slot_bytes(n, kTile);
+    int64_t slots = std::min<int64_t>(job.num_items, static_cast<int64_t>(g->sm_count) * per_sm);
+    slots = std::min<int64_t>(slots, static_cast<int64_t>(ws_bytes / slot_bytes));
+    if (slots <= 0) {
+        return fail(NGX_OUT_OF_MEMORY, "the workspace holds no slot of " + std::to_string(slot_bytes) + " bytes");
+    }
+    char* w = static_cast<char*>(ws);
+    SsspParams p{};
+    p.g = g->csr(opts->metric);
+    p.g.n = n;
+    p.sources = o.sources;
+    p.num_sources = job.num_sources;
+    p.num_tiles = job.num_items;
+    p.delta = job.plain_delta;
+    p.graphs = o.graphs;
+    p.items = job.d_items;
+    p.max_iterations = opts->max_iterations > 0 ? opts->max_iterations : static_cast<unsigned long long>(4 * n + 64);
+    p.tile_counter = o.tile_counter;
+    p.error = o.error;
+    p.abort_flag = g->d_abort;
+    p.ws_dist = reinterpret_cast<unsigned long long*>(w);
+    w += static_cast<size_t>(slots) * n * kTile * 8;
+    p.ws_pend = reinterpret_cast<uint32_t*>(w);
+    w += static_cast<size_t>(slots) * 2 * n * 4;
+    p.ws_far = reinterpret_cast<uint32_t*>(w);
+    w += static_cast<size_t>(slots) * n * 4;
+    p.ws_queue = reinterpret_cast<int32_t*>(w);
+    w += static_cast<size_t>(slots) * 2 * n * 4;
+    p.ws_stamp = reinterpret_cast<uint32_t*>(w);
+    BrandesParams bp{};
+    p.out.acc_sum = o.acc;
+    p.out.acc_inv = o.acc + kAccDigits;
+    p.out.counters = o.counters;
+    p.out.hist = hist_bins > 0 ? o.hist : nullptr;
+    p.out.hist_bins = static_cast<int>(hist_bins);
+    p.out.hist_max = hist_max;
+    p.out.hist_width = hist_bins > 0 ? hist_max / static_cast<double>(hist_bins) : 0.0;
+    if (o.src_f64 != nullptr) {
+        p.out.src_sum = o.src_f64;
+        p.out.src_max = o.src_f64 + job.num_sources;
+        p.out.src_inv = o.src_f64 + 2 * job.num_sources;
+    }
+    if (o.src_u64 != nullptr) {
+        p.out.src_unreach = o.src_u64;
+        p.out.src_arcs = o.src_u64 + job.num_sources;
+    }
+    void* args[] = { &p, &bp };
+    const cudaError_t err = cudaLaunchKernel(kernel, dim3(static_cast<unsigned>(slots)), dim3(block), args, smem, g->stream);
+    return err == cudaSuccess ? NGX_OK : cuda_fail(err, "tile kernel launch");
+}
+
 void clear_result_totals(ngx_apsp_result* r) {
     r->sum_distances = r->sum_inverse = r->diameter = 0.0;
     r->unreachable = r->reached_pairs = r->traversed_arcs = r->hist_overflow = 0;
