@@ -145,9 +145,9 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic_per_arc():
-    """DRAM bytes per traversed arc of the Brandes tile kernel, from the committed ncu summary (or None)."""
-    path = os.path.join(ROOT, "profiles", "tile_kernel_brandes_c2.md")
+def profiled_traffic_per_arc(mode):
+    """DRAM bytes per traversed arc of the mode's tile kernel on this workload, from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, "profiles", f"tile_kernel_{mode}_connectome_n100k.md")
     if not os.path.exists(path):
         return None
     with open(path) as f:
@@ -326,13 +326,13 @@ def main():
     arcs_total = sum_over_ranks(float(arcs))
     value = arcs_total / elapsed_max / 1e9
 
-    # roofline of the dominant kernel (the Brandes tile kernel): algorithmic bytes per SURVEY 8(d) accounting:
-    # SSSP 20 B per traversed arc + 24 B per reached vertex, Brandes 56 B per arc + 32 B per vertex
+    # roofline of the dominant kernel (the Brandes tile kernel), algorithmic bytes: SSSP 20 B per traversed arc
+    # + 24 B per reached vertex; Brandes adds 56 B per arc + 32 B per vertex; the adjoint adds 84 B + 56 B
     per_arc, per_vertex = {"brandes": (76.0, 56.0), "grad": (104.0, 80.0), "apsp": (20.0, 24.0), "plain": (20.0, 24.0)}[args.mode]
     alg_bytes = per_arc * arcs + per_vertex * reached
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
-    traffic_per_arc = profiled_traffic_per_arc()
+    traffic_per_arc = profiled_traffic_per_arc(args.mode)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6.65 TB/s",
                 "traffic": None if traffic_per_arc is None else traffic_per_arc * arcs / launches,
