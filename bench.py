@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--delta", type=float, default=0.25)
     ap.add_argument("--mode", choices=["brandes", "apsp", "grad", "plain"], default="brandes",
                     help="what one step runs: APSP+Brandes (the headline), APSP only, APSP+gradient, or the plain per-source form")
+    ap.add_argument("--block-threads", type=int, default=0, help="tile kernel block size (0 = the library default)")
+    ap.add_argument("--ctas-per-sm", type=int, default=0, help="resident tile CTAs per SM (0 = as many as fit)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the plain/batched APSP comparison runs")
@@ -104,6 +106,17 @@ class ClockSampler:
                                           "-i", str(self.device_index)], stdout=self.file, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+
+    def wait_first_sample(self, timeout_s=10.0):
+        """nvidia-smi's start-up (NVML initialisation) can stall the GPU's host interface; wait for its first sample so
+        that this happens before the timed region, not inside it."""
+        t0 = time.perf_counter()
+        while self.proc is not None and time.perf_counter() - t0 < timeout_s:
+            self.file.flush()
+            if os.path.getsize(self.file.name) > 0:
+                break
+            time.sleep(0.05)
+        time.sleep(0.3)
 
     def stop(self):
         if self.proc is not None:
@@ -221,17 +234,25 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline_single_core(c, sources):
+def cpu_baseline_single_core(c, sources, budget_s=12.0):
+    """The CPU restatement on one core, source after source, until about `budget_s` seconds of work are done."""
     import oracle
 
     g = oracle.Csr.from_arrays(c.n, c.row_ptr, c.col, c.w)
     r = oracle.Restatement()
+    arcs, done = 0, 0
     t0 = time.perf_counter()
-    a = r.apsp(g, sources=sources, bins=HIST_BINS, hist_max=64.0)
-    r.brandes(g, sources=sources)
+    for s in sources:
+        one = np.array([s], dtype=np.int64)
+        a = r.apsp(g, sources=one, bins=HIST_BINS, hist_max=64.0)
+        r.brandes(g, sources=one)
+        arcs += a["traversed_arcs"]
+        done += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
     dt = time.perf_counter() - t0
-    return {"value": a["traversed_arcs"] / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
-            "sample": f"{len(sources)} sources of the same graph, APSP summaries + histogram + Brandes, {dt:.1f} s, single thread; "
+    return {"value": arcs / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "port",
+            "sample": f"{done} sources of the same graph, APSP summaries + histogram + Brandes, {dt:.1f} s, single thread; "
                       "CPU restatement of the reference Dijkstra/Brandes (bit-exact with the reference on integer weights)"}
 
 
@@ -288,14 +309,15 @@ def main():
     def step(graph, sources, hist_max):
         """One step of the selected mode; returns (result, host outputs)."""
         if args.mode == "brandes":
-            bc, r = graph.brandes(sources=sources, delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max, per_source=True)
+            bc, r = graph.brandes(sources=sources, delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max, per_source=True,
+                                  block_threads=args.block_threads, ctas_per_sm=args.ctas_per_sm)
             return r, [bc]
         if args.mode == "grad":
-            dcpl, deff, r = graph.apsp_grad(sources=sources, delta=args.delta)
+            dcpl, deff, r = graph.apsp_grad(sources=sources, delta=args.delta, block_threads=args.block_threads, ctas_per_sm=args.ctas_per_sm)
             return r, [dcpl, deff]
         mode = "plain" if args.mode == "plain" else "batched"
         r = graph.apsp(sources=sources, mode=mode, delta=args.delta if mode == "batched" else 0.1, hist_bins=HIST_BINS, hist_max=hist_max,
-                       per_source=True)
+                       per_source=True, block_threads=args.block_threads, ctas_per_sm=args.ctas_per_sm)
         return r, []
 
     # histogram bound: sampled eccentricity x 1.5 from the first warm-up step, fixed for the timed steps
@@ -306,22 +328,34 @@ def main():
         hist_max = r.hist_max if r.hist_max > 0 else hist_max
     clocks = ClockSampler(local_rank)
     clocks.start()
+    clocks.wait_first_sample()
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     arcs = 0
     reached = 0
     kernel_ms = 0.0
+    step_events = []
+    step_kernel_ms = []
     for i in range(args.warmup, args.warmup + args.steps):
         r, _ = step(g, batches[i], hist_max)
         arcs += r.traversed_arcs
         reached += r.reached_pairs + len(batches[i])
         kernel_ms += r.kernel_ms
+        step_kernel_ms.append(r.kernel_ms)
+        log(f"[bench] counters: phases {r.phases} expansions {r.expansions} lane_expansions {r.lane_expansions} "
+            f"dag_levels {r.dag_levels} dag_entries {r.dag_entries} dag_scan_tiles {r.dag_scan_tiles} phase_cycles {list(r.phase_cycles)}")
         launches += 1
+        step_events.append(torch.cuda.Event(enable_timing=True))
+        step_events[-1].record(stream)
     ev1.record(stream)
     barrier()
     clock_info = clocks.stop()
     elapsed = ev0.elapsed_time(ev1) / 1e3
+    prev = ev0
+    for k, (e, kms) in enumerate(zip(step_events, step_kernel_ms)):
+        log(f"[bench] step {k}: {prev.elapsed_time(e):.1f} ms, kernel {kms:.1f} ms")
+        prev = e
     elapsed_max = max_over_ranks(elapsed)
     arcs_total = sum_over_ranks(float(arcs))
     value = arcs_total / elapsed_max / 1e9
@@ -371,7 +405,7 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_single_core(c, batches[0][:2])
+        cpu = cpu_baseline_single_core(c, batches[0])
 
     if dist is not None:
         dist.barrier()

@@ -73,6 +73,7 @@ __device__ __forceinline__ void brandes_count(const DeviceCsr& rg, int64_t n, in
         const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
         const bool active = lane < nsrc && dv != kInfBits && v != s_src[lane];
         uint32_t c = 0;
+        uint32_t first = 0;
         if (__ballot_sync(0xFFFFFFFFu, active) != 0u) {
             const int64_t beg = __ldg(&rg.row_ptr[v]);
             const int64_t end = __ldg(&rg.row_ptr[v + 1]);
@@ -347,13 +348,15 @@ __device__ __forceinline__ void brandes_delta_vertex(const DeviceCsr& g, int v, 
 // a second dense pass fills the lists (forward-CSR arc indices), and each list is sorted so that every sum over it has
 // a fixed order. sigma and delta then touch only DAG arcs.
 
-// cnt[v][s] = DAG predecessors; scnt[u][s] += 1 for each DAG arc u -> v (warp per vertex, lane per source).
+// cnt[v][s] = DAG predecessors; scnt[u][s] += 1 for each DAG arc u -> v (warp per vertex, lane per source);
+// pred[v][s] = reverse-CSR index of the first DAG in-arc found (the only one when cnt[v][s] == 1).
 __device__ __forceinline__ void dag_count(const DeviceCsr& rg, int64_t n, int nsrc, const int* s_src, const unsigned long long* dist, uint32_t* cnt,
-                                          uint32_t* scnt, int lane, int warp, int nwarps) {
+                                          uint32_t* scnt, uint32_t* pred, int lane, int warp, int nwarps) {
     for (int64_t v = warp; v < n; v += nwarps) {
         const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
         const bool active = lane < nsrc && dv != kInfBits && v != s_src[lane];
         uint32_t c = 0;
+        uint32_t first = 0;
         if (__ballot_sync(0xFFFFFFFFu, active) != 0u) {
             const int64_t beg = __ldg(&rg.row_ptr[v]);
             const int64_t end = __ldg(&rg.row_ptr[v + 1]);
@@ -377,6 +380,9 @@ __device__ __forceinline__ void dag_count(const DeviceCsr& rg, int64_t n, int ns
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         if (du[u] != kInfBits && on_dag(du[u], len[u], dv)) {
+                            if (c == 0) {
+                                first = static_cast<uint32_t>(e0 + j + u);
+                            }
                             ++c;
                             atomicAdd(&scnt[static_cast<int64_t>(src[u]) * kTile + lane], 1u);
                         }
@@ -385,6 +391,7 @@ __device__ __forceinline__ void dag_count(const DeviceCsr& rg, int64_t n, int ns
             }
         }
         cnt[v * kTile + lane] = c;
+        pred[v * kTile + lane] = first;
     }
 }
 
@@ -425,15 +432,23 @@ __device__ __forceinline__ unsigned long long block_exclusive_scan(const uint32_
     return total;
 }
 
-// Fills the successor lists: for each DAG arc u -> v (forward index in the reverse record), appended to (u, s).
-__device__ __forceinline__ void dag_fill(const DeviceCsr& rg, int64_t n, int nsrc, const int* s_src, const unsigned long long* dist, const uint32_t* soff,
-                                         uint32_t* sfill, uint32_t* succ, int lane, int warp, int nwarps) {
+// Fills the successor lists: each DAG arc u -> v (its forward index, from the reverse record) is appended to (u, s).
+// A (v, s) with a single DAG predecessor takes it from pred[v][s]; only lanes with ties re-scan v's in-arcs.
+__device__ __forceinline__ void dag_fill(const DeviceCsr& rg, int64_t n, const unsigned long long* dist, const uint32_t* cnt, const uint32_t* pred,
+                                         const uint32_t* soff, uint32_t* sfill, uint32_t* succ, int lane, int warp, int nwarps) {
     for (int64_t v = warp; v < n; v += nwarps) {
-        const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
-        const bool active = lane < nsrc && dv != kInfBits && v != s_src[lane];
+        const uint32_t c = __ldcg(&cnt[v * kTile + lane]);
+        if (c == 1u) {
+            const Arc a = rg.arcs[__ldcg(&pred[v * kTile + lane])];
+            const int64_t urow = static_cast<int64_t>(a.col) * kTile + lane;
+            const uint32_t pos = atomicAdd(&sfill[urow], 1u);
+            succ[__ldcg(&soff[urow]) + pos] = static_cast<uint32_t>(a.id);
+        }
+        const bool active = c >= 2u;
         if (__ballot_sync(0xFFFFFFFFu, active) == 0u) {
             continue;
         }
+        const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
         const int64_t beg = __ldg(&rg.row_ptr[v]);
         const int64_t end = __ldg(&rg.row_ptr[v + 1]);
         for (int64_t e0 = beg; e0 < end; e0 += 32) {

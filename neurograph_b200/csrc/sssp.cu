@@ -22,7 +22,7 @@ namespace ngx {
 namespace {
 constexpr int kBatchedUnroll = 4;
 constexpr int kPlainWarpsMax = 16;
-constexpr int kBatchedDefaultBlock = 384;
+constexpr int kBatchedDefaultBlock = 512;
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 }  // namespace
@@ -145,10 +145,13 @@ int device_error_status(int code) {
     }
 }
 
+// The instantiation for a block size; 256 threads with ctas_per_sm >= 4 selects the 4-CTA (64-register) build.
 template <int kMode>
-const void* tile_kernel_for_block(int block) {
+const void* tile_kernel_for_block(int block, int ctas_per_sm = 0) {
     switch (block) {
-    case 256: return reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 256, 3>);
+    case 256:
+        return ctas_per_sm >= 4 ? reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 256, 4>)
+                                : reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 256, 3>);
     case 384: return reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 384, 2>);
     case 512: return reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 512, 2>);
     default: return nullptr;
@@ -172,9 +175,9 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
 
     const void* kernel = reinterpret_cast<const void*>(&sssp_plain_kernel);
     if (batched) {
-        kernel = tile_mode == kModeBrandes ? tile_kernel_for_block<kModeBrandes>(block)
-                 : tile_mode == kModeGrad  ? tile_kernel_for_block<kModeGrad>(block)
-                                           : tile_kernel_for_block<kModeApsp>(block);
+        kernel = tile_mode == kModeBrandes ? tile_kernel_for_block<kModeBrandes>(block, opts->ctas_per_sm)
+                 : tile_mode == kModeGrad  ? tile_kernel_for_block<kModeGrad>(block, opts->ctas_per_sm)
+                                           : tile_kernel_for_block<kModeApsp>(block, opts->ctas_per_sm);
         if (kernel == nullptr) {
             return fail(NGX_INVALID_ARGUMENT, "batched mode supports block_threads 256, 384 or 512");
         }
@@ -318,7 +321,7 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
 int launch_apsp_in_workspace(ngx_graph* g, const ngx_apsp_opts* opts, const TileJob& job, int64_t hist_bins, double hist_max, RunOutputs& o, void* ws,
                              size_t ws_bytes) {
     const int block = opts->block_threads > 0 ? opts->block_threads : kBatchedDefaultBlock;
-    const void* kernel = tile_kernel_for_block<kModeApsp>(block);
+    const void* kernel = tile_kernel_for_block<kModeApsp>(block, opts->ctas_per_sm);
     if (kernel == nullptr) {
         return fail(NGX_INVALID_ARGUMENT, "batched mode supports block_threads 256, 384 or 512");
     }

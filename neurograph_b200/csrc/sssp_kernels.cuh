@@ -455,7 +455,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         }
         if constexpr (kMode != kModeApsp) {
             // ------------------------------------------------------------ shortest-path DAG: counts, sigma, delta
-            dag_count(rg, n, nsrc, s_src, dist, cnt, scnt, lane, warp, nwarps);
+            // the level lists are built only after the successor lists: their storage holds pred[][] until then
+            uint32_t* const pred = reinterpret_cast<uint32_t*>(list);
+            dag_count(rg, n, nsrc, s_src, dist, cnt, scnt, pred, lane, warp, nwarps);
             __syncthreads();
             const unsigned long long dag_arcs = block_exclusive_scan(scnt, soff, nt, s_part);
             const bool use_lists = dag_arcs <= static_cast<unsigned long long>(b.succ_capacity);
@@ -464,7 +466,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             }
             __syncthreads();
             if (use_lists) {
-                dag_fill(rg, n, nsrc, s_src, dist, soff, scnt, succ, lane, warp, nwarps);
+                dag_fill(rg, n, dist, cnt, pred, soff, scnt, succ, lane, warp, nwarps);
                 __syncthreads();
                 dag_sort(soff, succ, nt);
                 __syncthreads();
