@@ -338,7 +338,9 @@ def main():
     step_events = []
     step_kernel_ms = []
     for i in range(args.warmup, args.warmup + args.steps):
+        t_host = time.perf_counter()
         r, _ = step(g, batches[i], hist_max)
+        log(f"[bench] host call {1e3 * (time.perf_counter() - t_host):.1f} ms")
         arcs += r.traversed_arcs
         reached += r.reached_pairs + len(batches[i])
         kernel_ms += r.kernel_ms

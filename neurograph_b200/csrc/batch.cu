@@ -381,9 +381,9 @@ int ngx_batch_autotune(ngx_graph* g, int task, double* class_scales) {
             const size_t dag_words = 1 + (mode == kModeBrandes ? 2 * static_cast<size_t>(g->n_total) : 0) +
                                      (mode == kModeGrad ? 4 * static_cast<size_t>(g->m_user) : 0);
             if (rc == NGX_OK && mode != kModeApsp) {
-                const cudaError_t e = cudaMallocAsync(&dag, dag_words * 8, g->stream);
-                rc = e == cudaSuccess ? NGX_OK : cuda_fail(e, "autotune buffers");
+                rc = grow_buffer(g, &g->d_call_dag, &g->call_dag_bytes, dag_words * 8);
                 if (rc == NGX_OK) {
+                    dag = static_cast<unsigned long long*>(g->d_call_dag);
                     cudaMemsetAsync(dag, 0, dag_words * 8, g->stream);
                     extra.sigma_inexact = reinterpret_cast<int*>(dag);
                     if (mode == kModeBrandes) extra.bc = dag + 1;
@@ -417,9 +417,6 @@ int ngx_batch_autotune(ngx_graph* g, int task, double* class_scales) {
                         }
                     }
                 }
-            }
-            if (dag != nullptr) {
-                cudaFreeAsync(dag, g->stream);
             }
             free_outputs(g, o);
             cudaStreamSynchronize(g->stream);

@@ -36,8 +36,10 @@ int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_res
     const size_t bc_words = tile_mode == kModeBrandes ? 2 * n : 0;
     const size_t grad_words = tile_mode == kModeGrad ? 2 * m : 0;
     const size_t words = 1 + bc_words + 2 * grad_words;
-    unsigned long long* block = nullptr;
-    NGX_CUDA_TRY(cudaMallocAsync(&block, words * 8, g->stream));
+    if (const int rc = grow_buffer(g, &g->d_call_dag, &g->call_dag_bytes, words * 8); rc != NGX_OK) {
+        return rc;
+    }
+    unsigned long long* block = static_cast<unsigned long long*>(g->d_call_dag);
     NGX_CUDA_TRY(cudaMemsetAsync(block, 0, words * 8, g->stream));
     extra.sigma_inexact = reinterpret_cast<int*>(block);
     if (bc_words != 0) {
@@ -90,7 +92,6 @@ int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_res
         }
         *reached_pairs = r->reached_pairs;
     }
-    cudaFreeAsync(block, g->stream);
     cudaStreamSynchronize(g->stream);
     return rc;
 }

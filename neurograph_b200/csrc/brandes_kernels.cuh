@@ -73,7 +73,6 @@ __device__ __forceinline__ void brandes_count(const DeviceCsr& rg, int64_t n, in
         const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
         const bool active = lane < nsrc && dv != kInfBits && v != s_src[lane];
         uint32_t c = 0;
-        uint32_t first = 0;
         if (__ballot_sync(0xFFFFFFFFu, active) != 0u) {
             const int64_t beg = __ldg(&rg.row_ptr[v]);
             const int64_t end = __ldg(&rg.row_ptr[v + 1]);
@@ -432,8 +431,10 @@ __device__ __forceinline__ unsigned long long block_exclusive_scan(const uint32_
     return total;
 }
 
-// Fills the successor lists: each DAG arc u -> v (its forward index, from the reverse record) is appended to (u, s).
-// A (v, s) with a single DAG predecessor takes it from pred[v][s]; only lanes with ties re-scan v's in-arcs.
+// Fills the successor lists: each DAG arc u -> v is appended to (u, s), as its target v (kTarget: betweenness needs
+// nothing else) or as its forward-CSR index (the adjoint also needs the arc). A (v, s) with a single DAG predecessor
+// takes it from pred[v][s]; only lanes with ties re-scan v's in-arcs.
+template <bool kTarget>
 __device__ __forceinline__ void dag_fill(const DeviceCsr& rg, int64_t n, const unsigned long long* dist, const uint32_t* cnt, const uint32_t* pred,
                                          const uint32_t* soff, uint32_t* sfill, uint32_t* succ, int lane, int warp, int nwarps) {
     for (int64_t v = warp; v < n; v += nwarps) {
@@ -442,7 +443,7 @@ __device__ __forceinline__ void dag_fill(const DeviceCsr& rg, int64_t n, const u
             const Arc a = rg.arcs[__ldcg(&pred[v * kTile + lane])];
             const int64_t urow = static_cast<int64_t>(a.col) * kTile + lane;
             const uint32_t pos = atomicAdd(&sfill[urow], 1u);
-            succ[__ldcg(&soff[urow]) + pos] = static_cast<uint32_t>(a.id);
+            succ[__ldcg(&soff[urow]) + pos] = kTarget ? static_cast<uint32_t>(v) : static_cast<uint32_t>(a.id);
         }
         const bool active = c >= 2u;
         if (__ballot_sync(0xFFFFFFFFu, active) == 0u) {
@@ -474,7 +475,7 @@ __device__ __forceinline__ void dag_fill(const DeviceCsr& rg, int64_t n, const u
                     if (du[u] != kInfBits && on_dag(du[u], len[u], dv)) {
                         const int64_t urow = static_cast<int64_t>(src[u]) * kTile + lane;
                         const uint32_t pos = atomicAdd(&sfill[urow], 1u);
-                        succ[__ldcg(&soff[urow]) + pos] = static_cast<uint32_t>(fwd[u]);
+                        succ[__ldcg(&soff[urow]) + pos] = kTarget ? static_cast<uint32_t>(v) : static_cast<uint32_t>(fwd[u]);
                     }
                 }
             }
@@ -482,7 +483,7 @@ __device__ __forceinline__ void dag_fill(const DeviceCsr& rg, int64_t n, const u
     }
 }
 
-// Sorts each successor list by forward arc index (the fill order depends on timing; the sums must not).
+// Sorts each successor list by its entries (the fill order depends on timing; the sums must not).
 __device__ __forceinline__ void dag_sort(const uint32_t* soff, uint32_t* succ, int64_t nt) {
     for (int64_t i = threadIdx.x; i < nt; i += blockDim.x) {
         const uint32_t beg = __ldcg(&soff[i]);
@@ -499,64 +500,211 @@ __device__ __forceinline__ void dag_sort(const uint32_t* soff, uint32_t* succ, i
     }
 }
 
-// sigma over one level of (vertex, source) entries (entry = v * 32 + s): push sigma[v][s] into the DAG successors
-// (exact integer sums, see brandes_sigma_vertex) and release those whose last predecessor this was.
+// ------------------------------------------------------------------------------------------ level passes
+// One level of (vertex, source) entries (entry = v << 5 | s) is processed a warp at a time: the warp takes 32 entries,
+// scans their successor-list lengths, and walks the (entry, successor) pairs 32 at a time, kLevelUnroll pairs per lane
+// in flight, so hubs with long lists do not serialise a lane and every lane keeps independent loads outstanding.
+constexpr int kLevelUnroll = 4;
+
+// The adjoint's delta pass carries twice the values per pair; it unrolls less to stay within 64 registers.
+constexpr int delta_level_unroll(int mode) { return mode == kModeGrad ? 2 : 4; }
+
+// Exclusive prefix of x over the warp's lanes; *total receives the sum.
+__device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t x, int lane, uint32_t* total) {
+    uint32_t incl = x;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= d) {
+            incl += y;
+        }
+    }
+    *total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    return incl - x;
+}
+
+// The lane whose list holds pair p: the largest lane L with off[L] <= p (lanes with empty lists share their
+// successor's offset, so L always has a non-empty list when p < total).
+__device__ __forceinline__ int pair_owner(uint32_t off, uint32_t p) {
+    int l = 0;
+#pragma unroll
+    for (int step = 16; step >= 1; step >>= 1) {
+        const uint32_t o = __shfl_sync(0xFFFFFFFFu, off, l + step);
+        if (o <= p) {
+            l += step;
+        }
+    }
+    return l;
+}
+
+// sigma over one level: every entry adds sigma[v][s] into its DAG successors and releases those whose last
+// predecessor this was. The adds are exact integer sums while below 2^53 (see brandes_sigma_vertex); since every
+// addend is positive, a final value below 2^53 proves every partial sum was too, so the check is made on each entry's
+// final sigma when its own level runs.
+template <bool kTarget>
 __device__ __forceinline__ void dag_sigma_level(const DeviceCsr& g, const int32_t* entries, int len, uint32_t level, double* sigma, uint32_t* cnt,
                                                 uint32_t* lvl, const uint32_t* soff, const uint32_t* succ, int32_t* next_list, int* next_len,
-                                                int* inexact) {
-    for (int i = threadIdx.x; i < len; i += blockDim.x) {
-        const uint32_t entry = static_cast<uint32_t>(__ldcg(&entries[i]));
-        const int64_t row = static_cast<int64_t>(entry >> 5) * kTile + (entry & 31u);
-        const double sv = __ldcg(&sigma[row]);
-        const uint32_t beg = __ldcg(&soff[row]);
-        const uint32_t end = __ldcg(&soff[row + 1]);
-        for (uint32_t j = beg; j < end; ++j) {
-            const Arc arc = g.arcs[__ldcg(&succ[j])];
-            const int64_t xrow = static_cast<int64_t>(arc.col) * kTile + (entry & 31u);
-            const double before = atomicAdd(&sigma[xrow], sv);
-            if (before + sv >= kSigmaExact) {
+                                                int* inexact, int lane, int warp, int nwarps) {
+    for (int base = warp * 32; base < len; base += nwarps * 32) {
+        const int i = base + lane;
+        uint32_t entry = 0, beg = 0, count = 0;
+        double sv = 0.0;
+        if (i < len) {
+            entry = static_cast<uint32_t>(__ldcg(&entries[i]));
+            const int64_t row = static_cast<int64_t>(entry >> 5) * kTile + (entry & 31u);
+            sv = __ldcg(&sigma[row]);
+            beg = __ldcg(&soff[row]);
+            count = __ldcg(&soff[row + 1]) - beg;
+            if (sv >= kSigmaExact) {
                 atomicExch(inexact, 1);
             }
-            if (atomicSub(&cnt[xrow], 1u) == 1u) {
-                lvl[xrow] = level + 1u;
-                next_list[atomicAdd(next_len, 1)] = static_cast<int32_t>((static_cast<uint32_t>(arc.col) << 5) | (entry & 31u));
+        }
+        uint32_t total = 0;
+        const uint32_t off = warp_exclusive_scan(count, lane, &total);
+        for (uint32_t p0 = 0; p0 < total; p0 += 32 * kLevelUnroll) {
+            uint32_t xrow_s[kLevelUnroll];
+            uint32_t x[kLevelUnroll];
+            double add[kLevelUnroll];
+            bool ok[kLevelUnroll];
+#pragma unroll
+            for (int u = 0; u < kLevelUnroll; ++u) {
+                const uint32_t q = p0 + static_cast<uint32_t>(u * 32 + lane);
+                ok[u] = q < total;
+                const int owner = pair_owner(off, ok[u] ? q : 0u);
+                const uint32_t j = __shfl_sync(0xFFFFFFFFu, beg, owner) + (q - __shfl_sync(0xFFFFFFFFu, off, owner));
+                xrow_s[u] = __shfl_sync(0xFFFFFFFFu, entry, owner) & 31u;
+                add[u] = __shfl_sync(0xFFFFFFFFu, sv, owner);
+                x[u] = 0;
+                if (ok[u]) {
+                    const uint32_t e = __ldcg(&succ[j]);
+                    x[u] = kTarget ? e : static_cast<uint32_t>(g.arcs[e].col);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kLevelUnroll; ++u) {
+                bool push = false;
+                const int64_t xrow = static_cast<int64_t>(x[u]) * kTile + xrow_s[u];
+                if (ok[u]) {
+                    atomicAdd(&sigma[xrow], add[u]);
+                    if (atomicSub(&cnt[xrow], 1u) == 1u) {
+                        lvl[xrow] = level + 1u;
+                        push = true;
+                    }
+                }
+                const unsigned pmask = __ballot_sync(0xFFFFFFFFu, push);
+                if (pmask != 0u) {
+                    int at = 0;
+                    const int leader = __ffs(pmask) - 1;
+                    if (lane == leader) {
+                        at = atomicAdd(next_len, __popc(pmask));
+                    }
+                    at = __shfl_sync(0xFFFFFFFFu, at, leader);
+                    if (push) {
+                        next_list[at + __popc(pmask & lanemask_lt())] = static_cast<int32_t>((x[u] << 5) | xrow_s[u]);
+                    }
+                }
             }
         }
     }
 }
 
-// delta (and the adjoint terms) over one level of (vertex, source) entries: pull over the sorted successor list.
+// delta (and the adjoint terms) over one level: each entry pulls over its sorted successor list. Pair contributions
+// go through the warp's slice of `buf` (32 values per unrolled pair, twice for the adjoint) and each entry's lane adds
+// its own in list order, so every sum runs in the same order as a sequential loop over the list.
 template <int kMode>
 __device__ __forceinline__ void dag_delta_level(const DeviceCsr& g, const int32_t* entries, int len, const unsigned long long* dist, const double* sigma,
                                                 double* delta, double* delta_g, const uint32_t* soff, const uint32_t* succ, unsigned long long* grad_cpl,
-                                                unsigned long long* grad_eff) {
-    for (int i = threadIdx.x; i < len; i += blockDim.x) {
-        const uint32_t entry = static_cast<uint32_t>(__ldcg(&entries[i]));
-        const uint32_t s = entry & 31u;
-        const int64_t row = static_cast<int64_t>(entry >> 5) * kTile + s;
-        const double sv = __ldcg(&sigma[row]);
-        const uint32_t beg = __ldcg(&soff[row]);
-        const uint32_t end = __ldcg(&soff[row + 1]);
-        double acc = 0.0, acc_g = 0.0;
-        for (uint32_t j = beg; j < end; ++j) {
-            const Arc arc = g.arcs[__ldcg(&succ[j])];
-            const int64_t xrow = static_cast<int64_t>(arc.col) * kTile + s;
-            if constexpr (kMode == kModeBrandes) {
-                acc += sv * ((1.0 + __ldcg(&delta[xrow])) / __ldcg(&sigma[xrow]));
-            } else {
-                const double share = sv / __ldcg(&sigma[xrow]);
-                const double inv = 1.0 / __longlong_as_double(static_cast<long long>(__ldcg(&dist[xrow])));
-                const double c = share * (1.0 + __ldcg(&delta[xrow]));
-                const double cg = share * (inv * inv + __ldcg(&delta_g[xrow]));
-                acc += c;
-                acc_g += cg;
-                fixed_add(&grad_cpl[2 * static_cast<int64_t>(arc.id)], c);
-                fixed_add(&grad_eff[2 * static_cast<int64_t>(arc.id)], cg);
-            }
+                                                unsigned long long* grad_eff, double* buf, int lane, int warp, int nwarps) {
+    constexpr bool kTarget = kMode == kModeBrandes;
+    constexpr int kU = delta_level_unroll(kMode);
+    double* const wbuf = buf + static_cast<size_t>(warp) * 32 * kU * (kMode == kModeGrad ? 2 : 1);
+    for (int base = warp * 32; base < len; base += nwarps * 32) {
+        const int i = base + lane;
+        uint32_t entry = 0, beg = 0, count = 0;
+        double sv = 0.0;
+        int64_t row = 0;
+        if (i < len) {
+            entry = static_cast<uint32_t>(__ldcg(&entries[i]));
+            row = static_cast<int64_t>(entry >> 5) * kTile + (entry & 31u);
+            sv = __ldcg(&sigma[row]);
+            beg = __ldcg(&soff[row]);
+            count = __ldcg(&soff[row + 1]) - beg;
         }
-        delta[row] = acc;
-        if constexpr (kMode == kModeGrad) {
-            delta_g[row] = acc_g;
+        uint32_t total = 0;
+        const uint32_t off = warp_exclusive_scan(count, lane, &total);
+        double acc = 0.0, acc_g = 0.0;
+        for (uint32_t p0 = 0; p0 < total; p0 += 32 * kU) {
+            double dx[kU], sx[kU], share_sv[kU], gx[kU], dgx[kU];
+            int32_t id[kU];
+            bool ok[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const uint32_t q = p0 + static_cast<uint32_t>(u * 32 + lane);
+                ok[u] = q < total;
+                const int owner = pair_owner(off, ok[u] ? q : 0u);
+                const uint32_t j = __shfl_sync(0xFFFFFFFFu, beg, owner) + (q - __shfl_sync(0xFFFFFFFFu, off, owner));
+                const uint32_t s = __shfl_sync(0xFFFFFFFFu, entry, owner) & 31u;
+                share_sv[u] = __shfl_sync(0xFFFFFFFFu, sv, owner);
+                dx[u] = 0.0;
+                sx[u] = 1.0;
+                gx[u] = 0.0;
+                dgx[u] = 0.0;
+                id[u] = 0;
+                if (ok[u]) {
+                    const uint32_t e = __ldcg(&succ[j]);
+                    uint32_t x = e;
+                    if constexpr (!kTarget) {
+                        const Arc arc = g.arcs[e];
+                        x = static_cast<uint32_t>(arc.col);
+                        id[u] = arc.id;
+                    }
+                    const int64_t xrow = static_cast<int64_t>(x) * kTile + s;
+                    dx[u] = __ldcg(&delta[xrow]);
+                    sx[u] = __ldcg(&sigma[xrow]);
+                    if constexpr (kMode == kModeGrad) {
+                        gx[u] = __longlong_as_double(static_cast<long long>(__ldcg(&dist[xrow])));
+                        dgx[u] = __ldcg(&delta_g[xrow]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                double c = 0.0, cg = 0.0;
+                if (ok[u]) {
+                    if constexpr (kMode == kModeBrandes) {
+                        c = share_sv[u] * ((1.0 + dx[u]) / sx[u]);
+                    } else {
+                        const double share = share_sv[u] / sx[u];
+                        const double inv = 1.0 / gx[u];
+                        c = share * (1.0 + dx[u]);
+                        cg = share * (inv * inv + dgx[u]);
+                        fixed_add(&grad_cpl[2 * static_cast<int64_t>(id[u])], c);
+                        fixed_add(&grad_eff[2 * static_cast<int64_t>(id[u])], cg);
+                    }
+                }
+                wbuf[u * 32 + lane] = c;
+                if constexpr (kMode == kModeGrad) {
+                    wbuf[32 * kU + u * 32 + lane] = cg;
+                }
+            }
+            __syncwarp();
+            const uint32_t lo = off > p0 ? off : p0;
+            const uint32_t end_own = off + count;
+            const uint32_t end_chunk = p0 + 32 * kU;
+            const uint32_t hi = end_own < end_chunk ? end_own : end_chunk;
+            for (uint32_t q = lo; q < hi; ++q) {
+                acc += wbuf[q - p0];
+                if constexpr (kMode == kModeGrad) {
+                    acc_g += wbuf[32 * kU + (q - p0)];
+                }
+            }
+            __syncwarp();
+        }
+        if (i < len) {
+            delta[row] = acc;
+            if constexpr (kMode == kModeGrad) {
+                delta_g[row] = acc_g;
+            }
         }
     }
 }

@@ -70,6 +70,22 @@ int ensure_workspace(ngx_graph* g, size_t bytes) {
     return NGX_OK;
 }
 
+int grow_buffer(ngx_graph* g, void** buf, size_t* cap, size_t bytes) {
+    if (bytes <= *cap && *buf != nullptr) {
+        return NGX_OK;
+    }
+    if (*buf != nullptr) {
+        NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        NGX_CUDA_TRY(cudaFree(*buf));
+        *buf = nullptr;
+        *cap = 0;
+    }
+    const size_t want = bytes + bytes / 4 + 256;  // headroom for source lists that grow a little between calls
+    NGX_CUDA_TRY(cudaMalloc(buf, want));
+    *cap = want;
+    return NGX_OK;
+}
+
 namespace {
 
 void release(ngx_graph* g) {
@@ -88,6 +104,8 @@ void release(ngx_graph* g) {
     cudaFree(g->d_workspace);
     cudaFree(g->d_items);
     cudaFree(g->d_persistent);
+    cudaFree(g->d_call_out);
+    cudaFree(g->d_call_dag);
     if (g->graph_exec != nullptr) {
         cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g->graph_exec));
     }

@@ -75,6 +75,13 @@ enum Counter : int {
 // Error codes written by kernels into a device flag (first writer wins).
 enum DeviceError : int { kDevOk = 0, kDevTimeout = 1, kDevAborted = 2 };
 
+// Bits of the lanes below this one in the warp.
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned mask;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(mask));
+    return mask;
+}
+
 // ------------------------------------------------------------------------------------------ exact accumulation
 // A non-negative finite double x = mant * 2^e (53-bit integer mant) is added exactly into 32-bit digits held in
 // 64-bit words: its bit 0 lands at absolute bit p = e - kAccExp0 >= 14 and the shifted mantissa touches at most three

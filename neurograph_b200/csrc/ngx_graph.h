@@ -67,6 +67,14 @@ struct ngx_graph {
     void* d_persistent = nullptr;  // output buffers the captured graph writes
     size_t persistent_bytes = 0;
 
+    // Grow-only output buffers of single-graph runs (summaries, per-source outputs; betweenness / gradient sums), so
+    // that a run allocates nothing once they have reached their size: stream-ordered frees were measured to stall a
+    // synchronizing call for hundreds of milliseconds while the pool returned memory.
+    void* d_call_out = nullptr;
+    size_t call_out_bytes = 0;
+    void* d_call_dag = nullptr;
+    size_t call_dag_bytes = 0;
+
     // bucket width per size class (floor(log2 n)), as a multiple of each graph's mean arc length (ngx_batch_autotune)
     double class_scale[64] = {};
     // stored forward index of each caller arc (-1 for zero weights), for ngx_graph_update_weights
@@ -85,6 +93,9 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
 
 // Grows the graph's cached workspace to at least `bytes`.
 int ensure_workspace(ngx_graph* g, size_t bytes);
+// Grows *buf (capacity *cap) to at least `bytes`; contents are not kept. Frees the old buffer only after the stream
+// is idle.
+int grow_buffer(ngx_graph* g, void** buf, size_t* cap, size_t bytes);
 
 // Bytes of device memory a run may use for workspaces (budget, or most of the free memory).
 size_t workspace_budget(const ngx_graph* g);

@@ -108,8 +108,11 @@ int alloc_outputs(ngx_graph* g, int64_t num_graphs, int64_t num_sources, int64_t
         o.block = g->d_persistent;
         o.owned = false;
     } else {
-        NGX_CUDA_TRY(cudaMallocAsync(&o.block, off, g->stream));
-        o.owned = true;
+        if (const int rc = grow_buffer(g, &g->d_call_out, &g->call_out_bytes, off); rc != NGX_OK) {
+            return rc;
+        }
+        o.block = g->d_call_out;
+        o.owned = false;
     }
     o.bytes = off;
     o.zeroed_bytes = zeroed;

@@ -80,11 +80,6 @@ inline size_t sssp_slot_bytes(int64_t n, int width) {
     return static_cast<size_t>(n) * (static_cast<size_t>(width) * 8 + 4 * 2 + 4 + 4 * 2 + 4) + 256;
 }
 
-__device__ __forceinline__ unsigned lanemask_lt() {
-    unsigned mask;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(mask));
-    return mask;
-}
 
 __device__ __forceinline__ double next_theta(double d_min, double delta) {
     const double theta = (floor(__ddiv_rn(d_min, delta)) + 1.0) * delta;
@@ -466,7 +461,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             }
             __syncthreads();
             if (use_lists) {
-                dag_fill(rg, n, dist, cnt, pred, soff, scnt, succ, lane, warp, nwarps);
+                dag_fill<kMode == kModeBrandes>(rg, n, dist, cnt, pred, soff, scnt, succ, lane, warp, nwarps);
                 __syncthreads();
                 dag_sort(soff, succ, nt);
                 __syncthreads();
@@ -506,7 +501,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                     break;
                 }
                 const unsigned level = s.level;
-                dag_sigma_level(g, list + start, len, level, sigma, cnt, lvl, soff, succ, list + start + len, &s.next_len, b.sigma_inexact);
+                dag_sigma_level<kMode == kModeBrandes>(g, list + start, len, level, sigma, cnt, lvl, soff, succ, list + start + len, &s.next_len,
+                                                       b.sigma_inexact, lane, warp, nwarps);
                 __syncthreads();
                 if (tid == 0) {
                     s.lvl_start = start + len;
@@ -527,9 +523,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             for (int level = levels - 1; level >= lowest; --level) {
                 const int start = __ldcg(&loff[level]);
                 const int end = __ldcg(&loff[level + 1]);
-                dag_delta_level<kMode>(g, list + start, end - start, dist, sigma, delta, delta_g, soff, succ, b.grad_cpl, b.grad_eff);
+                dag_delta_level<kMode>(g, list + start, end - start, dist, sigma, delta, delta_g, soff, succ, b.grad_cpl, b.grad_eff,
+                                       reinterpret_cast<double*>(s_acc_sum), lane, warp, nwarps);
                 __syncthreads();
             }
+            // the pair buffers borrowed the epilogue's accumulators, which must start the epilogue at zero
+            for (int k = tid; k < nwarps * 32 * delta_level_unroll(kMode) * (kMode == kModeGrad ? 2 : 1); k += blockDim.x) {
+                s_acc_sum[k] = 0ull;
+            }
+            __syncthreads();
             if (tid == 0) {
                 atomicAdd(&cnts[kDagLevels], static_cast<unsigned long long>(levels));
                 atomicAdd(&cnts[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
