@@ -19,8 +19,30 @@
 namespace ngx {
 namespace {
 
-int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_result* result, std::vector<unsigned long long>& host_bc,
-            std::vector<unsigned long long>& host_cpl, std::vector<unsigned long long>& host_eff, uint64_t* reached_pairs) {
+// 128-bit fixed-point sums -> doubles, scaled: out[i] = sign * value(sum[i]) / divisor (IEEE division, as on the host).
+__global__ void fixed_to_double_kernel(const unsigned long long* sums, int64_t count, double divisor, double sign, double* out) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count; i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double v = fixed_value(sums[2 * i], sums[2 * i + 1]);
+        out[i] = divisor == 1.0 ? sign * v : sign * v / divisor;
+    }
+}
+
+int convert_fixed(ngx_graph* g, const unsigned long long* sums, int64_t count, double divisor, double sign, double* d_out, double* h_out) {
+    if (count == 0) {
+        return NGX_OK;
+    }
+    const int block = 256;
+    const int64_t want = (count + block - 1) / block;
+    const int grid = static_cast<int>(want < 8 * g->sm_count ? want : 8 * g->sm_count);
+    fixed_to_double_kernel<<<grid, block, 0, g->stream>>>(sums, count, divisor, sign, d_out);
+    NGX_CUDA_TRY(cudaGetLastError());
+    NGX_CUDA_TRY(cudaMemcpyAsync(h_out, d_out, static_cast<size_t>(count) * 8, cudaMemcpyDeviceToHost, g->stream));
+    return NGX_OK;
+}
+
+// One Brandes (bc != nullptr) or adjoint (dcpl, deff != nullptr) run of a single-graph handle. The fixed-point sums
+// are converted on the device and copied straight into the caller's arrays.
+int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_result* result, double* bc, double* dcpl, double* deff) {
     if (const int rc = check_opts(g, opts); rc != NGX_OK) {
         return rc;
     }
@@ -36,10 +58,12 @@ int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_res
     const size_t bc_words = tile_mode == kModeBrandes ? 2 * n : 0;
     const size_t grad_words = tile_mode == kModeGrad ? 2 * m : 0;
     const size_t words = 1 + bc_words + 2 * grad_words;
-    if (const int rc = grow_buffer(g, &g->d_call_dag, &g->call_dag_bytes, words * 8); rc != NGX_OK) {
+    const size_t out_doubles = tile_mode == kModeBrandes ? n : 2 * m;  // converted results, after the sums
+    if (const int rc = grow_buffer(g, &g->d_call_dag, &g->call_dag_bytes, (words + out_doubles) * 8); rc != NGX_OK) {
         return rc;
     }
     unsigned long long* block = static_cast<unsigned long long*>(g->d_call_dag);
+    double* d_out = reinterpret_cast<double*>(block + words);
     NGX_CUDA_TRY(cudaMemsetAsync(block, 0, words * 8, g->stream));
     extra.sigma_inexact = reinterpret_cast<int*>(block);
     if (bc_words != 0) {
@@ -70,27 +94,21 @@ int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_res
             r->kernel_ms += first_ms;
         }
     }
-    if (rc == NGX_OK) {
-        host_bc.resize(bc_words);
-        host_cpl.resize(grad_words);
-        host_eff.resize(grad_words);
-        cudaError_t err = cudaSuccess;
-        if (bc_words != 0) {
-            err = cudaMemcpyAsync(host_bc.data(), extra.bc, bc_words * 8, cudaMemcpyDeviceToHost, g->stream);
+    if (rc == NGX_OK && g->n > 0) {
+        if (tile_mode == kModeBrandes) {
+            rc = convert_fixed(g, extra.bc, static_cast<int64_t>(n), 1.0, 1.0, d_out, bc);
+        } else {
+            // dCPL/dw = c / R and dE/dw = -f / R over the R reached ordered pairs (0 / 0 = NaN without any)
+            const double reached = static_cast<double>(r->reached_pairs);
+            rc = convert_fixed(g, extra.grad_cpl, static_cast<int64_t>(m), reached, 1.0, d_out, dcpl);
+            if (rc == NGX_OK) {
+                rc = convert_fixed(g, extra.grad_eff, static_cast<int64_t>(m), reached, -1.0, d_out + m, deff);
+            }
         }
-        if (err == cudaSuccess && grad_words != 0) {
-            err = cudaMemcpyAsync(host_cpl.data(), extra.grad_cpl, grad_words * 8, cudaMemcpyDeviceToHost, g->stream);
+        const cudaError_t err = cudaStreamSynchronize(g->stream);
+        if (rc == NGX_OK && err != cudaSuccess) {
+            rc = cuda_fail(err, "converting betweenness / gradients");
         }
-        if (err == cudaSuccess && grad_words != 0) {
-            err = cudaMemcpyAsync(host_eff.data(), extra.grad_eff, grad_words * 8, cudaMemcpyDeviceToHost, g->stream);
-        }
-        if (err == cudaSuccess) {
-            err = cudaStreamSynchronize(g->stream);
-        }
-        if (err != cudaSuccess) {
-            rc = cuda_fail(err, "copying betweenness / gradients");
-        }
-        *reached_pairs = r->reached_pairs;
     }
     cudaStreamSynchronize(g->stream);
     return rc;
@@ -107,37 +125,14 @@ int ngx_brandes(ngx_graph* graph, const ngx_apsp_opts* opts, double* bc, ngx_aps
     if (graph == nullptr || opts == nullptr || (bc == nullptr && graph->n > 0)) {
         return fail(NGX_INVALID_ARGUMENT, "ngx_brandes: graph, opts or bc is NULL");
     }
-    std::vector<unsigned long long> fixed, unused_a, unused_b;
-    uint64_t reached = 0;
-    const int rc = dag_run(graph, opts, kModeBrandes, result, fixed, unused_a, unused_b, &reached);
-    if (rc != NGX_OK) {
-        return rc;
-    }
-    for (int64_t v = 0; v < graph->n; ++v) {
-        bc[v] = fixed.empty() ? 0.0 : fixed_value(fixed[static_cast<size_t>(2 * v)], fixed[static_cast<size_t>(2 * v + 1)]);
-    }
-    return NGX_OK;
+    return dag_run(graph, opts, kModeBrandes, result, bc, nullptr, nullptr);
 }
 
 int ngx_apsp_grad(ngx_graph* graph, const ngx_apsp_opts* opts, double* dcpl, double* deff, ngx_apsp_result* result) {
     if (graph == nullptr || opts == nullptr || ((dcpl == nullptr || deff == nullptr) && graph->m_user > 0)) {
         return fail(NGX_INVALID_ARGUMENT, "ngx_apsp_grad: graph, opts, dcpl or deff is NULL");
     }
-    std::vector<unsigned long long> unused, fixed_cpl, fixed_eff;
-    uint64_t reached = 0;
-    const int rc = dag_run(graph, opts, kModeGrad, result, unused, fixed_cpl, fixed_eff, &reached);
-    if (rc != NGX_OK) {
-        return rc;
-    }
-    const double r = static_cast<double>(reached);
-    for (int64_t e = 0; e < graph->m_user; ++e) {
-        const size_t i = static_cast<size_t>(2 * e);
-        const double c = fixed_cpl.empty() ? 0.0 : fixed_value(fixed_cpl[i], fixed_cpl[i + 1]);
-        const double f = fixed_eff.empty() ? 0.0 : fixed_value(fixed_eff[i], fixed_eff[i + 1]);
-        dcpl[e] = c / r;
-        deff[e] = -f / r;
-    }
-    return NGX_OK;
+    return dag_run(graph, opts, kModeGrad, result, nullptr, dcpl, deff);
 }
 
 }  // extern "C"

@@ -27,6 +27,9 @@ constexpr uint32_t kNoLevel = 0xFFFFFFFFu;
 
 struct BrandesParams {
     DeviceCsr rg;                   // reverse CSR (in-arcs), regular lengths; Arc::col = source, Arc::id = forward stored index
+    const int32_t* arc_src;         // source vertex of each stored forward arc
+    int64_t m_total;                // stored forward arcs of all graphs
+    uint32_t* ws_tie;               // slots * n: bit s set when a relaxation of (v, s) tied with its distance
     double* ws_sigma;               // slots * n * kTile
     double* ws_delta;               // slots * n * kTile
     double* ws_delta_g;             // slots * n * kTile (adjoint only)
@@ -51,7 +54,7 @@ constexpr int kSuccPerPair = 2;  // successor-list capacity, in DAG arcs per (ve
 inline size_t brandes_slot_bytes(int64_t n, bool adjoint) {
     const size_t nt = static_cast<size_t>(n) * kTile;
     return nt * (8 + 8 + (adjoint ? 8 : 0) + 4 + 4 + 4) + static_cast<size_t>(n + 2) * 4 +
-           nt * 4 + (nt + 1) * 4 + nt * kSuccPerPair * 4 + 1024;
+           nt * 4 + (nt + 1) * 4 + static_cast<size_t>(n) * 4 + nt * kSuccPerPair * 4 + 1024;
 }
 
 __device__ __forceinline__ bool on_dag(unsigned long long du_bits, double len, unsigned long long dv_bits) {
@@ -66,44 +69,6 @@ __device__ __forceinline__ double warp_sum(double x) {
     return x;
 }
 
-// cnt[v][s] for every vertex of the graph (warp per vertex, lane per source).
-__device__ __forceinline__ void brandes_count(const DeviceCsr& rg, int64_t n, int nsrc, const int* s_src, const unsigned long long* dist, uint32_t* cnt,
-                                              int lane, int warp, int nwarps) {
-    for (int64_t v = warp; v < n; v += nwarps) {
-        const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
-        const bool active = lane < nsrc && dv != kInfBits && v != s_src[lane];
-        uint32_t c = 0;
-        if (__ballot_sync(0xFFFFFFFFu, active) != 0u) {
-            const int64_t beg = __ldg(&rg.row_ptr[v]);
-            const int64_t end = __ldg(&rg.row_ptr[v + 1]);
-            for (int64_t e0 = beg; e0 < end; e0 += 32) {
-                const int cntr = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
-                Arc a{ 0, 0, 0.0 };
-                if (lane < cntr) {
-                    a = rg.arcs[e0 + lane];
-                }
-                for (int j = 0; j < cntr; j += 4) {
-                    unsigned long long du[4];
-                    double len[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int jj = j + u < cntr ? j + u : 0;
-                        const int src = __shfl_sync(0xFFFFFFFFu, a.col, jj);
-                        len[u] = __shfl_sync(0xFFFFFFFFu, a.len, jj);
-                        du[u] = (active && j + u < cntr) ? __ldcg(&dist[static_cast<int64_t>(src) * kTile + lane]) : kInfBits;
-                    }
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        if (du[u] != kInfBits && on_dag(du[u], len[u], dv)) {
-                            ++c;
-                        }
-                    }
-                }
-            }
-        }
-        cnt[v * kTile + lane] = c;
-    }
-}
 
 // Pair-parallel walk over the deg x k (arc, ready source) pairs of one vertex, as in the SSSP expansion: pair
 // p = 32 i + lane takes arc p / k and the (p % k)-th ready source. Sums per source are gathered in arc order: in each
@@ -348,15 +313,39 @@ __device__ __forceinline__ void brandes_delta_vertex(const DeviceCsr& g, int v, 
 // a fixed order. sigma and delta then touch only DAG arcs.
 
 // cnt[v][s] = DAG predecessors; scnt[u][s] += 1 for each DAG arc u -> v (warp per vertex, lane per source);
-// pred[v][s] = reverse-CSR index of the first DAG in-arc found (the only one when cnt[v][s] == 1).
-__device__ __forceinline__ void dag_count(const DeviceCsr& rg, int64_t n, int nsrc, const int* s_src, const unsigned long long* dist, uint32_t* cnt,
-                                          uint32_t* scnt, uint32_t* pred, int lane, int warp, int nwarps) {
+// pred[v][s] = forward-CSR index of a DAG in-arc (the only one when cnt[v][s] == 1).
+// A lane whose tie bit stayed clear in the SSSP phase takes its single DAG arc from the predecessor key recorded
+// there (pred_key, which shares storage with sigma and is zeroed here for the sigma pass), after checking it; lanes
+// with ties (or a key that does not check out) count by scanning v's in-arcs.
+__device__ __forceinline__ void dag_count(const DeviceCsr& g, const DeviceCsr& rg, const int32_t* arc_src, int64_t m_total, int64_t n, int nsrc,
+                                          const int* s_src, const unsigned long long* dist, const uint32_t* tie, unsigned long long* pred_key,
+                                          uint32_t* cnt, uint32_t* scnt, uint32_t* pred, int lane, int warp, int nwarps) {
     for (int64_t v = warp; v < n; v += nwarps) {
         const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
         const bool active = lane < nsrc && dv != kInfBits && v != s_src[lane];
+        const bool tied = (__ldcg(&tie[v]) >> lane) & 1u;
+        const unsigned long long key = __ldcg(&pred_key[v * kTile + lane]);
+        pred_key[v * kTile + lane] = 0ull;  // sigma = 0.0
         uint32_t c = 0;
         uint32_t first = 0;
-        if (__ballot_sync(0xFFFFFFFFu, active) != 0u) {
+        bool scan = active;
+        if (active && !tied && (key >> 32) == (dv >> 32)) {
+            const uint32_t e = static_cast<uint32_t>(key);
+            if (static_cast<int64_t>(e) < m_total) {
+                const Arc a = g.arcs[e];
+                const int32_t u = __ldg(&arc_src[e]);
+                if (a.col == static_cast<int32_t>(v)) {
+                    const unsigned long long du = __ldcg(&dist[static_cast<int64_t>(u) * kTile + lane]);
+                    if (du != kInfBits && on_dag(du, a.len, dv)) {
+                        c = 1;
+                        first = e;
+                        scan = false;
+                        atomicAdd(&scnt[static_cast<int64_t>(u) * kTile + lane], 1u);
+                    }
+                }
+            }
+        }
+        if (__ballot_sync(0xFFFFFFFFu, scan) != 0u) {
             const int64_t beg = __ldg(&rg.row_ptr[v]);
             const int64_t end = __ldg(&rg.row_ptr[v + 1]);
             for (int64_t e0 = beg; e0 < end; e0 += 32) {
@@ -368,19 +357,20 @@ __device__ __forceinline__ void dag_count(const DeviceCsr& rg, int64_t n, int ns
                 for (int j = 0; j < cntr; j += 4) {
                     unsigned long long du[4];
                     double len[4];
-                    int src[4];
+                    int src[4], fwd[4];
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const int jj = j + u < cntr ? j + u : 0;
                         src[u] = __shfl_sync(0xFFFFFFFFu, a.col, jj);
+                        fwd[u] = __shfl_sync(0xFFFFFFFFu, a.id, jj);
                         len[u] = __shfl_sync(0xFFFFFFFFu, a.len, jj);
-                        du[u] = (active && j + u < cntr) ? __ldcg(&dist[static_cast<int64_t>(src[u]) * kTile + lane]) : kInfBits;
+                        du[u] = (scan && j + u < cntr) ? __ldcg(&dist[static_cast<int64_t>(src[u]) * kTile + lane]) : kInfBits;
                     }
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         if (du[u] != kInfBits && on_dag(du[u], len[u], dv)) {
                             if (c == 0) {
-                                first = static_cast<uint32_t>(e0 + j + u);
+                                first = static_cast<uint32_t>(fwd[u]);
                             }
                             ++c;
                             atomicAdd(&scnt[static_cast<int64_t>(src[u]) * kTile + lane], 1u);
@@ -433,17 +423,17 @@ __device__ __forceinline__ unsigned long long block_exclusive_scan(const uint32_
 
 // Fills the successor lists: each DAG arc u -> v is appended to (u, s), as its target v (kTarget: betweenness needs
 // nothing else) or as its forward-CSR index (the adjoint also needs the arc). A (v, s) with a single DAG predecessor
-// takes it from pred[v][s]; only lanes with ties re-scan v's in-arcs.
+// takes it from pred[v][s] (a forward index); only lanes with several re-scan v's in-arcs.
 template <bool kTarget>
-__device__ __forceinline__ void dag_fill(const DeviceCsr& rg, int64_t n, const unsigned long long* dist, const uint32_t* cnt, const uint32_t* pred,
-                                         const uint32_t* soff, uint32_t* sfill, uint32_t* succ, int lane, int warp, int nwarps) {
+__device__ __forceinline__ void dag_fill(const DeviceCsr& rg, const int32_t* arc_src, int64_t n, const unsigned long long* dist, const uint32_t* cnt,
+                                         const uint32_t* pred, const uint32_t* soff, uint32_t* sfill, uint32_t* succ, int lane, int warp, int nwarps) {
     for (int64_t v = warp; v < n; v += nwarps) {
         const uint32_t c = __ldcg(&cnt[v * kTile + lane]);
         if (c == 1u) {
-            const Arc a = rg.arcs[__ldcg(&pred[v * kTile + lane])];
-            const int64_t urow = static_cast<int64_t>(a.col) * kTile + lane;
+            const uint32_t e = __ldcg(&pred[v * kTile + lane]);
+            const int64_t urow = static_cast<int64_t>(__ldg(&arc_src[e])) * kTile + lane;
             const uint32_t pos = atomicAdd(&sfill[urow], 1u);
-            succ[__ldcg(&soff[urow]) + pos] = kTarget ? static_cast<uint32_t>(v) : static_cast<uint32_t>(a.id);
+            succ[__ldcg(&soff[urow]) + pos] = kTarget ? static_cast<uint32_t>(v) : e;
         }
         const bool active = c >= 2u;
         if (__ballot_sync(0xFFFFFFFFu, active) == 0u) {

@@ -101,6 +101,7 @@ void release(ngx_graph* g) {
     cudaFree(g->d_arcs_inverse);
     cudaFree(g->d_rrow_ptr);
     cudaFree(g->d_rarcs);
+    cudaFree(g->d_arc_src);
     cudaFree(g->d_workspace);
     cudaFree(g->d_items);
     cudaFree(g->d_persistent);
@@ -221,6 +222,7 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
     std::vector<int64_t> rrow_ptr;
     std::vector<Arc> regular;
     std::vector<Arc> inverse;
+    std::vector<int32_t> arc_src;
     row_ptr.reserve(static_cast<size_t>(n_total + count));
     rrow_ptr.reserve(static_cast<size_t>(n_total + count));
     regular.reserve(static_cast<size_t>(m_total));
@@ -254,6 +256,7 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
                 const int32_t id = static_cast<int32_t>(user_arc_off + e);
                 g->stored_of_user[static_cast<size_t>(id)] = static_cast<int32_t>(regular.size());
                 regular.push_back(Arc{ v, id, a });
+                arc_src.push_back(static_cast<int32_t>(u));
                 inverse.push_back(Arc{ v, id, 1.0 / a });
                 part_regular += a;
                 part_inverse += 1.0 / a;
@@ -313,6 +316,7 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
     if (rc == NGX_OK) rc = upload(&g->d_arcs_inverse, inverse);
     if (rc == NGX_OK) rc = upload(&g->d_rrow_ptr, rrow_ptr);
     if (rc == NGX_OK) rc = upload(&g->d_rarcs, rarcs);
+    if (rc == NGX_OK) rc = upload(&g->d_arc_src, arc_src);
     if (rc == NGX_OK) {
         const cudaError_t err = cudaStreamSynchronize(g->stream);
         if (err != cudaSuccess) {

@@ -44,6 +44,7 @@ struct ngx_graph {
     // Reverse CSR (in-arcs) with regular lengths; Arc::col is the arc's source, Arc::id its index in the stored forward CSR.
     int64_t* d_rrow_ptr = nullptr;
     ngx::Arc* d_rarcs = nullptr;
+    int32_t* d_arc_src = nullptr;  // source vertex (graph-local) of each stored forward arc
 
     double mean_len_regular = 1.0;
     double mean_len_inverse = 1.0;

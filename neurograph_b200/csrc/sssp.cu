@@ -234,6 +234,8 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
         const size_t nt = static_cast<size_t>(n) * kTile;
         ws = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(ws) + 255) & ~uintptr_t(255));
         bp.rg = g->reverse_csr();
+        bp.arc_src = g->d_arc_src;
+        bp.m_total = g->m_stored;
         bp.ws_sigma = reinterpret_cast<double*>(ws);
         ws += static_cast<size_t>(slots) * nt * 8;
         bp.ws_delta = reinterpret_cast<double*>(ws);
@@ -256,6 +258,8 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
         ws += static_cast<size_t>(slots) * (nt + 1) * 4;
         // list entries pack (vertex << 5 | source) into 32 bits; larger graphs use the arc-scanning passes
         bp.succ_capacity = n < (int64_t(1) << 26) ? static_cast<int64_t>(nt) * kSuccPerPair : 0;
+        bp.ws_tie = reinterpret_cast<uint32_t*>(ws);
+        ws += static_cast<size_t>(slots) * n * 4;
         bp.ws_succ = reinterpret_cast<uint32_t*>(ws);
         if (extra != nullptr) {
             bp.bc = extra->bc;

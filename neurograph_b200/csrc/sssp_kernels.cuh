@@ -108,27 +108,58 @@ struct TileShared {
 // Expands vertex v for the k sources pending on it. The deg(v) x k (arc, source) pairs are spread over the 32 lanes:
 // pair p = 32 i + lane takes arc p / k and the (p % k)-th pending source, so no lane idles when few sources are
 // pending, and when all 32 are, every iteration reads one whole distance row d[x][0..31] (256 contiguous bytes).
-template <int kUnroll>
+// kTrack (betweenness / adjoint): each improvement of d[x][s] to nb offers the key (top 32 bits of nb, arc index) to
+// pred_key[x][s] with an atomic minimum, so the key of the smallest distance wins whatever the order of the stores;
+// a relaxation that ties with d[x][s] sets bit s of tie[x]. Every DAG arc is relaxed with final distances, so a
+// (x, s) whose tie bit stayed clear has exactly one DAG predecessor: the arc in its key (the DAG count pass checks it).
+// For that, no (v, s) may be expanded twice with one distance (the repeat would look like a tie): an expansion reads
+// the newest distance, and the improvement that produced it has queued another expansion. last[v][s] keeps the
+// distance of the latest expansion, and sources whose distance has not changed since are dropped from the next.
+template <int kUnroll, bool kTrack>
 __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, int lane, unsigned long long* __restrict__ dist, uint32_t* pend_cur,
                                                uint32_t* pend_nxt, uint32_t* far, int32_t* q_nxt, int* qlen_nxt, uint32_t* stamp, unsigned next_stamp,
-                                               double theta, unsigned long long& expansions, unsigned long long& lane_expansions) {
-    const uint32_t amask = __ldcg(&pend_cur[v]);
+                                               double theta, unsigned long long& expansions, unsigned long long& lane_expansions,
+                                               unsigned long long* pred_key, uint32_t* tie, unsigned long long* last) {
+    uint32_t amask = __ldcg(&pend_cur[v]);
     if (amask == 0) {
         return;
     }
+    const uint32_t amask0 = amask;
     __syncwarp();
-    const int k = __popc(amask);
-    expansions += 1;
-    lane_expansions += static_cast<unsigned long long>(k);
-    // lane r < k holds the r-th pending source and its distance to v
-    const int rank_src = lane < k ? static_cast<int>(__fns(amask, 0, lane + 1)) : 0;
-    const double rank_dv = __longlong_as_double(static_cast<long long>(__ldcg(&dist[static_cast<int64_t>(v) * kTile + rank_src])));
     if (lane == 0) {
         pend_cur[v] = 0u;
         if (__ldcg(&far[v]) & amask) {
             atomicAnd(&far[v], ~amask);  // those far marks are superseded by the near values expanded now
         }
     }
+    int k = __popc(amask);
+    // lane r < k holds the r-th pending source and its distance to v
+    int rank_src = lane < k ? static_cast<int>(__fns(amask, 0, lane + 1)) : 0;
+    unsigned long long rank_bits = __ldcg(&dist[static_cast<int64_t>(v) * kTile + rank_src]);
+    if constexpr (kTrack) {
+        unsigned long long* const slot = &last[static_cast<int64_t>(v) * kTile + rank_src];
+        const bool repeat = lane < k && __ldcg(slot) == rank_bits;
+        if (lane < k && !repeat) {
+            *slot = rank_bits;
+        }
+        const uint32_t drop = __reduce_or_sync(kFullMask, repeat ? (1u << rank_src) : 0u);
+        if (drop != 0u) {
+            amask &= ~drop;
+            if (amask == 0u) {
+                return;
+            }
+            // re-rank the remaining sources; their distances come from the lanes that read them
+            const int new_k = __popc(amask);
+            const int src_new = lane < new_k ? static_cast<int>(__fns(amask, 0, lane + 1)) : 0;
+            const int old_rank = __popc(amask0 & ((1u << src_new) - 1u));
+            rank_bits = __shfl_sync(kFullMask, rank_bits, old_rank);
+            rank_src = src_new;
+            k = new_k;
+        }
+    }
+    expansions += 1;
+    lane_expansions += static_cast<unsigned long long>(k);
+    const double rank_dv = __longlong_as_double(static_cast<long long>(rank_bits));
     const int64_t beg = __ldg(&g.row_ptr[v]);
     const int deg = static_cast<int>(__ldg(&g.row_ptr[v + 1]) - beg);
     const Arc* arcs = g.arcs + beg;
@@ -143,10 +174,12 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, int la
         int src[kUnroll];
         double nd[kUnroll];
         unsigned long long cur[kUnroll];
+        uint32_t eidx[kUnroll];
         bool valid[kUnroll];
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
             valid[u] = a < deg;
+            eidx[u] = static_cast<uint32_t>(beg + a);
             src[u] = __shfl_sync(kFullMask, rank_src, r);
             const double dvs = __shfl_sync(kFullMask, rank_dv, r);
             x[u] = 0;
@@ -172,6 +205,13 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, int la
                 const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd[u]));
                 if (nb < cur[u]) {
                     const unsigned long long old = atomicMin(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]], nb);
+                    if constexpr (kTrack) {
+                        if (nb < old) {
+                            atomicMin(&pred_key[static_cast<int64_t>(x[u]) * kTile + src[u]], ((nb >> 32) << 32) | eidx[u]);
+                        } else if (nb == old) {
+                            atomicOr(&tie[x[u]], 1u << src[u]);
+                        }
+                    }
                     if (nb < old) {
                         const uint32_t bit = 1u << src[u];
                         if (nd[u] < theta) {
@@ -181,6 +221,8 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, int la
                             atomicOr(&far[x[u]], bit);
                         }
                     }
+                } else if (kTrack && nb == cur[u]) {
+                    atomicOr(&tie[x[u]], 1u << src[u]);
                 }
             }
             const unsigned pmask = __ballot_sync(kFullMask, push);
@@ -237,6 +279,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     uint32_t* scnt = nullptr;
     uint32_t* soff = nullptr;
     uint32_t* succ = nullptr;
+    uint32_t* tie = nullptr;
     __shared__ unsigned long long s_part[kBlock + 1];
     if constexpr (kMode != kModeApsp) {
         scnt = b.ws_scnt + slot * nt_slot;
@@ -252,9 +295,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         lvl = b.ws_lvl + slot * nt_slot;
         list = b.ws_list + slot * nt_slot;
         loff = b.ws_loff + slot * (n_slot + 2);
+        tie = b.ws_tie + slot * n_slot;
+        for (int64_t i = tid; i < n_slot; i += blockDim.x) {
+            tie[i] = 0u;
+        }
         for (int64_t i = tid; i < nt_slot; i += blockDim.x) {
-            sigma[i] = 0.0;
-            delta[i] = 0.0;
+            sigma[i] = __longlong_as_double(-1ll);  // all-ones: the empty predecessor key (sigma is zeroed by the count pass)
+            delta[i] = __longlong_as_double(-1ll);  // all-ones: no expansion yet (delta holds last[][] in the SSSP phase)
             if constexpr (kMode == kModeGrad) {
                 delta_g[i] = 0.0;
             }
@@ -350,8 +397,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 const unsigned next_stamp = s.stamp + 1u;
                 const double theta = s.theta;
                 for (int i = warp; i < qlen; i += nwarps) {
-                    batched_expand<kUnroll>(g, __ldcg(&q_cur[i]), lane, dist, pend_cur, pend_nxt, far, q_nxt, &s.qlen[cur ^ 1], stamp, next_stamp, theta,
-                                            expansions, lane_expansions);
+                    batched_expand<kUnroll, kMode != kModeApsp>(g, __ldcg(&q_cur[i]), lane, dist, pend_cur, pend_nxt, far, q_nxt, &s.qlen[cur ^ 1],
+                                                                stamp, next_stamp, theta, expansions, lane_expansions,
+                                                                reinterpret_cast<unsigned long long*>(sigma), tie,
+                                                                reinterpret_cast<unsigned long long*>(delta));
                 }
                 __syncthreads();
                 if (tid == 0) {
@@ -452,7 +501,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             // ------------------------------------------------------------ shortest-path DAG: counts, sigma, delta
             // the level lists are built only after the successor lists: their storage holds pred[][] until then
             uint32_t* const pred = reinterpret_cast<uint32_t*>(list);
-            dag_count(rg, n, nsrc, s_src, dist, cnt, scnt, pred, lane, warp, nwarps);
+            dag_count(g, rg, b.arc_src, b.m_total, n, nsrc, s_src, dist, tie, reinterpret_cast<unsigned long long*>(sigma), cnt, scnt, pred, lane, warp,
+                      nwarps);
             __syncthreads();
             const unsigned long long dag_arcs = block_exclusive_scan(scnt, soff, nt, s_part);
             const bool use_lists = dag_arcs <= static_cast<unsigned long long>(b.succ_capacity);
@@ -461,7 +511,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             }
             __syncthreads();
             if (use_lists) {
-                dag_fill<kMode == kModeBrandes>(rg, n, dist, cnt, pred, soff, scnt, succ, lane, warp, nwarps);
+                dag_fill<kMode == kModeBrandes>(rg, b.arc_src, n, dist, cnt, pred, soff, scnt, succ, lane, warp, nwarps);
                 __syncthreads();
                 dag_sort(soff, succ, nt);
                 __syncthreads();
@@ -633,20 +683,23 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 const int64_t row = v * kTile + lane;
                 if constexpr (kMode == kModeBrandes) {
                     // BrandesVariant.h:156: every settled vertex but the source gains its dependency
-                    const double dep = (valid && v != my_src) ? __ldcg(&delta[row]) : 0.0;
+                    const double dep = (valid && v != my_src && bits != kInfBits) ? __ldcg(&delta[row]) : 0.0;
                     const double total = warp_sum(dep);
                     if (lane == 0 && total > 0.0) {
                         fixed_add(&bc_g[2 * v], total);
                     }
                 }
-                sigma[row] = 0.0;
-                delta[row] = 0.0;
+                sigma[row] = __longlong_as_double(-1ll);
+                delta[row] = __longlong_as_double(-1ll);
                 if constexpr (kMode == kModeGrad) {
                     delta_g[row] = 0.0;
                 }
                 cnt[row] = 0u;
                 lvl[row] = kNoLevel;
                 scnt[row] = 0u;
+                if (lane == 0) {
+                    tie[v] = 0u;
+                }
             }
             if (!valid) {
                 continue;
