@@ -115,7 +115,27 @@ typedef struct {
     double* src_sum_inverse;  /* per source: exactly rounded sum of 1/d */
     uint64_t* src_unreachable;/* per source: unreachable vertices */
     uint64_t* src_arcs;       /* per source: traversed arcs */
+    uint64_t* acc_digits;     /* 2 x NGX_ACC_DIGITS: the exact sums of d and of 1/d before rounding (normalized digits,
+                                 for merging the runs of several ranks exactly; see ngx_exact_round) */
 } ngx_apsp_result;
+
+/*
+ * Exact sums. An accumulator is NGX_ACC_DIGITS unsigned 64-bit words, digit i holding a multiple of
+ * 2^(32 i + NGX_ACC_EXP0); any non-negative finite double is a sum of at most three such digits. Digit-wise integer
+ * addition is associative, so accumulators of different ranks (or runs) can be summed word by word, in any order
+ * (e.g. an all-reduce with SUM), as long as each word stays below 2^64: normalized digits are below 2^32, so up to
+ * 2^32 accumulators can be summed before ngx_exact_round. Replaces the sequential double sums of
+ * AllPairsShortestPath.h:146-158 when results of several ranks are combined.
+ */
+#define NGX_ACC_DIGITS 72
+#define NGX_ACC_EXP0 (-1088)
+
+/* Adds values[0..count) (non-negative finite doubles, else NGX_INVALID_ARGUMENT) into the accumulator `digits` and
+ * normalizes it. Host-only: needs no GPU. */
+NGX_API int ngx_exact_accumulate(const double* values, int64_t count, uint64_t* digits);
+
+/* Normalizes the accumulator `digits` in place (carries) and returns its value rounded once to nearest-even. */
+NGX_API double ngx_exact_round(uint64_t* digits);
 
 NGX_API const char* ngx_status_string(int status);
 NGX_API const char* ngx_last_error(void);

@@ -35,6 +35,7 @@ MODES = {"batched": 0, "plain": 1}
 TASKS = {"apsp": 0, "brandes": 1, "grad": 2}
 SIZE_CLASSES = 32
 TILE = 32
+ACC_DIGITS = 72
 
 
 class NgxError(RuntimeError):
@@ -73,7 +74,7 @@ class _Result(C.Structure):
         ("dag_levels", C.c_uint64), ("dag_entries", C.c_uint64), ("dag_scan_tiles", C.c_uint64),
         ("phase_cycles", C.c_uint64 * 5),
         ("hist", C.c_void_p), ("src_sum", C.c_void_p), ("src_max", C.c_void_p), ("src_sum_inverse", C.c_void_p),
-        ("src_unreachable", C.c_void_p), ("src_arcs", C.c_void_p),
+        ("src_unreachable", C.c_void_p), ("src_arcs", C.c_void_p), ("acc_digits", C.c_void_p),
     ]
 
 
@@ -83,7 +84,7 @@ _LIB = None
 EXPORTED = [
     "ngx_status_string", "ngx_last_error", "ngx_version", "ngx_graph_create", "ngx_graph_destroy", "ngx_graph_size",
     "ngx_graph_request_abort", "ngx_graph_set_stream", "ngx_graph_set_memory_budget", "ngx_apsp", "ngx_sssp_rows", "ngx_brandes",
-    "ngx_apsp_grad", "ngx_batch_create", "ngx_batch_run", "ngx_batch_autotune", "ngx_graph_update_weights", "ngx_apsp_noalloc",
+    "ngx_apsp_grad", "ngx_batch_create", "ngx_batch_run", "ngx_batch_autotune", "ngx_graph_update_weights", "ngx_apsp_noalloc", "ngx_exact_accumulate", "ngx_exact_round",
 ]
 
 
@@ -115,6 +116,9 @@ def library() -> C.CDLL:
         lib.ngx_batch_autotune.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         lib.ngx_graph_update_weights.argtypes = [C.c_void_p, C.c_void_p]
         lib.ngx_apsp_noalloc.argtypes = [C.c_void_p, C.POINTER(_Opts), C.POINTER(_Result)]
+        lib.ngx_exact_accumulate.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        lib.ngx_exact_round.argtypes = [C.c_void_p]
+        lib.ngx_exact_round.restype = C.c_double
         _LIB = lib
     return _LIB
 
@@ -149,6 +153,7 @@ class ApspResult:
     hist: np.ndarray | None = None
     per_source: dict | None = None
     cluster_sizes: dict = field(default_factory=dict)
+    acc_digits: np.ndarray | None = None  # (2, ACC_DIGITS) exact sums of d and 1/d before rounding (exact=True)
 
     @property
     def gteps(self) -> float:
@@ -234,7 +239,7 @@ class Graph:
         return out
 
     @staticmethod
-    def _result_struct(hist_bins, per_source, k):
+    def _result_struct(hist_bins, per_source, k, exact=False):
         r = _Result()
         hist = np.zeros(hist_bins, np.uint64) if hist_bins > 0 else None
         per = None
@@ -245,14 +250,22 @@ class Graph:
             r.src_unreachable, r.src_arcs = per["unreachable"].ctypes.data, per["arcs"].ctypes.data
         if hist is not None:
             r.hist = hist.ctypes.data
+        if exact:
+            digits = np.zeros((2, ACC_DIGITS), np.uint64)
+            r.acc_digits = digits.ctypes.data
+            r._digits = digits  # kept alive with the struct
         return r, hist, per
 
     def apsp(self, sources=None, metric="regular", mode="batched", delta=0.0, hist_bins=0, hist_max=0.0,
-             per_source=False, block_threads=0, ctas_per_sm=0, max_iterations=0) -> ApspResult:
+             per_source=False, block_threads=0, ctas_per_sm=0, max_iterations=0, exact=False) -> ApspResult:
+        """exact=True also returns the unrounded exact sums (acc_digits), for merging the runs of several ranks."""
         opts, srcs, k = self._opts(sources, metric, mode, delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations)
-        r, hist, per = self._result_struct(hist_bins, per_source, k)
+        r, hist, per = self._result_struct(hist_bins, per_source, k, exact)
         _check(library().ngx_apsp(self._handle, C.byref(opts), C.byref(r)))
-        return self._result(r, hist, per, k)
+        out = self._result(r, hist, per, k)
+        if exact:
+            out.acc_digits = r._digits
+        return out
 
     def apsp_noalloc(self, sources=None, metric="regular", delta=0.0, hist_bins=0, hist_max=0.0, per_source=False,
                      block_threads=0, ctas_per_sm=0, max_iterations=0) -> ApspResult:
@@ -377,6 +390,24 @@ class Batch:
         if flat.size != sum(self.ms):
             raise ValueError("weights do not match the batch's arcs")
         _check(library().ngx_graph_update_weights(self._handle, flat.ctypes.data if flat.size else None))
+
+
+def exact_accumulate(values, digits=None) -> np.ndarray:
+    """Adds non-negative finite doubles exactly into an accumulator ((ACC_DIGITS,) uint64, new if None). Host only."""
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    d = np.zeros(ACC_DIGITS, np.uint64) if digits is None else digits
+    if d.dtype != np.uint64 or d.size != ACC_DIGITS or not d.flags.c_contiguous:
+        raise ValueError("digits must be a contiguous uint64 array of ACC_DIGITS words")
+    _check(library().ngx_exact_accumulate(v.ctypes.data if v.size else None, v.size, d.ctypes.data))
+    return d
+
+
+def exact_round(digits) -> float:
+    """The accumulator's value rounded once to nearest-even (digits may be a sum of several normalized accumulators)."""
+    d = np.array(digits, dtype=np.uint64, copy=True)
+    if d.size != ACC_DIGITS:
+        raise ValueError("expected ACC_DIGITS words")
+    return float(library().ngx_exact_round(d.ctypes.data))
 
 
 def version() -> str:

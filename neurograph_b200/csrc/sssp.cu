@@ -419,6 +419,9 @@ int collect_graph(ngx_graph* g, const RunOutputs& o, const unsigned long long* a
     acc_normalize(acc + kAccDigits);
     r->sum_distances = acc_round_normalized(acc);
     r->sum_inverse = acc_round_normalized(acc + kAccDigits);
+    if (r->acc_digits != nullptr) {
+        std::memcpy(r->acc_digits, acc, sizeof(acc));
+    }
     std::memcpy(&r->diameter, &counters[kDiameterBits], sizeof(double));
     r->unreachable = counters[kUnreachable];
     r->reached_pairs = counters[kReachedPairs];
