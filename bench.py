@@ -63,6 +63,10 @@ def parse():
     ap.add_argument("--sources-per-step", type=int, default=DEFAULT_SOURCES_PER_STEP)
     ap.add_argument("--n", type=int, default=WORKLOAD["n"])
     ap.add_argument("--degree", type=float, default=WORKLOAD["mean_degree"])
+    ap.add_argument("--length-scale", type=float, default=WORKLOAD["length_scale"])
+    ap.add_argument("--sigma", type=float, default=1.0, help="log-normal sigma of the weights")
+    ap.add_argument("--workload", choices=["single", "uneven-batch"], default="single",
+                    help="single: one connectome (the headline); uneven-batch: 512 connectomes of 500-20000 vertices in one handle")
     ap.add_argument("--delta", type=float, default=0.25)
     ap.add_argument("--mode", choices=["brandes", "apsp", "grad", "plain"], default="brandes",
                     help="what one step runs: APSP+Brandes (the headline), APSP only, APSP+gradient, or the plain per-source form")
@@ -74,10 +78,19 @@ def parse():
     return ap.parse_args()
 
 
-def make_graph(n, degree):
+def make_graph(n, degree, length_scale=WORKLOAD["length_scale"], sigma=1.0):
     from neurograph_b200 import synth
 
-    return synth.connectome(n, degree, WORKLOAD["length_scale"], weights="lognormal", mu=0.0, sigma=1.0, seed=WORKLOAD["seed"])
+    return synth.connectome(n, degree, length_scale, weights="lognormal", mu=0.0, sigma=sigma, seed=WORKLOAD["seed"])
+
+
+def workload_overrides(args):
+    """Config keys that differ from the default connectome (other generator parameters on the same code path)."""
+    if (args.n, args.degree, args.length_scale, args.sigma) == (WORKLOAD["n"], WORKLOAD["mean_degree"], WORKLOAD["length_scale"], 1.0):
+        return {}
+    return {"workload": f"single graph: synthetic connectome N={args.n}, out-degree Poisson({args.degree:g}), kernel "
+                        f"exp(-d/{args.length_scale:g}), log-normal(0,{args.sigma:g}) FP64 weights; mode {args.mode}",
+            "mean_degree": args.degree, "length_scale": args.length_scale, "weights": f"lognormal(0,{args.sigma:g})"}
 
 
 def reduce_over_ranks(dist, x, op, device):
@@ -212,7 +225,7 @@ def run_reference(args, rank, world):
         return
     import multiprocessing as mp
 
-    c = make_graph(args.n, args.degree)
+    c = make_graph(args.n, args.degree, args.length_scale, args.sigma)
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     directory = tempfile.mkdtemp(prefix="ngx_ref_")
     for name, arr in (("row_ptr", c.row_ptr), ("col", c.col), ("w", c.w)):
@@ -269,6 +282,105 @@ def cpu_baseline_single_core(c, sources, budget_s=12.0):
                       "CPU restatement of the reference Dijkstra/Brandes (bit-exact with the reference on integer weights)"}
 
 
+UNEVEN_BATCH = {"graphs": 512, "n_min": 500, "n_max": 20000, "degree_min": 5.0, "degree_max": 60.0, "length_scale": 0.1,
+                "weights": "45% integer U{1..10}, 45% log-normal(0,1), 10% unit", "seed": 3, "hist_max": 200.0}
+
+
+def uneven_batch_graphs(rank=0, world=1):
+    """The uneven-batch workload: 512 seeded connectomes (rank r builds graphs r, r + world, ...)."""
+    from neurograph_b200 import synth
+
+    cfg = UNEVEN_BATCH
+    rng = np.random.default_rng(cfg["seed"])
+    specs = []
+    for i in range(cfg["graphs"]):
+        n = int(rng.integers(cfg["n_min"], cfg["n_max"] + 1))
+        deg = float(rng.uniform(cfg["degree_min"], cfg["degree_max"]))
+        u = rng.random()
+        kind = "int" if u < 0.45 else ("lognormal" if u < 0.9 else "unit")
+        specs.append((n, deg, kind))
+    graphs = []
+    for i in range(rank, cfg["graphs"], world):
+        n, deg, kind = specs[i]
+        # the dense sampler on the GPU: its O(n^2) CPU form takes over half an hour for the 512 graphs
+        c = synth.connectome(n, deg, cfg["length_scale"], weights=kind, seed=10_000 + i, use_gpu=True)
+        graphs.append((c.n, c.row_ptr, c.col, c.w))
+    return graphs
+
+
+def run_uneven_batch(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ranks, local_rank):
+    """All sources of every graph of the batch per step (APSP summaries + histogram + Brandes), one persistent launch,
+    replayed from a captured CUDA graph after the first step."""
+    t0 = time.perf_counter()
+    graphs = uneven_batch_graphs(rank, world)
+    m_total = sum(int(g[2].size) for g in graphs)
+    log(f"[bench] {len(graphs)} graphs, {m_total} arcs generated in {time.perf_counter() - t0:.1f}s")
+    stream = torch.cuda.Stream()
+    b = ngx.Batch(graphs, device=local_rank)
+    b.set_stream(stream.cuda_stream)
+    run = dict(task="brandes", hist_bins=HIST_BINS, hist_max=UNEVEN_BATCH["hist_max"], use_cuda_graph=True)
+    for _ in range(args.warmup):
+        b.run(**run)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    clocks.wait_first_sample()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    arcs, kernel_ms = 0, 0.0
+    for _ in range(args.steps):
+        results, _ = b.run(**run)
+        arcs += sum(r.traversed_arcs for r in results)
+        kernel_ms += results[0].kernel_ms if results else 0.0
+    ev1.record(stream)
+    barrier()
+    clock_info = clocks.stop()
+    elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    value = sum_over_ranks(float(arcs)) / elapsed / 1e9
+    reached = 0
+    for (n, rp, c, w), r in zip(graphs, results):
+        reached += r.reached_pairs + n
+    per_arc, per_vertex = 76.0, 56.0
+    alg = (per_arc * arcs + per_vertex * reached * args.steps) / args.steps
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (kernel_ms / args.steps / 1e3) / 1e9
+    b.close()
+    e2e = None
+    if not args.no_e2e:
+        pinned = [(n, torch.from_numpy(rp).pin_memory().numpy(), torch.from_numpy(c).pin_memory().numpy(),
+                   torch.from_numpy(w).pin_memory().numpy()) for n, rp, c, w in graphs]
+        h2d = sum(rp.nbytes + c.nbytes + w.nbytes for _, rp, c, w in pinned)
+        barrier()
+        t1 = time.perf_counter()
+        with ngx.Batch(pinned, device=local_rank) as be:
+            res, extra = be.run(task="brandes", hist_bins=HIST_BINS, hist_max=UNEVEN_BATCH["hist_max"])
+        barrier()
+        e2e_elapsed = max_over_ranks(time.perf_counter() - t1)
+        d2h = sum(x.nbytes for x in extra) + sum(r.hist.nbytes for r in res)
+        e2e = {"value": sum_over_ranks(float(sum(r.traversed_arcs for r in res))) / e2e_elapsed / 1e9, "unit": "GTEPS",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "timing": "wall clock, synchronized; batch created from pinned host CSRs, one all-sources run, results to host"}
+    if rank != 0:
+        return
+    line = {
+        "metric": "APSP+Brandes GTEPS (uneven multi-graph batch)", "value": value, "unit": "GTEPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(UNEVEN_BATCH, workload="uneven batch: 512 connectomes, N ~ U{500..20000}, out-degree ~ U[5,60], "
+                       "kernel exp(-d/0.1), mixed weights; all-source APSP + 1024-bin histogram + Brandes per graph, one "
+                       "persistent launch replayed from a CUDA graph", arcs=m_total, graphs_on_rank0=len(graphs),
+                       l2="workspaces (GBs) exceed the 126 MB L2; no flush needed"),
+        "gpu_launches": args.steps * 2,
+        "clocks": clock_info,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)", "traffic": None,
+                     "algorithmic_bytes_per_launch": alg, "kernel": "tile_kernel<Brandes> (ngx_batch_run)"},
+        "e2e": e2e,
+        "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
@@ -303,8 +415,15 @@ def main():
     def sum_over_ranks(x):
         return reduce_over_ranks(dist, x, "sum", "cuda")
 
+    if args.workload == "uneven-batch":
+        run_uneven_batch(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ranks, local_rank)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
     t0 = time.perf_counter()
-    c = make_graph(args.n, args.degree)
+    c = make_graph(args.n, args.degree, args.length_scale, args.sigma)
     log(f"[bench] graph n={c.n} m={c.m} generated in {time.perf_counter() - t0:.1f}s")
     stream = torch.cuda.Stream()
     g = ngx.Graph(c.n, c.row_ptr, c.col, c.w, device=local_rank)
@@ -433,7 +552,7 @@ def main():
         "metric": metric, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(WORKLOAD, n=c.n, arcs=c.m, mode=args.mode, sources_per_step=args.sources_per_step, delta=args.delta, hist_bins=HIST_BINS,
+        "config": dict(WORKLOAD, **workload_overrides(args), n=c.n, arcs=c.m, mode=args.mode, sources_per_step=args.sources_per_step, delta=args.delta, hist_bins=HIST_BINS,
                        hist_max=hist_max, parallelism=f"sources sharded over {world} GPU(s), no data-path collective",
                        l2="graph (320 MB CSR + reverse CSR) and workspaces (GBs) exceed the 126 MB L2; no flush needed"),
         "gpu_launches": gpu_launches,
