@@ -4,8 +4,8 @@
 
 Workload (the batched single-graph configuration): a synthetic connectome with N = 100,000 vertices in the unit cube,
 out-degree Poisson(100) (about 1e7 arcs after merging repeated targets), spatial kernel exp(-d / 0.08), log-normal(0, 1)
-FP64 weights, generated from a fixed seed. One step = one batch of sources (a fixed seeded permutation of all
-vertices, consumed batch after batch) run through ngx_brandes: distances by batched delta-stepping, the fused APSP
+FP64 weights, generated from a fixed seed. One step = one batch of sources (a contiguous chunk of the library's
+all-sources order, ngx_graph_source_order, consumed batch after batch) run through ngx_brandes: distances by batched delta-stepping, the fused APSP
 summaries (exact sums of d and 1/d, diameter, unreachable count, 1024-bin distance histogram, per-source outputs) and
 Brandes betweenness, in one persistent launch. GTEPS = traversed arcs (sum over sources of the out-degrees of the
 vertices they reach) / seconds.
@@ -105,8 +105,10 @@ def reduce_over_ranks(dist, x, op, device):
     return float(t.item())
 
 
-def source_batches(n, per_step, count, rank, world):
-    perm = np.random.default_rng(12345).permutation(n)
+def source_batches(n, per_step, count, rank, world, order=None):
+    """Step i of rank r takes the (i * world + r)-th chunk of `per_step` sources of `order` (wrapping around): the
+    library's all-sources order (ngx_graph_source_order) for the GPU arm, a seeded permutation otherwise."""
+    perm = np.random.default_rng(12345).permutation(n) if order is None else np.asarray(order, dtype=np.int64)
     out = []
     for i in range(count):
         start = ((i * world + rank) * per_step) % n
@@ -428,7 +430,8 @@ def main():
     stream = torch.cuda.Stream()
     g = ngx.Graph(c.n, c.row_ptr, c.col, c.w, device=local_rank)
     g.set_stream(stream.cuda_stream)
-    batches = source_batches(c.n, args.sources_per_step, args.warmup + args.steps, rank, world)
+    # one step = one wave of the all-sources job in the library's order (tiles of nearby sources)
+    batches = source_batches(c.n, args.sources_per_step, args.warmup + args.steps, rank, world, order=g.source_order())
 
     def step(graph, sources, hist_max):
         """One step of the selected mode; returns (result, host outputs)."""

@@ -157,6 +157,16 @@ NGX_API int ngx_graph_set_stream(ngx_graph* graph, void* stream);
 /* Caps the device memory the graph's runs may use for workspaces (bytes; 0 = no cap beyond free memory). */
 NGX_API int ngx_graph_set_memory_budget(ngx_graph* graph, uint64_t bytes);
 
+/*
+ * The order in which all-sources runs (opts.sources == NULL, and batch runs) take the sources: clusters of nearby
+ * vertices, 32 to a tile (each seed with its lightest unassigned out-neighbours), so that a tile's sources share arc
+ * passes. order: n entries (for a batch, each graph's local ids, graph after graph). Per-source outputs are always
+ * indexed by vertex. Callers that split an all-sources job into batches get the same tiles by taking contiguous
+ * chunks of this order. No reference counterpart (the reference loops over its local vertices in id order,
+ * AllPairsShortestPath.h:130-143).
+ */
+NGX_API int ngx_graph_source_order(const ngx_graph* graph, int64_t* order);
+
 /* APSP summaries (and optional histogram / per-source outputs) over the requested sources. */
 NGX_API int ngx_apsp(ngx_graph* graph, const ngx_apsp_opts* opts, ngx_apsp_result* result);
 

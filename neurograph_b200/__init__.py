@@ -84,7 +84,7 @@ _LIB = None
 EXPORTED = [
     "ngx_status_string", "ngx_last_error", "ngx_version", "ngx_graph_create", "ngx_graph_destroy", "ngx_graph_size",
     "ngx_graph_request_abort", "ngx_graph_set_stream", "ngx_graph_set_memory_budget", "ngx_apsp", "ngx_sssp_rows", "ngx_brandes",
-    "ngx_apsp_grad", "ngx_batch_create", "ngx_batch_run", "ngx_batch_autotune", "ngx_graph_update_weights", "ngx_apsp_noalloc", "ngx_exact_accumulate", "ngx_exact_round",
+    "ngx_apsp_grad", "ngx_batch_create", "ngx_batch_run", "ngx_batch_autotune", "ngx_graph_update_weights", "ngx_apsp_noalloc", "ngx_exact_accumulate", "ngx_exact_round", "ngx_graph_source_order",
 ]
 
 
@@ -116,6 +116,7 @@ def library() -> C.CDLL:
         lib.ngx_batch_autotune.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         lib.ngx_graph_update_weights.argtypes = [C.c_void_p, C.c_void_p]
         lib.ngx_apsp_noalloc.argtypes = [C.c_void_p, C.POINTER(_Opts), C.POINTER(_Result)]
+        lib.ngx_graph_source_order.argtypes = [C.c_void_p, C.c_void_p]
         lib.ngx_exact_accumulate.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
         lib.ngx_exact_round.argtypes = [C.c_void_p]
         lib.ngx_exact_round.restype = C.c_double
@@ -202,6 +203,13 @@ class Graph:
 
     def set_memory_budget(self, nbytes: int) -> None:
         _check(library().ngx_graph_set_memory_budget(self._handle, int(nbytes)))
+
+    def source_order(self) -> np.ndarray:
+        """The order in which all-sources runs take the sources (tiles of nearby vertices); contiguous chunks of it
+        split an all-sources job into batches with the same tiles."""
+        out = np.zeros(max(self.n, 1), np.int64)
+        _check(library().ngx_graph_source_order(self._handle, out.ctypes.data))
+        return out[: self.n]
 
     def update_weights(self, w) -> None:
         """Replaces the arc weights in place (same arcs; no weight may change between zero and non-zero)."""

@@ -202,14 +202,12 @@ int ngx_batch_run(ngx_graph* g, const ngx_batch_opts* opts, ngx_apsp_result* res
 
     // graph table and sources (every vertex of every graph) for these options
     const std::vector<GraphDesc> descs = graph_table(g, opts->metric, opts->delta_scale);
-    std::vector<int32_t> sources(n_total);
-    for (const GraphPart& part : g->parts) {
-        for (int64_t v = 0; v < part.n; ++v) {
-            sources[static_cast<size_t>(part.vertex_off + v)] = static_cast<int32_t>(v);
-        }
-    }
+    // every graph's sources in its locality order (per-source results are scattered back by vertex)
+    const std::vector<int32_t>& sources = g->source_order;
     NGX_CUDA_TRY(cudaMemcpyAsync(o.graphs, descs.data(), descs.size() * sizeof(GraphDesc), cudaMemcpyHostToDevice, g->stream));
-    NGX_CUDA_TRY(cudaMemcpyAsync(o.sources, sources.data(), std::max<size_t>(1, sources.size()) * 4, cudaMemcpyHostToDevice, g->stream));
+    if (!sources.empty()) {
+        NGX_CUDA_TRY(cudaMemcpyAsync(o.sources, sources.data(), sources.size() * 4, cudaMemcpyHostToDevice, g->stream));
+    }
     NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
     TileJob job;
     job.num_graphs = count;
@@ -298,7 +296,8 @@ int ngx_batch_run(ngx_graph* g, const ngx_batch_opts* opts, ngx_apsp_result* res
         ngx_apsp_result* r = &results[gi];
         clear_result_totals(r);
         const GraphPart& part = g->parts[static_cast<size_t>(gi)];
-        if ((rc = collect_graph(g, o, acc.data(), counters.data(), gi, part.vertex_off, part.n, hist_bins, hist_max, r)) != NGX_OK) {
+        if ((rc = collect_graph(g, o, acc.data(), counters.data(), gi, part.vertex_off, part.n, hist_bins, hist_max, r,
+                                g->source_order.data() + part.vertex_off)) != NGX_OK) {
             return rc;
         }
         r->kernel_ms = ms;
@@ -365,10 +364,8 @@ int ngx_batch_autotune(ngx_graph* g, int task, double* class_scales) {
         for (int64_t t = 0; t < tiles; ++t) {
             items[static_cast<size_t>(t)] = WorkItem{ 0, static_cast<int32_t>(t) };
         }
-        std::vector<int32_t> sources(static_cast<size_t>(part.n));
-        for (int64_t v = 0; v < part.n; ++v) {
-            sources[static_cast<size_t>(v)] = static_cast<int32_t>(v);
-        }
+        // the graph's sources in the order a run takes them
+        const std::vector<int32_t> sources(g->source_order.begin() + part.vertex_off, g->source_order.begin() + part.vertex_off + part.n);
         WorkItem* d_items = nullptr;
         NGX_CUDA_TRY(cudaMalloc(&d_items, items.size() * sizeof(WorkItem)));
         NGX_CUDA_TRY(cudaMemcpy(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));

@@ -11,8 +11,9 @@
 //          adjoint   share = sigma[v][s] / sigma[x][s]; c = share * (1 + delta[x][s]); c_g = share * (g[x][s] + dg[x][s])
 //                    with g = (1 / d)^2; delta[v] = sum c, dg[v] = sum c_g; each DAG arc e = (v -> x) receives
 //                    sum over the tile's sources of c (d sum_t d(s,t) / d len_e) and of c_g (-d sum_t 1/d(s,t) / d len_e).
-// Betweenness per vertex and the gradients per arc are summed across tiles in 128-bit fixed point (fixed_add), so the
-// totals do not depend on the order in which CTAs finish; within a tile the lanes are combined by a fixed butterfly.
+// Betweenness per vertex and the gradients per arc are summed in 128-bit fixed point (integer adds: per (arc, source)
+// term for the gradients, per tile after an exact integer sum over the tile's lanes for betweenness), so the totals do
+// not depend on the order in which CTAs finish nor on how the sources are grouped into tiles.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -60,15 +61,6 @@ inline size_t brandes_slot_bytes(int64_t n, bool adjoint) {
 __device__ __forceinline__ bool on_dag(unsigned long long du_bits, double len, unsigned long long dv_bits) {
     return static_cast<unsigned long long>(__double_as_longlong(__dadd_rn(__longlong_as_double(static_cast<long long>(du_bits)), len))) == dv_bits;
 }
-
-__device__ __forceinline__ double warp_sum(double x) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        x += __shfl_xor_sync(0xFFFFFFFFu, x, off);
-    }
-    return x;
-}
-
 
 // Pair-parallel walk over the deg x k (arc, ready source) pairs of one vertex, as in the SSSP expansion: pair
 // p = 32 i + lane takes arc p / k and the (p % k)-th ready source. Sums per source are gathered in arc order: in each

@@ -88,6 +88,59 @@ int grow_buffer(ngx_graph* g, void** buf, size_t* cap, size_t bytes) {
 
 namespace {
 
+// Tiles of nearby sources: from each unassigned seed (in id order), the seed and its lightest unassigned out-neighbours,
+// then theirs (one hop at a time, lightest first, continuing from the 64 lightest), until a tile of 32 is full or the
+// search has looked at 256 vertices. Close sources reach most vertices at similar distances, so more of them are pending on a vertex when it is
+// expanded, and one pass over its arcs serves more of them. O(n * 256 * degree) at worst, on the host.
+void append_source_order(int64_t n, const int64_t* row_ptr, const Arc* arcs, std::vector<int32_t>& order) {
+    std::vector<uint8_t> assigned(static_cast<size_t>(n), 0);
+    std::vector<int32_t> seen_stamp(static_cast<size_t>(n), -1);
+    std::vector<int32_t> frontier, next;
+    std::vector<std::pair<double, int32_t>> cand;
+    int32_t stamp = 0;
+    for (int64_t seed = 0; seed < n; ++seed) {
+        if (assigned[static_cast<size_t>(seed)]) {
+            continue;
+        }
+        ++stamp;
+        int taken = 0;
+        int looked = 1;
+        frontier.assign(1, static_cast<int32_t>(seed));
+        seen_stamp[static_cast<size_t>(seed)] = stamp;
+        assigned[static_cast<size_t>(seed)] = 1;
+        order.push_back(static_cast<int32_t>(seed));
+        ++taken;
+        while (taken < kTile && !frontier.empty() && looked < 256) {
+            cand.clear();
+            for (const int32_t u : frontier) {
+                for (int64_t e = row_ptr[u]; e < row_ptr[u + 1]; ++e) {
+                    const int32_t v = arcs[e].col;
+                    if (seen_stamp[static_cast<size_t>(v)] != stamp) {
+                        seen_stamp[static_cast<size_t>(v)] = stamp;
+                        cand.emplace_back(arcs[e].len, v);
+                    }
+                }
+            }
+            std::sort(cand.begin(), cand.end());
+            next.clear();
+            for (const auto& c : cand) {
+                ++looked;
+                if (next.size() < 64) {
+                    next.push_back(c.second);  // the next hop continues from the lightest candidates only
+                }
+                if (!assigned[static_cast<size_t>(c.second)]) {
+                    assigned[static_cast<size_t>(c.second)] = 1;
+                    order.push_back(c.second);
+                    if (++taken == kTile) {
+                        break;
+                    }
+                }
+            }
+            frontier.swap(next);
+        }
+    }
+}
+
 void release(ngx_graph* g) {
     if (g == nullptr) {
         return;
@@ -288,6 +341,14 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
                 rarcs[static_cast<size_t>(fill[static_cast<size_t>(a.col)]++)] = Arc{ static_cast<int32_t>(u), static_cast<int32_t>(e), a.len };
             }
         }
+        // arcs of this graph's rows, with graph-local row offsets
+        {
+            std::vector<int64_t> local_rows(static_cast<size_t>(n) + 1);
+            for (int64_t v = 0; v <= n; ++v) {
+                local_rows[static_cast<size_t>(v)] = row_ptr[static_cast<size_t>(part.row_off + v)] - first_arc;
+            }
+            append_source_order(n, local_rows.data(), regular.data() + first_arc, g->source_order);
+        }
         g->n = std::max(g->n, n);
         user_arc_off += csr->m;
         vertex_off += n;
@@ -343,6 +404,16 @@ const char* ngx_status_string(int status) {
     case NGX_UNSUPPORTED: return "unsupported";
     default: return "unknown status";
     }
+}
+
+int ngx_graph_source_order(const ngx_graph* graph, int64_t* order) {
+    if (graph == nullptr || (order == nullptr && graph->n_total > 0)) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_source_order: graph or order is NULL");
+    }
+    for (size_t i = 0; i < graph->source_order.size(); ++i) {
+        order[i] = graph->source_order[i];
+    }
+    return NGX_OK;
 }
 
 const char* ngx_last_error(void) { return last_error_message.c_str(); }

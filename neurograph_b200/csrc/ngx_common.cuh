@@ -178,6 +178,39 @@ __device__ __forceinline__ void fixed_add(unsigned long long* lo_hi, double x) {
     }
 }
 
+// The fixed-point words of a non-negative double (the same truncation as fixed_add).
+__device__ __forceinline__ void fixed_parts(double x, unsigned long long& lo, unsigned long long& hi) {
+    lo = 0ull;
+    hi = 0ull;
+    if (x > 0.0) {
+        const double whole = floor(x);
+        hi = static_cast<unsigned long long>(whole);
+        lo = static_cast<unsigned long long>(ldexp(x - whole, 64));
+    }
+}
+
+// Adds a fixed-point value given as words (e.g. an exact sum of fixed_parts) to a 128-bit accumulator.
+__device__ __forceinline__ void fixed_add_parts(unsigned long long* lo_hi, unsigned long long lo, unsigned long long hi) {
+    const unsigned long long old = atomicAdd(&lo_hi[0], lo);
+    const unsigned long long carry = (old + lo < old) ? 1ull : 0ull;
+    if (hi + carry != 0) {
+        atomicAdd(&lo_hi[1], hi + carry);
+    }
+}
+
+// Exact sum over the warp's lanes of 128-bit fixed-point values (integer adds: the result does not depend on which
+// values sit in which lane); every lane receives it.
+__device__ __forceinline__ void fixed_warp_sum(unsigned long long& lo, unsigned long long& hi) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long o_lo = __shfl_xor_sync(0xFFFFFFFFu, lo, off);
+        const unsigned long long o_hi = __shfl_xor_sync(0xFFFFFFFFu, hi, off);
+        const unsigned long long s = lo + o_lo;
+        hi += o_hi + (s < lo ? 1ull : 0ull);
+        lo = s;
+    }
+}
+
 __host__ __device__ inline double fixed_value(unsigned long long lo, unsigned long long hi) {
     return static_cast<double>(hi) + ldexp(static_cast<double>(lo), -64);
 }

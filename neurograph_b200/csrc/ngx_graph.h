@@ -80,6 +80,9 @@ struct ngx_graph {
     double class_scale[64] = {};
     // stored forward index of each caller arc (-1 for zero weights), for ngx_graph_update_weights
     std::vector<int32_t> stored_of_user;
+    // all-sources processing order of each graph (graph-local ids, graph after graph): clusters of nearby vertices,
+    // so that the 32 sources of a tile reach most vertices in the same phases and share arc passes
+    std::vector<int32_t> source_order;
 
     ngx::DeviceCsr csr(int metric) const {
         return ngx::DeviceCsr{ n, m_stored, d_row_ptr, metric == NGX_METRIC_INVERSE ? d_arcs_inverse : d_arcs_regular };

@@ -66,7 +66,8 @@ int launch_apsp_in_workspace(ngx_graph* g, const ngx_apsp_opts* opts, const Tile
                              size_t ws_bytes);
 int read_totals(ngx_graph* g, const RunOutputs& o, std::vector<unsigned long long>& acc, std::vector<unsigned long long>& counters);
 int collect_graph(ngx_graph* g, const RunOutputs& o, const unsigned long long* acc_all, const unsigned long long* counters_all, int64_t gi,
-                  int64_t src_off, int64_t num_sources, int64_t hist_bins, double hist_max, ngx_apsp_result* r);
+                  int64_t src_off, int64_t num_sources, int64_t hist_bins, double hist_max, ngx_apsp_result* r,
+                  const int32_t* scatter = nullptr);
 void clear_result_totals(ngx_apsp_result* r);
 
 }  // namespace ngx

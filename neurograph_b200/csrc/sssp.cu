@@ -411,7 +411,7 @@ void clear_result_totals(ngx_apsp_result* r) {
 
 // Reduces graph `gi`'s accumulators and counters (host copies) into a result; copies its optional device outputs.
 int collect_graph(ngx_graph* g, const RunOutputs& o, const unsigned long long* acc_all, const unsigned long long* counters_all, int64_t gi,
-                  int64_t src_off, int64_t num_sources, int64_t hist_bins, double hist_max, ngx_apsp_result* r) {
+                  int64_t src_off, int64_t num_sources, int64_t hist_bins, double hist_max, ngx_apsp_result* r, const int32_t* scatter) {
     unsigned long long acc[2 * kAccDigits];
     std::memcpy(acc, acc_all + gi * 2 * kAccDigits, sizeof(acc));
     const unsigned long long* counters = counters_all + gi * kCounterCount;
@@ -445,6 +445,28 @@ int collect_graph(ngx_graph* g, const RunOutputs& o, const unsigned long long* a
     const size_t at = static_cast<size_t>(src_off);
     if (r->hist != nullptr && hist_bins > 0) {
         NGX_CUDA_TRY(cudaMemcpyAsync(r->hist, o.hist + gi * hist_bins, static_cast<size_t>(hist_bins) * 8, cudaMemcpyDeviceToHost, g->stream));
+    }
+    if (s > 0 && scatter != nullptr) {
+        // the run took the sources in the graph's locality order: entry i belongs to vertex scatter[i]
+        std::vector<unsigned long long> tmp(s);
+        const auto put = [&](void* dst, const void* src) -> int {
+            if (dst == nullptr) {
+                return NGX_OK;
+            }
+            NGX_CUDA_TRY(cudaMemcpyAsync(tmp.data(), src, s * 8, cudaMemcpyDeviceToHost, g->stream));
+            NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            auto* out = static_cast<unsigned long long*>(dst);
+            for (size_t i = 0; i < s; ++i) {
+                out[scatter[i]] = tmp[i];
+            }
+            return NGX_OK;
+        };
+        int rc = put(r->src_sum, o.src_f64 + at);
+        if (rc == NGX_OK) rc = put(r->src_max, o.src_f64 + total + at);
+        if (rc == NGX_OK) rc = put(r->src_sum_inverse, o.src_f64 + 2 * total + at);
+        if (rc == NGX_OK) rc = put(r->src_unreachable, o.src_u64 + at);
+        if (rc == NGX_OK) rc = put(r->src_arcs, o.src_u64 + total + at);
+        return rc;
     }
     if (s > 0) {
         if (r->src_sum != nullptr) NGX_CUDA_TRY(cudaMemcpyAsync(r->src_sum, o.src_f64 + at, s * 8, cudaMemcpyDeviceToHost, g->stream));
@@ -530,6 +552,13 @@ int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, d
     if (const int rc = prepare_sources(g, opts, sources); rc != NGX_OK) {
         return rc;
     }
+    // all sources: in the graph's locality order (tiles of nearby sources), results scattered back by vertex;
+    // distance rows keep vertex order
+    const int32_t* scatter = nullptr;
+    if (opts->sources == nullptr && rows == nullptr && g->source_order.size() == sources.size()) {
+        sources.assign(g->source_order.begin(), g->source_order.end());
+        scatter = g->source_order.data();
+    }
     ngx_apsp_result scratch{};
     ngx_apsp_result* r = result != nullptr ? result : &scratch;
     clear_result_totals(r);
@@ -552,7 +581,7 @@ int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, d
         std::vector<unsigned long long> acc, counters;
         rc = read_totals(g, o, acc, counters);
         if (rc == NGX_OK) {
-            rc = collect_graph(g, o, acc.data(), counters.data(), 0, 0, num_sources, hist_bins, hist_max, r);
+            rc = collect_graph(g, o, acc.data(), counters.data(), 0, 0, num_sources, hist_bins, hist_max, r, scatter);
         }
         r->kernel_ms = ms;
     }

@@ -684,9 +684,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 if constexpr (kMode == kModeBrandes) {
                     // BrandesVariant.h:156: every settled vertex but the source gains its dependency
                     const double dep = (valid && v != my_src && bits != kInfBits) ? __ldcg(&delta[row]) : 0.0;
-                    const double total = warp_sum(dep);
-                    if (lane == 0 && total > 0.0) {
-                        fixed_add(&bc_g[2 * v], total);
+                    // summed over the tile's sources in fixed point, exactly: betweenness does not depend on how
+                    // the sources are grouped into tiles
+                    unsigned long long lo, hi;
+                    fixed_parts(dep, lo, hi);
+                    fixed_warp_sum(lo, hi);
+                    if (lane == 0 && (lo | hi) != 0ull) {
+                        fixed_add_parts(&bc_g[2 * v], lo, hi);
                     }
                 }
                 sigma[row] = __longlong_as_double(-1ll);

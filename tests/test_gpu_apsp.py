@@ -160,3 +160,27 @@ def test_errors_leave_the_context_usable(restatement):
             gg.apsp(max_iterations=1, delta=1e-6)
         assert e.value.status == 4  # TIMEOUT: the iteration cap stops the kernel, it reports instead of spinning
         check_against_oracle(gg, csr, restatement)
+
+
+def test_source_order_is_a_permutation_and_runs_agree():
+    """All-sources runs take the sources in the graph's locality order; the order is a permutation, per-source outputs
+    still come back by vertex, and running contiguous chunks of the order gives the same totals as one run."""
+    c = synth.connectome(2000, 12, 0.15, weights="lognormal", seed=5, use_gpu=False)
+    with ngx.Graph(c.n, c.row_ptr, c.col, c.w) as g:
+        order = g.source_order()
+        assert np.array_equal(np.sort(order), np.arange(c.n))
+        whole = g.apsp(per_source=True)
+        by_vertex = g.apsp(sources=np.arange(c.n), per_source=True)
+        for k in ("sum", "sum_inv", "max", "unreachable", "arcs"):
+            assert np.array_equal(whole.per_source[k], by_vertex.per_source[k]), k
+        assert whole.sum_distances == by_vertex.sum_distances and whole.cluster_sizes == by_vertex.cluster_sizes
+        digits = np.zeros((2, ngx.ACC_DIGITS), np.uint64)
+        for chunk in np.array_split(order, 5):
+            digits += g.apsp(sources=chunk, exact=True).acc_digits
+        assert ngx.exact_round(digits[0]) == whole.sum_distances
+        assert ngx.exact_round(digits[1]) == whole.sum_inverse
+    small = synth.connectome(40, 4, 0.3, weights="int", seed=6, use_gpu=False)
+    graphs = [(c.n, c.row_ptr, c.col, c.w), (small.n, small.row_ptr, small.col, small.w)]
+    with ngx.Batch(graphs) as b:
+        results, _ = b.run("apsp", per_source=True)
+    assert np.array_equal(results[0].per_source["sum"], whole.per_source["sum"])
