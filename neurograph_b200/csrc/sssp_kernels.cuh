@@ -115,23 +115,15 @@ struct TileShared {
 // For that, no (v, s) may be expanded twice with one distance (the repeat would look like a tie): an expansion reads
 // the newest distance, and the improvement that produced it has queued another expansion. last[v][s] keeps the
 // distance of the latest expansion, and sources whose distance has not changed since are dropped from the next.
+// The caller has taken v's pending mask (amask, non-zero), cleared it and v's superseded far marks, and read its row
+// offsets (beg, deg): see expand_queue.
 template <int kUnroll, bool kTrack>
-__device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, int lane, unsigned long long* __restrict__ dist, uint32_t* pend_cur,
-                                               uint32_t* pend_nxt, uint32_t* far, int32_t* q_nxt, int* qlen_nxt, uint32_t* stamp, unsigned next_stamp,
-                                               double theta, unsigned long long& expansions, unsigned long long& lane_expansions,
-                                               unsigned long long* pred_key, uint32_t* tie, unsigned long long* last) {
-    uint32_t amask = __ldcg(&pend_cur[v]);
-    if (amask == 0) {
-        return;
-    }
+__device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32_t amask, int64_t beg, int deg, int lane,
+                                               unsigned long long* __restrict__ dist, uint32_t* pend_nxt, uint32_t* far, int32_t* q_nxt,
+                                               int* qlen_nxt, uint32_t* stamp, unsigned next_stamp, double theta, unsigned long long& expansions,
+                                               unsigned long long& lane_expansions, unsigned long long* pred_key, uint32_t* tie,
+                                               unsigned long long* last) {
     const uint32_t amask0 = amask;
-    __syncwarp();
-    if (lane == 0) {
-        pend_cur[v] = 0u;
-        if (__ldcg(&far[v]) & amask) {
-            atomicAnd(&far[v], ~amask);  // those far marks are superseded by the near values expanded now
-        }
-    }
     int k = __popc(amask);
     // lane r < k holds the r-th pending source and its distance to v
     int rank_src = lane < k ? static_cast<int>(__fns(amask, 0, lane + 1)) : 0;
@@ -160,8 +152,6 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, int la
     expansions += 1;
     lane_expansions += static_cast<unsigned long long>(k);
     const double rank_dv = __longlong_as_double(static_cast<long long>(rank_bits));
-    const int64_t beg = __ldg(&g.row_ptr[v]);
-    const int deg = static_cast<int>(__ldg(&g.row_ptr[v + 1]) - beg);
     const Arc* arcs = g.arcs + beg;
     // position of this lane's first pair, and the per-iteration advance of 32 pairs
     int a = lane / k;
@@ -237,6 +227,49 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, int la
                     q_nxt[base + __popc(pmask & lanemask_lt())] = x[u];
                 }
             }
+        }
+    }
+}
+
+// One near iteration of a tile: the warps take the queue 32 entries at a time; lane j fetches entry j's vertex, its
+// pending mask, far marks and row offsets (one round of parallel loads for 32 vertices), clears the mask and the
+// superseded far marks, and the warp then expands the 32 vertices one after another.
+template <int kUnroll, bool kTrack>
+__device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* q_cur, int qlen, int lane, int warp, int nwarps,
+                                             unsigned long long* __restrict__ dist, uint32_t* pend_cur, uint32_t* pend_nxt, uint32_t* far,
+                                             int32_t* q_nxt, int* qlen_nxt, uint32_t* stamp, unsigned next_stamp, double theta,
+                                             unsigned long long& expansions, unsigned long long& lane_expansions, unsigned long long* pred_key,
+                                             uint32_t* tie, unsigned long long* last) {
+    for (int base = warp * 32; base < qlen; base += nwarps * 32) {
+        const int i = base + lane;
+        int vj = 0;
+        uint32_t mj = 0;
+        int64_t bj = 0;
+        int dj = 0;
+        if (i < qlen) {
+            vj = __ldcg(&q_cur[i]);
+            mj = __ldcg(&pend_cur[vj]);
+            const uint32_t fm = __ldcg(&far[vj]);
+            bj = __ldg(&g.row_ptr[vj]);
+            dj = static_cast<int>(__ldg(&g.row_ptr[vj + 1]) - bj);
+            if (mj != 0u) {
+                pend_cur[vj] = 0u;
+                if (fm & mj) {
+                    atomicAnd(&far[vj], ~mj);  // those far marks are superseded by the near values expanded now
+                }
+            }
+        }
+        const int count = qlen - base < 32 ? qlen - base : 32;
+        for (int j = 0; j < count; ++j) {
+            const uint32_t amask = __shfl_sync(kFullMask, mj, j);
+            if (amask == 0u) {
+                continue;
+            }
+            const int v = __shfl_sync(kFullMask, vj, j);
+            const int64_t beg = __shfl_sync(kFullMask, bj, j);
+            const int deg = __shfl_sync(kFullMask, dj, j);
+            batched_expand<kUnroll, kTrack>(g, v, amask, beg, deg, lane, dist, pend_nxt, far, q_nxt, qlen_nxt, stamp, next_stamp, theta,
+                                            expansions, lane_expansions, pred_key, tie, last);
         }
     }
 }
@@ -396,12 +429,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 int32_t* q_nxt = cur ? q0 : q1;
                 const unsigned next_stamp = s.stamp + 1u;
                 const double theta = s.theta;
-                for (int i = warp; i < qlen; i += nwarps) {
-                    batched_expand<kUnroll, kMode != kModeApsp>(g, __ldcg(&q_cur[i]), lane, dist, pend_cur, pend_nxt, far, q_nxt, &s.qlen[cur ^ 1],
-                                                                stamp, next_stamp, theta, expansions, lane_expansions,
-                                                                reinterpret_cast<unsigned long long*>(sigma), tie,
-                                                                reinterpret_cast<unsigned long long*>(delta));
-                }
+                expand_queue<kUnroll, kMode != kModeApsp>(g, q_cur, qlen, lane, warp, nwarps, dist, pend_cur, pend_nxt, far, q_nxt,
+                                                          &s.qlen[cur ^ 1], stamp, next_stamp, theta, expansions, lane_expansions,
+                                                          reinterpret_cast<unsigned long long*>(sigma), tie,
+                                                          reinterpret_cast<unsigned long long*>(delta));
                 __syncthreads();
                 if (tid == 0) {
                     s.qlen[cur] = 0;
