@@ -311,7 +311,9 @@ __device__ __forceinline__ void brandes_delta_vertex(const DeviceCsr& g, int v, 
 // with ties (or a key that does not check out) count by scanning v's in-arcs.
 __device__ __forceinline__ void dag_count(const DeviceCsr& g, const DeviceCsr& rg, const int32_t* arc_src, int64_t m_total, int64_t n, int nsrc,
                                           const int* s_src, const unsigned long long* dist, const uint32_t* tie, unsigned long long* pred_key,
-                                          uint32_t* cnt, uint32_t* scnt, uint32_t* pred, int lane, int warp, int nwarps) {
+                                          uint32_t* cnt, uint32_t* scnt, uint32_t* pred, int lane, int warp, int nwarps,
+                                          unsigned long long* active_pairs) {
+    unsigned long long active_count = 0;
     for (int64_t v = warp; v < n; v += nwarps) {
         const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
         const bool active = lane < nsrc && dv != kInfBits && v != s_src[lane];
@@ -321,6 +323,7 @@ __device__ __forceinline__ void dag_count(const DeviceCsr& g, const DeviceCsr& r
         uint32_t c = 0;
         uint32_t first = 0;
         bool scan = active;
+        active_count += active ? 1ull : 0ull;
         if (active && !tied && (key >> 32) == (dv >> 32)) {
             const uint32_t e = static_cast<uint32_t>(key);
             if (static_cast<int64_t>(e) < m_total) {
@@ -373,6 +376,13 @@ __device__ __forceinline__ void dag_count(const DeviceCsr& g, const DeviceCsr& r
         }
         cnt[v * kTile + lane] = c;
         pred[v * kTile + lane] = first;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        active_count += __shfl_xor_sync(0xFFFFFFFFu, active_count, off);
+    }
+    if (lane == 0 && active_count != 0ull) {
+        atomicAdd(active_pairs, active_count);
     }
 }
 
@@ -584,6 +594,55 @@ __device__ __forceinline__ void dag_sigma_level(const DeviceCsr& g, const int32_
                     if (push) {
                         next_list[at + __popc(pmask & lanemask_lt())] = static_cast<int32_t>((x[u] << 5) | xrow_s[u]);
                     }
+                }
+            }
+        }
+    }
+}
+
+// One level of the sigma pass when the tile's DAGs are trees: every successor gets sigma 1 and joins the next level.
+template <bool kTarget>
+__device__ __forceinline__ void dag_tree_level(const DeviceCsr& g, const int32_t* entries, int len, double* sigma, const uint32_t* soff,
+                                               const uint32_t* succ, int32_t* next_list, int* next_len, int lane, int warp, int nwarps) {
+    for (int base = warp * 32; base < len; base += nwarps * 32) {
+        const int i = base + lane;
+        uint32_t entry = 0, beg = 0, count = 0;
+        if (i < len) {
+            entry = static_cast<uint32_t>(__ldcg(&entries[i]));
+            const int64_t row = static_cast<int64_t>(entry >> 5) * kTile + (entry & 31u);
+            beg = __ldcg(&soff[row]);
+            count = __ldcg(&soff[row + 1]) - beg;
+        }
+        uint32_t total = 0;
+        const uint32_t off = warp_exclusive_scan(count, lane, &total);
+        // every pair pushes exactly one entry: reserve the warp's slots once
+        int at = 0;
+        if (lane == 0 && total != 0u) {
+            at = atomicAdd(next_len, static_cast<int>(total));
+        }
+        at = __shfl_sync(0xFFFFFFFFu, at, 0);
+        for (uint32_t p0 = 0; p0 < total; p0 += 32 * kLevelUnroll) {
+            uint32_t x[kLevelUnroll], sx[kLevelUnroll];
+            bool ok[kLevelUnroll];
+#pragma unroll
+            for (int u = 0; u < kLevelUnroll; ++u) {
+                const uint32_t q = p0 + static_cast<uint32_t>(u * 32 + lane);
+                ok[u] = q < total;
+                const int owner = pair_owner(off, ok[u] ? q : 0u);
+                const uint32_t j = __shfl_sync(0xFFFFFFFFu, beg, owner) + (q - __shfl_sync(0xFFFFFFFFu, off, owner));
+                sx[u] = __shfl_sync(0xFFFFFFFFu, entry, owner) & 31u;
+                x[u] = 0;
+                if (ok[u]) {
+                    const uint32_t e = __ldcg(&succ[j]);
+                    x[u] = kTarget ? e : static_cast<uint32_t>(g.arcs[e].col);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kLevelUnroll; ++u) {
+                const uint32_t q = p0 + static_cast<uint32_t>(u * 32 + lane);
+                if (ok[u]) {
+                    sigma[static_cast<int64_t>(x[u]) * kTile + sx[u]] = 1.0;
+                    next_list[at + static_cast<int>(q)] = static_cast<int32_t>((x[u] << 5) | sx[u]);
                 }
             }
         }

@@ -102,6 +102,7 @@ struct TileShared {
     int lvl_start;
     int lvl_len;
     int next_len;
+    unsigned long long active_pairs;  // reached (vertex, source) pairs other than the sources, counted by the DAG pass
 };
 
 // ------------------------------------------------------------------------------------------ batched form
@@ -532,8 +533,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             // ------------------------------------------------------------ shortest-path DAG: counts, sigma, delta
             // the level lists are built only after the successor lists: their storage holds pred[][] until then
             uint32_t* const pred = reinterpret_cast<uint32_t*>(list);
+            if (tid == 0) {
+                s.active_pairs = 0ull;
+            }
+            __syncthreads();
             dag_count(g, rg, b.arc_src, b.m_total, n, nsrc, s_src, dist, tie, reinterpret_cast<unsigned long long*>(sigma), cnt, scnt, pred, lane, warp,
-                      nwarps);
+                      nwarps, &s.active_pairs);
             __syncthreads();
             const unsigned long long dag_arcs = block_exclusive_scan(scnt, soff, nt, s_part);
             const bool use_lists = dag_arcs <= static_cast<unsigned long long>(b.succ_capacity);
@@ -556,7 +561,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 }
             }
           if (use_lists) {
-            // --- sigma and delta over the successor lists, one (vertex, source) entry per thread
+            // --- sigma and delta over the successor lists. When every reached pair has exactly one DAG predecessor
+            // (as many DAG arcs as reached non-source pairs) the DAGs are trees: every sigma is 1 and every child is
+            // released by its only parent, so the sigma levels need neither sums nor counts.
+            const bool tree = dag_arcs == s.active_pairs;
             if (tid == 0) {
                 s.level = 0u;
                 s.lvl_start = 0;
@@ -582,8 +590,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                     break;
                 }
                 const unsigned level = s.level;
-                dag_sigma_level<kMode == kModeBrandes>(g, list + start, len, level, sigma, cnt, lvl, soff, succ, list + start + len, &s.next_len,
-                                                       b.sigma_inexact, lane, warp, nwarps);
+                if (tree) {
+                    dag_tree_level<kMode == kModeBrandes>(g, list + start, len, sigma, soff, succ, list + start + len, &s.next_len, lane, warp, nwarps);
+                } else {
+                    dag_sigma_level<kMode == kModeBrandes>(g, list + start, len, level, sigma, cnt, lvl, soff, succ, list + start + len, &s.next_len,
+                                                           b.sigma_inexact, lane, warp, nwarps);
+                }
                 __syncthreads();
                 if (tid == 0) {
                     s.lvl_start = start + len;
