@@ -652,7 +652,7 @@ __device__ __forceinline__ void dag_tree_level(const DeviceCsr& g, const int32_t
 // delta (and the adjoint terms) over one level: each entry pulls over its sorted successor list. Pair contributions
 // go through the warp's slice of `buf` (32 values per unrolled pair, twice for the adjoint) and each entry's lane adds
 // its own in list order, so every sum runs in the same order as a sequential loop over the list.
-template <int kMode>
+template <int kMode, bool kTree>
 __device__ __forceinline__ void dag_delta_level(const DeviceCsr& g, const int32_t* entries, int len, const unsigned long long* dist, const double* sigma,
                                                 double* delta, double* delta_g, const uint32_t* soff, const uint32_t* succ, unsigned long long* grad_cpl,
                                                 unsigned long long* grad_eff, double* buf, int lane, int warp, int nwarps) {
@@ -667,7 +667,7 @@ __device__ __forceinline__ void dag_delta_level(const DeviceCsr& g, const int32_
         if (i < len) {
             entry = static_cast<uint32_t>(__ldcg(&entries[i]));
             row = static_cast<int64_t>(entry >> 5) * kTile + (entry & 31u);
-            sv = __ldcg(&sigma[row]);
+            sv = kTree ? 1.0 : __ldcg(&sigma[row]);
             beg = __ldcg(&soff[row]);
             count = __ldcg(&soff[row + 1]) - beg;
         }
@@ -701,7 +701,7 @@ __device__ __forceinline__ void dag_delta_level(const DeviceCsr& g, const int32_
                     }
                     const int64_t xrow = static_cast<int64_t>(x) * kTile + s;
                     dx[u] = __ldcg(&delta[xrow]);
-                    sx[u] = __ldcg(&sigma[xrow]);
+                    sx[u] = kTree ? 1.0 : __ldcg(&sigma[xrow]);  // every sigma is 1 in a tree
                     if constexpr (kMode == kModeGrad) {
                         gx[u] = __longlong_as_double(static_cast<long long>(__ldcg(&dist[xrow])));
                         dgx[u] = __ldcg(&delta_g[xrow]);

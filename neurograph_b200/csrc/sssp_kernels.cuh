@@ -616,8 +616,13 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             for (int level = levels - 1; level >= lowest; --level) {
                 const int start = __ldcg(&loff[level]);
                 const int end = __ldcg(&loff[level + 1]);
-                dag_delta_level<kMode>(g, list + start, end - start, dist, sigma, delta, delta_g, soff, succ, b.grad_cpl, b.grad_eff,
-                                       reinterpret_cast<double*>(s_acc_sum), lane, warp, nwarps);
+                if (tree) {
+                    dag_delta_level<kMode, true>(g, list + start, end - start, dist, sigma, delta, delta_g, soff, succ, b.grad_cpl, b.grad_eff,
+                                                 reinterpret_cast<double*>(s_acc_sum), lane, warp, nwarps);
+                } else {
+                    dag_delta_level<kMode, false>(g, list + start, end - start, dist, sigma, delta, delta_g, soff, succ, b.grad_cpl, b.grad_eff,
+                                                  reinterpret_cast<double*>(s_acc_sum), lane, warp, nwarps);
+                }
                 __syncthreads();
             }
             // the pair buffers borrowed the epilogue's accumulators, which must start the epilogue at zero
