@@ -317,6 +317,7 @@ def run_uneven_batch(args, ngx, torch, rank, world, barrier, max_over_ranks, sum
     graphs = uneven_batch_graphs(rank, world)
     m_total = sum(int(g[2].size) for g in graphs)
     log(f"[bench] {len(graphs)} graphs, {m_total} arcs generated in {time.perf_counter() - t0:.1f}s")
+    torch.cuda.empty_cache()
     stream = torch.cuda.Stream()
     b = ngx.Batch(graphs, device=local_rank)
     b.set_stream(stream.cuda_stream)
@@ -427,6 +428,7 @@ def main():
     t0 = time.perf_counter()
     c = make_graph(args.n, args.degree, args.length_scale, args.sigma)
     log(f"[bench] graph n={c.n} m={c.m} generated in {time.perf_counter() - t0:.1f}s")
+    torch.cuda.empty_cache()  # the generator's cached blocks would otherwise shrink the library's workspace budget
     stream = torch.cuda.Stream()
     g = ngx.Graph(c.n, c.row_ptr, c.col, c.w, device=local_rank)
     g.set_stream(stream.cuda_stream)
