@@ -60,3 +60,31 @@ def test_against_finite_differences():
         fd_eff = float(np.sum(1.0 / dp[fin] - 1.0 / dm[fin])) / (2 * h) / res.reached_pairs
         assert abs(dcpl[e] - fd_cpl) <= 1e-6 * abs(fd_cpl), (e, dcpl[e], fd_cpl)
         assert abs(deff[e] - fd_eff) <= 1e-6 * abs(fd_eff), (e, deff[e], fd_eff)
+
+
+def test_autograd_function_matches_the_adjoint_and_finite_differences():
+    """neurograph_b200.autograd: backward of (CPL, E) equals the adjoint outputs and a central finite difference."""
+    import torch
+
+    from neurograph_b200.autograd import apsp_metrics
+
+    c = synth.connectome(300, 6, 0.2, weights="lognormal", seed=13, use_gpu=False)
+    w = torch.tensor(c.w, dtype=torch.float64, requires_grad=True)
+    out = apsp_metrics(w, c.n, c.row_ptr, c.col)
+    (out[0] + 2.0 * out[1]).backward()
+    with ngx.Graph(c.n, c.row_ptr, c.col, c.w) as g:
+        dcpl, deff, r = g.apsp_grad()
+    assert out[0].item() == r.cpl and out[1].item() == r.efficiency
+    want = dcpl + 2.0 * deff
+    assert np.allclose(w.grad.numpy(), want, rtol=1e-12, atol=0.0)
+    rng = np.random.default_rng(2)
+    for e in rng.choice(c.m, size=5, replace=False):
+        h = 1e-6 * c.w[e]
+        vals = []
+        for sign in (1.0, -1.0):
+            wp = c.w.copy()
+            wp[e] += sign * h
+            o = apsp_metrics(torch.tensor(wp), c.n, c.row_ptr, c.col)
+            vals.append(o[0].item() + 2.0 * o[1].item())
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(fd - want[e]) <= 1e-4 * max(1e-12, abs(want[e])) + 1e-9, (e, fd, want[e])
