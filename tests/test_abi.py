@@ -72,3 +72,23 @@ def test_null_arguments():
     assert lib.ngx_graph_create(None, 0, None) == 1
     assert lib.ngx_apsp(None, None, None) == 1
     assert lib.ngx_graph_size(None, None, None) == 1
+
+
+def test_exact_sums_on_the_host():
+    """ngx_exact_accumulate / ngx_exact_round (host only): the exactly rounded sum whatever the split or order,
+    equal to math.fsum; negative or non-finite values are rejected."""
+    import math
+
+    rng = np.random.default_rng(4)
+    x = np.concatenate([rng.lognormal(0.0, 6.0, 50000), [0.0, 5e-324, 2.2250738585072014e-308, 1.7976931348623157e308 / 4]])
+    whole = ngx.exact_accumulate(x)
+    assert ngx.exact_round(whole) == math.fsum(x)
+    parts = [ngx.exact_accumulate(p) for p in np.array_split(rng.permutation(x), 7)]
+    assert ngx.exact_round(sum(parts)) == math.fsum(x)
+    assert ngx.exact_round(np.zeros(ngx.ACC_DIGITS, np.uint64)) == 0.0
+    # ties to even at the rounding boundary: 1 + 2^-53 rounds to 1, 1 + 3 * 2^-53 to 1 + 2^-51
+    assert ngx.exact_round(ngx.exact_accumulate([1.0, 2.0 ** -53])) == 1.0
+    assert ngx.exact_round(ngx.exact_accumulate([1.0, 2.0 ** -53, 2.0 ** -52])) == 1.0 + 2.0 ** -51
+    for bad in ([-1.0], [float("nan")], [float("inf")]):
+        with pytest.raises(ngx.NgxError):
+            ngx.exact_accumulate(bad)
