@@ -304,6 +304,46 @@ __device__ __forceinline__ void brandes_delta_vertex(const DeviceCsr& g, int v, 
 // a second dense pass fills the lists (forward-CSR arc indices), and each list is sorted so that every sum over it has
 // a fixed order. sigma and delta then touch only DAG arcs.
 
+// Counts the DAG in-arcs of v for the lanes in `scan` by scanning v's in-arcs (ties, or no usable recorded key).
+__device__ __forceinline__ void dag_count_scan(const DeviceCsr& rg, int64_t v, unsigned long long dv, bool scan, const unsigned long long* dist,
+                                               uint32_t* scnt, int lane, uint32_t& c, uint32_t& first) {
+    const int64_t beg = __ldg(&rg.row_ptr[v]);
+    const int64_t end = __ldg(&rg.row_ptr[v + 1]);
+    for (int64_t e0 = beg; e0 < end; e0 += 32) {
+        const int cntr = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
+        Arc a{ 0, 0, 0.0 };
+        if (lane < cntr) {
+            a = rg.arcs[e0 + lane];
+        }
+        for (int j = 0; j < cntr; j += 4) {
+            unsigned long long du[4];
+            double len[4];
+            int src[4], fwd[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int jj = j + u < cntr ? j + u : 0;
+                src[u] = __shfl_sync(0xFFFFFFFFu, a.col, jj);
+                fwd[u] = __shfl_sync(0xFFFFFFFFu, a.id, jj);
+                len[u] = __shfl_sync(0xFFFFFFFFu, a.len, jj);
+                du[u] = (scan && j + u < cntr) ? __ldcg(&dist[static_cast<int64_t>(src[u]) * kTile + lane]) : kInfBits;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (du[u] != kInfBits && on_dag(du[u], len[u], dv)) {
+                    if (c == 0) {
+                        first = static_cast<uint32_t>(fwd[u]);
+                    }
+                    ++c;
+                    atomicAdd(&scnt[static_cast<int64_t>(src[u]) * kTile + lane], 1u);
+                }
+            }
+        }
+    }
+}
+
+// Vertices handled together by one warp in the count and fill passes (their loads are issued side by side).
+constexpr int kDagVertices = 2;
+
 // cnt[v][s] = DAG predecessors; scnt[u][s] += 1 for each DAG arc u -> v (warp per vertex, lane per source);
 // pred[v][s] = forward-CSR index of a DAG in-arc (the only one when cnt[v][s] == 1).
 // A lane whose tie bit stayed clear in the SSSP phase takes its single DAG arc from the predecessor key recorded
@@ -314,68 +354,65 @@ __device__ __forceinline__ void dag_count(const DeviceCsr& g, const DeviceCsr& r
                                           uint32_t* cnt, uint32_t* scnt, uint32_t* pred, int lane, int warp, int nwarps,
                                           unsigned long long* active_pairs) {
     unsigned long long active_count = 0;
-    for (int64_t v = warp; v < n; v += nwarps) {
-        const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
-        const bool active = lane < nsrc && dv != kInfBits && v != s_src[lane];
-        const bool tied = (__ldcg(&tie[v]) >> lane) & 1u;
-        const unsigned long long key = __ldcg(&pred_key[v * kTile + lane]);
-        pred_key[v * kTile + lane] = 0ull;  // sigma = 0.0
-        uint32_t c = 0;
-        uint32_t first = 0;
-        bool scan = active;
-        active_count += active ? 1ull : 0ull;
-        if (active && !tied && (key >> 32) == (dv >> 32)) {
-            const uint32_t e = static_cast<uint32_t>(key);
-            if (static_cast<int64_t>(e) < m_total) {
-                const Arc a = g.arcs[e];
-                const int32_t u = __ldg(&arc_src[e]);
-                if (a.col == static_cast<int32_t>(v)) {
-                    const unsigned long long du = __ldcg(&dist[static_cast<int64_t>(u) * kTile + lane]);
-                    if (du != kInfBits && on_dag(du, a.len, dv)) {
-                        c = 1;
-                        first = e;
-                        scan = false;
-                        atomicAdd(&scnt[static_cast<int64_t>(u) * kTile + lane], 1u);
-                    }
-                }
+    const int src_lane = lane < nsrc ? s_src[lane] : -1;
+    for (int64_t v0 = warp; v0 < n; v0 += static_cast<int64_t>(kDagVertices) * nwarps) {
+        int64_t vv[kDagVertices];
+        unsigned long long dv[kDagVertices], key[kDagVertices], du[kDagVertices];
+        bool active[kDagVertices], fast[kDagVertices];
+        uint32_t e[kDagVertices];
+        Arc a[kDagVertices];
+        int32_t u[kDagVertices];
+#pragma unroll
+        for (int i = 0; i < kDagVertices; ++i) {
+            vv[i] = v0 + static_cast<int64_t>(i) * nwarps;
+            dv[i] = kInfBits;
+            key[i] = 0ull;
+            bool tied = true;
+            if (vv[i] < n) {
+                dv[i] = __ldcg(&dist[vv[i] * kTile + lane]);
+                tied = (__ldcg(&tie[vv[i]]) >> lane) & 1u;
+                key[i] = __ldcg(&pred_key[vv[i] * kTile + lane]);
+                pred_key[vv[i] * kTile + lane] = 0ull;  // sigma = 0.0
+            }
+            active[i] = vv[i] < n && lane < nsrc && dv[i] != kInfBits && vv[i] != src_lane;
+            active_count += active[i] ? 1ull : 0ull;
+            e[i] = static_cast<uint32_t>(key[i]);
+            fast[i] = active[i] && !tied && (key[i] >> 32) == (dv[i] >> 32) && static_cast<int64_t>(e[i]) < m_total;
+        }
+#pragma unroll
+        for (int i = 0; i < kDagVertices; ++i) {
+            a[i] = Arc{ -1, 0, 0.0 };
+            u[i] = 0;
+            if (fast[i]) {
+                a[i] = g.arcs[e[i]];
+                u[i] = __ldg(&arc_src[e[i]]);
             }
         }
-        if (__ballot_sync(0xFFFFFFFFu, scan) != 0u) {
-            const int64_t beg = __ldg(&rg.row_ptr[v]);
-            const int64_t end = __ldg(&rg.row_ptr[v + 1]);
-            for (int64_t e0 = beg; e0 < end; e0 += 32) {
-                const int cntr = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
-                Arc a{ 0, 0, 0.0 };
-                if (lane < cntr) {
-                    a = rg.arcs[e0 + lane];
-                }
-                for (int j = 0; j < cntr; j += 4) {
-                    unsigned long long du[4];
-                    double len[4];
-                    int src[4], fwd[4];
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int jj = j + u < cntr ? j + u : 0;
-                        src[u] = __shfl_sync(0xFFFFFFFFu, a.col, jj);
-                        fwd[u] = __shfl_sync(0xFFFFFFFFu, a.id, jj);
-                        len[u] = __shfl_sync(0xFFFFFFFFu, a.len, jj);
-                        du[u] = (scan && j + u < cntr) ? __ldcg(&dist[static_cast<int64_t>(src[u]) * kTile + lane]) : kInfBits;
-                    }
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        if (du[u] != kInfBits && on_dag(du[u], len[u], dv)) {
-                            if (c == 0) {
-                                first = static_cast<uint32_t>(fwd[u]);
-                            }
-                            ++c;
-                            atomicAdd(&scnt[static_cast<int64_t>(src[u]) * kTile + lane], 1u);
-                        }
-                    }
-                }
-            }
+        for (int i = 0; i < kDagVertices; ++i) {
+            fast[i] = fast[i] && a[i].col == static_cast<int32_t>(vv[i]);
+            du[i] = fast[i] ? __ldcg(&dist[static_cast<int64_t>(u[i]) * kTile + lane]) : kInfBits;
         }
-        cnt[v * kTile + lane] = c;
-        pred[v * kTile + lane] = first;
+#pragma unroll
+        for (int i = 0; i < kDagVertices; ++i) {
+            if (vv[i] >= n) {
+                continue;  // warp-uniform
+            }
+            uint32_t c = 0;
+            uint32_t first = 0;
+            bool scan = active[i];
+            if (du[i] != kInfBits && on_dag(du[i], a[i].len, dv[i])) {
+                c = 1;
+                first = e[i];
+                scan = false;
+                atomicAdd(&scnt[static_cast<int64_t>(u[i]) * kTile + lane], 1u);
+            }
+            if (__ballot_sync(0xFFFFFFFFu, scan) != 0u) {
+                dag_count_scan(rg, vv[i], dv[i], scan, dist, scnt, lane, c, first);
+            }
+            cnt[vv[i] * kTile + lane] = c;
+            pred[vv[i] * kTile + lane] = first;
+        }
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -423,24 +460,58 @@ __device__ __forceinline__ unsigned long long block_exclusive_scan(const uint32_
     return total;
 }
 
+template <bool kTarget>
+__device__ __forceinline__ void dag_fill_scan(const DeviceCsr& rg, int64_t v, bool active, const unsigned long long* dist, const uint32_t* soff,
+                                              uint32_t* sfill, uint32_t* succ, int lane);
+
 // Fills the successor lists: each DAG arc u -> v is appended to (u, s), as its target v (kTarget: betweenness needs
 // nothing else) or as its forward-CSR index (the adjoint also needs the arc). A (v, s) with a single DAG predecessor
 // takes it from pred[v][s] (a forward index); only lanes with several re-scan v's in-arcs.
 template <bool kTarget>
 __device__ __forceinline__ void dag_fill(const DeviceCsr& rg, const int32_t* arc_src, int64_t n, const unsigned long long* dist, const uint32_t* cnt,
                                          const uint32_t* pred, const uint32_t* soff, uint32_t* sfill, uint32_t* succ, int lane, int warp, int nwarps) {
-    for (int64_t v = warp; v < n; v += nwarps) {
-        const uint32_t c = __ldcg(&cnt[v * kTile + lane]);
-        if (c == 1u) {
-            const uint32_t e = __ldcg(&pred[v * kTile + lane]);
-            const int64_t urow = static_cast<int64_t>(__ldg(&arc_src[e])) * kTile + lane;
-            const uint32_t pos = atomicAdd(&sfill[urow], 1u);
-            succ[__ldcg(&soff[urow]) + pos] = kTarget ? static_cast<uint32_t>(v) : e;
+    for (int64_t v0 = warp; v0 < n; v0 += static_cast<int64_t>(kDagVertices) * nwarps) {
+        // single-predecessor lanes of kDagVertices vertices, their loads side by side
+        uint32_t c[kDagVertices], e[kDagVertices], pos[kDagVertices], off[kDagVertices];
+        int64_t urow[kDagVertices];
+#pragma unroll
+        for (int i = 0; i < kDagVertices; ++i) {
+            const int64_t v = v0 + static_cast<int64_t>(i) * nwarps;
+            c[i] = v < n ? __ldcg(&cnt[v * kTile + lane]) : 0u;
+            e[i] = c[i] == 1u ? __ldcg(&pred[v * kTile + lane]) : 0u;
         }
-        const bool active = c >= 2u;
-        if (__ballot_sync(0xFFFFFFFFu, active) == 0u) {
-            continue;
+#pragma unroll
+        for (int i = 0; i < kDagVertices; ++i) {
+            urow[i] = c[i] == 1u ? static_cast<int64_t>(__ldg(&arc_src[e[i]])) * kTile + lane : 0;
         }
+#pragma unroll
+        for (int i = 0; i < kDagVertices; ++i) {
+            pos[i] = c[i] == 1u ? atomicAdd(&sfill[urow[i]], 1u) : 0u;
+            off[i] = c[i] == 1u ? __ldcg(&soff[urow[i]]) : 0u;
+        }
+#pragma unroll
+        for (int i = 0; i < kDagVertices; ++i) {
+            if (c[i] == 1u) {
+                const int64_t v = v0 + static_cast<int64_t>(i) * nwarps;
+                succ[off[i] + pos[i]] = kTarget ? static_cast<uint32_t>(v) : e[i];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kDagVertices; ++i) {
+            const int64_t v = v0 + static_cast<int64_t>(i) * nwarps;
+            const bool active = c[i] >= 2u;
+            if (v < n && __ballot_sync(0xFFFFFFFFu, active) != 0u) {
+                dag_fill_scan<kTarget>(rg, v, active, dist, soff, sfill, succ, lane);
+            }
+        }
+    }
+}
+
+// Appends v's DAG in-arcs for the lanes in `active` (several predecessors) by scanning v's in-arcs.
+template <bool kTarget>
+__device__ __forceinline__ void dag_fill_scan(const DeviceCsr& rg, int64_t v, bool active, const unsigned long long* dist, const uint32_t* soff,
+                                              uint32_t* sfill, uint32_t* succ, int lane) {
+    {  // one scope, so the scan below keeps its layout
         const unsigned long long dv = __ldcg(&dist[v * kTile + lane]);
         const int64_t beg = __ldg(&rg.row_ptr[v]);
         const int64_t end = __ldg(&rg.row_ptr[v + 1]);
