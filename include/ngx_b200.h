@@ -249,6 +249,28 @@ NGX_API int ngx_batch_autotune(ngx_graph* batch, int task, double* class_scales)
  */
 NGX_API int ngx_graph_update_weights(ngx_graph* graph, const double* w);
 
+/* ------------------------------------------------------------------------------------------------------------------
+ * Loading neurograph's network files (host only; no GPU needed until ngx_graph_create_from_network). Replaces
+ * DistributedGraph::construct_graph's loading for one process that reads every rank's files
+ * (source/graph/DistributedGraph.cpp:68-127 over FileLoader.cpp:96-327 and ArcTransformer.cpp:21-69): vertices per rank
+ * from <dir>/positions/rank_<r>_positions.txt, out arcs from <dir>/network/rank_<r><prefix>_out_network.txt (and in
+ * arcs from ..._in_network.txt when undirected), the same line rules, repeated arcs summed as int32, the same
+ * transforms in the same order, zero weights dropped. Vertex v of rank r gets the global id prefix[r] + v. Each row of
+ * the CSR is sorted by target. Files are parsed on `threads` host threads (0 = all).
+ */
+typedef struct ngx_network ngx_network;
+
+#define NGX_LOAD_REMOVE_SELF_ARCS 1 /* ArcTransformer::remove_self_arcs */
+#define NGX_LOAD_UNDIRECTED 2       /* ArcTransformer::synchronize_arcs: out arcs plus reversed in arcs */
+#define NGX_LOAD_ONE_WEIGHT 4       /* ArcTransformer::all_weights_one */
+
+NGX_API int ngx_network_load(const char* directory, int32_t number_ranks, const char* file_prefix, int flags, int threads, ngx_network** out);
+NGX_API int ngx_network_size(const ngx_network* network, int64_t* n, int64_t* m);
+/* row_ptr: n + 1 entries; col, w: m entries (weights as doubles of the summed int32 values). */
+NGX_API int ngx_network_csr(const ngx_network* network, int64_t* row_ptr, int32_t* col, double* w);
+NGX_API int ngx_graph_create_from_network(const ngx_network* network, int device, ngx_graph** out);
+NGX_API void ngx_network_destroy(ngx_network* network);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,6 +85,7 @@ EXPORTED = [
     "ngx_status_string", "ngx_last_error", "ngx_version", "ngx_graph_create", "ngx_graph_destroy", "ngx_graph_size",
     "ngx_graph_request_abort", "ngx_graph_set_stream", "ngx_graph_set_memory_budget", "ngx_apsp", "ngx_sssp_rows", "ngx_brandes",
     "ngx_apsp_grad", "ngx_batch_create", "ngx_batch_run", "ngx_batch_autotune", "ngx_graph_update_weights", "ngx_apsp_noalloc", "ngx_exact_accumulate", "ngx_exact_round", "ngx_graph_source_order",
+    "ngx_network_load", "ngx_network_size", "ngx_network_csr", "ngx_graph_create_from_network", "ngx_network_destroy",
 ]
 
 
@@ -117,6 +118,12 @@ def library() -> C.CDLL:
         lib.ngx_graph_update_weights.argtypes = [C.c_void_p, C.c_void_p]
         lib.ngx_apsp_noalloc.argtypes = [C.c_void_p, C.POINTER(_Opts), C.POINTER(_Result)]
         lib.ngx_graph_source_order.argtypes = [C.c_void_p, C.c_void_p]
+        lib.ngx_network_load.argtypes = [C.c_char_p, C.c_int32, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        lib.ngx_network_size.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        lib.ngx_network_csr.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.ngx_graph_create_from_network.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]
+        lib.ngx_network_destroy.argtypes = [C.c_void_p]
+        lib.ngx_network_destroy.restype = None
         lib.ngx_exact_accumulate.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
         lib.ngx_exact_round.argtypes = [C.c_void_p]
         lib.ngx_exact_round.restype = C.c_double
@@ -176,6 +183,33 @@ class Graph:
         handle = C.c_void_p()
         _check(lib.ngx_graph_create(C.byref(csr), int(device), C.byref(handle)))
         self._handle = handle
+
+    @classmethod
+    def from_network(cls, directory: str, number_ranks: int, file_prefix: str = "", remove_self_arcs: bool = False,
+                     undirected: bool = False, one_weight: bool = False, threads: int = 0, device: int = 0) -> "Graph":
+        """Loads neurograph's per-rank network files (ngx_network_load) straight into a device graph
+        (ngx_graph_create_from_network); the CSR is also kept on the host as row_ptr / col / w."""
+        lib = library()
+        flags = (LOAD_REMOVE_SELF_ARCS if remove_self_arcs else 0) | (LOAD_UNDIRECTED if undirected else 0) | \
+            (LOAD_ONE_WEIGHT if one_weight else 0)
+        net = C.c_void_p()
+        _check(lib.ngx_network_load(os.fsencode(directory), int(number_ranks), file_prefix.encode(), flags, int(threads), C.byref(net)))
+        try:
+            n, m = C.c_int64(), C.c_int64()
+            _check(lib.ngx_network_size(net, C.byref(n), C.byref(m)))
+            self = cls.__new__(cls)
+            self.n, self.m = n.value, m.value
+            self.row_ptr = np.zeros(self.n + 1, np.int64)
+            self.col = np.zeros(max(self.m, 1), np.int32)
+            self.w = np.zeros(max(self.m, 1), np.float64)
+            _check(lib.ngx_network_csr(net, self.row_ptr.ctypes.data, self.col.ctypes.data, self.w.ctypes.data))
+            self.col, self.w = self.col[: self.m], self.w[: self.m]
+            handle = C.c_void_p()
+            _check(lib.ngx_graph_create_from_network(net, int(device), C.byref(handle)))
+            self._handle = handle
+        finally:
+            lib.ngx_network_destroy(net)
+        return self
 
     def close(self) -> None:
         if getattr(self, "_handle", None):
@@ -398,6 +432,30 @@ class Batch:
         if flat.size != sum(self.ms):
             raise ValueError("weights do not match the batch's arcs")
         _check(library().ngx_graph_update_weights(self._handle, flat.ctypes.data if flat.size else None))
+
+
+LOAD_REMOVE_SELF_ARCS, LOAD_UNDIRECTED, LOAD_ONE_WEIGHT = 1, 2, 4
+
+
+def load_network(directory: str, number_ranks: int, file_prefix: str = "", remove_self_arcs: bool = False,
+                 undirected: bool = False, one_weight: bool = False, threads: int = 0):
+    """Reads neurograph's per-rank network files (ngx_network_load, host only) and returns (n, row_ptr, col, w), the
+    global CSR a Graph is built from."""
+    flags = (LOAD_REMOVE_SELF_ARCS if remove_self_arcs else 0) | (LOAD_UNDIRECTED if undirected else 0) | \
+        (LOAD_ONE_WEIGHT if one_weight else 0)
+    lib = library()
+    handle = C.c_void_p()
+    _check(lib.ngx_network_load(os.fsencode(directory), int(number_ranks), file_prefix.encode(), flags, int(threads), C.byref(handle)))
+    try:
+        n, m = C.c_int64(), C.c_int64()
+        _check(lib.ngx_network_size(handle, C.byref(n), C.byref(m)))
+        row_ptr = np.zeros(n.value + 1, np.int64)
+        col = np.zeros(max(m.value, 1), np.int32)
+        w = np.zeros(max(m.value, 1), np.float64)
+        _check(lib.ngx_network_csr(handle, row_ptr.ctypes.data, col.ctypes.data, w.ctypes.data))
+    finally:
+        lib.ngx_network_destroy(handle)
+    return n.value, row_ptr, col[: m.value], w[: m.value]
 
 
 def exact_accumulate(values, digits=None) -> np.ndarray:

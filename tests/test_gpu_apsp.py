@@ -184,3 +184,21 @@ def test_source_order_is_a_permutation_and_runs_agree():
     with ngx.Batch(graphs) as b:
         results, _ = b.run("apsp", per_source=True)
     assert np.array_equal(results[0].per_source["sum"], whole.per_source["sum"])
+
+
+def test_graph_from_network_files(tmp_path, restatement):
+    """ngx_network_load + ngx_graph_create_from_network: a graph built straight from per-rank network files runs the
+    same APSP as one built from the loaded CSR, and matches the oracle on that CSR."""
+    from test_loader import write_network
+
+    write_network(str(tmp_path), 500, 2, np.random.default_rng(3))
+    with ngx.Graph.from_network(str(tmp_path), 2, remove_self_arcs=True) as g:
+        got = g.apsp(per_source=True, hist_bins=64, hist_max=40.0)
+        csr = oracle.Csr.from_arrays(g.n, g.row_ptr, g.col, g.w)
+    want = restatement.apsp(csr, bins=64, hist_max=40.0)
+    assert got.sum_distances == want["sum_distances"] and got.unreachable == want["unreachable"]
+    assert got.cluster_sizes == want["cluster_sizes"] and np.array_equal(got.hist, want["hist"])
+    n, rp, c, w = ngx.load_network(str(tmp_path), 2, remove_self_arcs=True)
+    with ngx.Graph(n, rp, c, w) as g2:
+        again = g2.apsp()
+    assert again.sum_distances == got.sum_distances and again.diameter == got.diameter
