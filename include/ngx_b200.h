@@ -271,6 +271,21 @@ NGX_API int ngx_network_csr(const ngx_network* network, int64_t* row_ptr, int32_
 NGX_API int ngx_graph_create_from_network(const ngx_network* network, int device, ngx_graph** out);
 NGX_API void ngx_network_destroy(ngx_network* network);
 
+/* ------------------------------------------------------------------------------------------------------------------
+ * Diameter approximation. Replaces DiameterApproximation::compute_approximation (metrics/paths/DiameterApproximation.h):
+ * balls of radius r grown around random centres, the graph contracted to its balls (arc weight w + d(u) + d(v), the
+ * last arc of a centre pair in CSR order winning), and the exact diameter of the contracted graph, plus 2r. Centres
+ * are drawn from std::mt19937 seeded with `seed` through std::uniform_real_distribution<double>(0, 1) (the reference's
+ * DefaultRandomNumberGenerator, seeded there with the MPI rank: 0 for one rank), or, when draws != NULL, from
+ * draws[0], draws[1], ... (the last one repeating). Weights must be positive integers below 2^31 (zeros are absent
+ * arcs), as the reference's 32-bit weights and unsigned distances require; the CSR's arc order is the reference's
+ * stored order when the results must agree exactly. ngx_diameter_contract (host only) returns the contracted graph;
+ * ngx_diameter_approximation runs its APSP on `device` with the batched kernel.
+ */
+NGX_API int ngx_diameter_contract(const ngx_csr* csr, uint64_t r, const double* draws, int64_t num_draws, uint32_t seed, ngx_network** contracted);
+NGX_API int ngx_diameter_approximation(const ngx_csr* csr, uint64_t r, const double* draws, int64_t num_draws, uint32_t seed, int device,
+                                       uint64_t* diameter);
+
 #ifdef __cplusplus
 }
 #endif

@@ -86,6 +86,7 @@ EXPORTED = [
     "ngx_graph_request_abort", "ngx_graph_set_stream", "ngx_graph_set_memory_budget", "ngx_apsp", "ngx_sssp_rows", "ngx_brandes",
     "ngx_apsp_grad", "ngx_batch_create", "ngx_batch_run", "ngx_batch_autotune", "ngx_graph_update_weights", "ngx_apsp_noalloc", "ngx_exact_accumulate", "ngx_exact_round", "ngx_graph_source_order",
     "ngx_network_load", "ngx_network_size", "ngx_network_csr", "ngx_graph_create_from_network", "ngx_network_destroy",
+    "ngx_diameter_contract", "ngx_diameter_approximation",
 ]
 
 
@@ -124,6 +125,9 @@ def library() -> C.CDLL:
         lib.ngx_graph_create_from_network.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]
         lib.ngx_network_destroy.argtypes = [C.c_void_p]
         lib.ngx_network_destroy.restype = None
+        lib.ngx_diameter_contract.argtypes = [C.POINTER(_Csr), C.c_uint64, C.c_void_p, C.c_int64, C.c_uint32, C.POINTER(C.c_void_p)]
+        lib.ngx_diameter_approximation.argtypes = [C.POINTER(_Csr), C.c_uint64, C.c_void_p, C.c_int64, C.c_uint32, C.c_int,
+                                                   C.POINTER(C.c_uint64)]
         lib.ngx_exact_accumulate.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
         lib.ngx_exact_round.argtypes = [C.c_void_p]
         lib.ngx_exact_round.restype = C.c_double
@@ -456,6 +460,48 @@ def load_network(directory: str, number_ranks: int, file_prefix: str = "", remov
     finally:
         lib.ngx_network_destroy(handle)
     return n.value, row_ptr, col[: m.value], w[: m.value]
+
+
+def _csr_struct(n, row_ptr, col, w):
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
+    c = np.ascontiguousarray(col, dtype=np.int32)
+    ww = np.ascontiguousarray(w, dtype=np.float64)
+    return _Csr(int(n), c.size, rp.ctypes.data, c.ctypes.data if c.size else None, ww.ctypes.data if c.size else None), (rp, c, ww)
+
+
+def _network_arrays(lib, handle):
+    n, m = C.c_int64(), C.c_int64()
+    _check(lib.ngx_network_size(handle, C.byref(n), C.byref(m)))
+    row_ptr = np.zeros(n.value + 1, np.int64)
+    col = np.zeros(max(m.value, 1), np.int32)
+    w = np.zeros(max(m.value, 1), np.float64)
+    _check(lib.ngx_network_csr(handle, row_ptr.ctypes.data, col.ctypes.data, w.ctypes.data))
+    return n.value, row_ptr, col[: m.value], w[: m.value]
+
+
+def diameter_contract(n, row_ptr, col, w, r: int, draws=None, seed: int = 0):
+    """The contracted graph of the diameter approximation (ngx_diameter_contract, host only): (n, row_ptr, col, w)."""
+    lib = library()
+    csr, keep = _csr_struct(n, row_ptr, col, w)
+    d = None if draws is None else np.ascontiguousarray(draws, np.float64)
+    handle = C.c_void_p()
+    _check(lib.ngx_diameter_contract(C.byref(csr), int(r), None if d is None else d.ctypes.data, 0 if d is None else d.size, int(seed),
+                                     C.byref(handle)))
+    try:
+        return _network_arrays(lib, handle)
+    finally:
+        lib.ngx_network_destroy(handle)
+
+
+def diameter_approximation(n, row_ptr, col, w, r: int, draws=None, seed: int = 0, device: int = 0) -> int:
+    """DiameterApproximation::compute_approximation: the contracted graph's exact diameter (GPU) plus 2r."""
+    lib = library()
+    csr, keep = _csr_struct(n, row_ptr, col, w)
+    d = None if draws is None else np.ascontiguousarray(draws, np.float64)
+    out = C.c_uint64()
+    _check(lib.ngx_diameter_approximation(C.byref(csr), int(r), None if d is None else d.ctypes.data, 0 if d is None else d.size, int(seed),
+                                          int(device), C.byref(out)))
+    return int(out.value)
 
 
 def exact_accumulate(values, digits=None) -> np.ndarray:

@@ -22,14 +22,8 @@
 #include <vector>
 
 #include "ngx_common.cuh"
+#include "ngx_network.h"
 
-struct ngx_network {
-    int64_t n = 0;
-    std::vector<int64_t> rank_nodes;  // vertices per rank
-    std::vector<int64_t> row_ptr;     // n + 1
-    std::vector<int32_t> col;         // global target ids, ascending within a row
-    std::vector<double> w;            // summed int32 weights (after the transforms), never 0
-};
 
 namespace ngx {
 namespace {

@@ -295,6 +295,14 @@ class RefGraph:
                                                            C.c_int64(srcs.size), summary.ctypes.data_as(C.c_void_p)))
         return summary
 
+    def diameter_approximation(self, r: int, draws=None, seed: int = 0) -> int:
+        """DiameterApproximation::compute_approximation of the reference (draws: replayed generator values)."""
+        out = C.c_uint64()
+        d = None if draws is None else np.ascontiguousarray(draws, np.float64)
+        self.ref._check(self.ref.lib.ngxref_diameter_approximation(self.handle, C.c_uint64(r), None if d is None else d.ctypes.data_as(C.c_void_p),
+                                                                    C.c_int64(0 if d is None else d.size), C.c_uint(seed), C.byref(out)))
+        return int(out.value)
+
     def betweenness(self, algorithm=0):
         bc = np.zeros(max(self.n, 1), np.float64)
         avg = C.c_double()

@@ -24,6 +24,8 @@
 #include "metrics/paths/DeltaStepping.h"
 #include "metrics/paths/Dijkstra.h"
 #include "metrics/paths/BetweennessCentralityVariants/BrandesVariant.h"
+#include "metrics/paths/DiameterApproximation.h"
+#include "utility/RandomNumberGenerator.h"
 
 #include <mpi-wrapper/MPIWrapper.h>
 #include <mpi-wrapper/instrumentation/MPIProgress.h>
@@ -288,6 +290,40 @@ int ngxref_delta_stepping(void* handle, std::uint64_t delta, int epoch, const st
 }
 
 /* Per-node betweenness of all sources (BrandesVariant) and the average (BetweennessCentrality, algorithm 0 Brandes / 1 PathEnumeration). */
+namespace {
+// Replays a fixed list of draws (the last one repeating), for the constant and single-centre generators of the
+// reference's own diameter tests.
+class ReplayRandomNumberGenerator : public RandomNumberGenerator {
+public:
+    ReplayRandomNumberGenerator(const double* draws, std::int64_t count)
+        : values(draws, draws + count) { }
+    [[nodiscard]] double draw() override {
+        const auto v = values[next < values.size() ? next : values.size() - 1];
+        ++next;
+        return v;
+    }
+
+private:
+    std::vector<double> values;
+    std::size_t next{ 0 };
+};
+} // namespace
+
+/* DiameterApproximation::compute_approximation (metrics/paths/DiameterApproximation.h) with the default generator
+ * (std::mt19937 seeded with `seed`) or, when draws != NULL, the replayed draws. */
+int ngxref_diameter_approximation(void* handle, std::uint64_t r, const double* draws, std::int64_t num_draws, unsigned int seed, std::uint64_t* out) {
+    return guarded([&] {
+        const auto& graph = static_cast<RefGraph*>(handle)->graph;
+        if (draws != nullptr && num_draws > 0) {
+            auto generator = ReplayRandomNumberGenerator{ draws, num_draws };
+            *out = DiameterApproximation::compute_approximation(graph, r, generator);
+        } else {
+            auto generator = DefaultRandomNumberGenerator{ seed };
+            *out = DiameterApproximation::compute_approximation(graph, r, generator);
+        }
+    });
+}
+
 int ngxref_betweenness(void* handle, int algorithm, double* per_node, double* average) {
     return guarded([&] {
         const auto& graph = static_cast<RefGraph*>(handle)->graph;
