@@ -26,6 +26,7 @@ bit-exact with the reference on integer weights) runs in one process per host co
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import math
 import os
@@ -65,8 +66,9 @@ def parse():
     ap.add_argument("--degree", type=float, default=WORKLOAD["mean_degree"])
     ap.add_argument("--length-scale", type=float, default=WORKLOAD["length_scale"])
     ap.add_argument("--sigma", type=float, default=1.0, help="log-normal sigma of the weights")
-    ap.add_argument("--workload", choices=["single", "uneven-batch"], default="single",
-                    help="single: one connectome (the headline); uneven-batch: 512 connectomes of 500-20000 vertices in one handle")
+    ap.add_argument("--workload", choices=["single", "uneven-batch", "scc"], default="single",
+                    help="single: one connectome (the headline); uneven-batch: 512 connectomes of 500-20000 vertices in one "
+                         "handle; scc: strongly connected components of the connectome (ngx_scc) beside the reference's SCC")
     ap.add_argument("--delta", type=float, default=0.25)
     ap.add_argument("--mode", choices=["brandes", "apsp", "grad", "plain"], default="brandes",
                     help="what one step runs: APSP+Brandes (the headline), APSP only, APSP+gradient, or the plain per-source form")
@@ -384,6 +386,111 @@ def run_uneven_batch(args, ngx, torch, rank, world, barrier, max_over_ranks, sum
     print(json.dumps(line), flush=True)
 
 
+@contextlib.contextmanager
+def stdout_to_stderr():
+    """Sends what native code prints on fd 1 (the reference's timer reports) to stderr, keeping stdout to the one
+    JSON line."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
+def run_scc(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ranks, local_rank):
+    """Strongly connected components of the connectome per step (ngx_scc: trim, colour and peel passes), every rank
+    on its own replica; the reference's StronglyConnectedComponents (Multistep, its default, and TarjanGathered) on the
+    host beside it."""
+    t0 = time.perf_counter()
+    c = make_graph(args.n, args.degree, args.length_scale, args.sigma)
+    log(f"[bench] graph n={c.n} m={c.m} generated in {time.perf_counter() - t0:.1f}s")
+    torch.cuda.empty_cache()
+    stream = torch.cuda.Stream()
+    g = ngx.Graph(c.n, c.row_ptr, c.col, c.w, device=local_rank)
+    g.set_stream(stream.cuda_stream)
+    for _ in range(args.warmup):
+        first = g.scc()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    clocks.wait_first_sample()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        out = g.scc()
+    ev1.record(stream)
+    barrier()
+    clock_info = clocks.stop()
+    elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    arcs = int(c.m)
+    value = sum_over_ranks(float(arcs * args.steps)) / elapsed / 1e9
+    assert out["number_components"] == first["number_components"]
+    g.close()
+    # compulsory bytes of one call: both CSRs read once (4 B target per arc and direction, 8 B row offset per vertex
+    # and direction) and the component array written once
+    alg = 2 * (4 * arcs + 8 * c.n) + 4 * c.n
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (elapsed / args.steps) / 1e9
+    e2e = None
+    if not args.no_e2e:
+        pinned = [torch.from_numpy(x).pin_memory().numpy() for x in (c.row_ptr, c.col, c.w)]
+        barrier()
+        t1 = time.perf_counter()
+        with ngx.Graph(c.n, *pinned, device=local_rank) as ge:
+            res = ge.scc()
+        barrier()
+        e2e_elapsed = max_over_ranks(time.perf_counter() - t1)
+        e2e = {"value": sum_over_ranks(float(arcs)) / e2e_elapsed / 1e9, "unit": "G arcs/s",
+               "h2d_bytes_per_step": int(sum(x.nbytes for x in pinned)), "d2h_bytes_per_step": int(res["component"].nbytes + 8 * (c.n + 3)),
+               "timing": "wall clock, synchronized; graph handle created from pinned host CSR arrays, one ngx_scc call, "
+                         "components and size histogram to host"}
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle
+
+        if oracle.Reference.available():
+            ref = oracle.Reference()
+            with stdout_to_stderr():
+                rg = ref.graph(c.n, c.row_ptr, c.col, np.ones(c.m, np.int32))  # SCC ignores the weights
+                timings = {}
+                for name, algorithm in (("multistep", 3), ("tarjan_gathered", 0)):
+                    t1 = time.perf_counter()
+                    got = rg.scc(algorithm)
+                    timings[name] = time.perf_counter() - t1
+                    if got["component_sizes"] != out["component_sizes"]:
+                        raise RuntimeError(f"the reference's {name} SCC differs from ngx_scc")
+            best = min(timings, key=timings.get)
+            cpu = {"value": arcs / timings[best] / 1e9, "unit": "G arcs/s", "cores": 1, "kind": "reference",
+                   "sample": f"the whole graph once per algorithm, reference StronglyConnectedComponents built from source "
+                             f"(one rank): multistep {timings['multistep']:.3f} s, tarjan_gathered {timings['tarjan_gathered']:.3f} s; "
+                             f"value from the faster ({best}); same component sizes as ngx_scc"}
+    if rank != 0:
+        return
+    line = {
+        "metric": "SCC arcs per second (strongly connected components of one graph)", "value": value, "unit": "G arcs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": dict(WORKLOAD, **workload_overrides(args), workload=f"strongly connected components of the synthetic connectome "
+                       f"N={c.n}, {c.m} arcs (ngx_scc per step, every rank on its own replica)",
+                       components=out["number_components"], largest=out["largest_component_size"],
+                       l2="graph arrays (both CSRs, ~16 B per arc each) exceed the 126 MB L2 at this size; no flush"),
+        "gpu_launches": None,
+        "clocks": clock_info,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)", "traffic": None,
+                     "algorithmic_bytes_per_launch": alg,
+                     "kernel": "the whole ngx_scc call (trim, colour, peel passes with host-read change flags); bytes: "
+                               "both CSRs read once + components written once"},
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
@@ -418,8 +525,9 @@ def main():
     def sum_over_ranks(x):
         return reduce_over_ranks(dist, x, "sum", "cuda")
 
-    if args.workload == "uneven-batch":
-        run_uneven_batch(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ranks, local_rank)
+    if args.workload in ("uneven-batch", "scc"):
+        run = run_uneven_batch if args.workload == "uneven-batch" else run_scc
+        run(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ranks, local_rank)
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()

@@ -286,6 +286,15 @@ NGX_API int ngx_diameter_contract(const ngx_csr* csr, uint64_t r, const double* 
 NGX_API int ngx_diameter_approximation(const ngx_csr* csr, uint64_t r, const double* draws, int64_t num_draws, uint32_t seed, int device,
                                        uint64_t* diameter);
 
+/* Strongly connected components of a single-graph handle, on its device.
+ * Replaces StronglyConnectedComponents::compute_strongly_connected_components (source/metrics/connectivity/
+ * StronglyConnectedComponents.h:17-36) and its SccResult (number_components, largest_component_size,
+ * component_sizes: size -> number of components), which all of the reference's algorithms (Tarjan gathered, forward
+ * backward, coloring, multistep) return identically. Weights and self arcs are ignored; a vertex without arcs is a
+ * component of its own. component (host int32[n] or NULL) receives each vertex's component, named by its largest
+ * vertex; size_histogram (host uint64[n + 1] or NULL) receives the number of components of each size. */
+NGX_API int ngx_scc(ngx_graph* graph, int32_t* component, uint64_t* number_components, uint64_t* largest_component, uint64_t* size_histogram);
+
 #ifdef __cplusplus
 }
 #endif

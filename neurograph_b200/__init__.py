@@ -86,7 +86,7 @@ EXPORTED = [
     "ngx_graph_request_abort", "ngx_graph_set_stream", "ngx_graph_set_memory_budget", "ngx_apsp", "ngx_sssp_rows", "ngx_brandes",
     "ngx_apsp_grad", "ngx_batch_create", "ngx_batch_run", "ngx_batch_autotune", "ngx_graph_update_weights", "ngx_apsp_noalloc", "ngx_exact_accumulate", "ngx_exact_round", "ngx_graph_source_order",
     "ngx_network_load", "ngx_network_size", "ngx_network_csr", "ngx_graph_create_from_network", "ngx_network_destroy",
-    "ngx_diameter_contract", "ngx_diameter_approximation",
+    "ngx_diameter_contract", "ngx_diameter_approximation", "ngx_scc",
 ]
 
 
@@ -128,6 +128,7 @@ def library() -> C.CDLL:
         lib.ngx_diameter_contract.argtypes = [C.POINTER(_Csr), C.c_uint64, C.c_void_p, C.c_int64, C.c_uint32, C.POINTER(C.c_void_p)]
         lib.ngx_diameter_approximation.argtypes = [C.POINTER(_Csr), C.c_uint64, C.c_void_p, C.c_int64, C.c_uint32, C.c_int,
                                                    C.POINTER(C.c_uint64)]
+        lib.ngx_scc.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_void_p]
         lib.ngx_exact_accumulate.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
         lib.ngx_exact_round.argtypes = [C.c_void_p]
         lib.ngx_exact_round.restype = C.c_double
@@ -248,6 +249,18 @@ class Graph:
         out = np.zeros(max(self.n, 1), np.int64)
         _check(library().ngx_graph_source_order(self._handle, out.ctypes.data))
         return out[: self.n]
+
+    def scc(self) -> dict:
+        """Strongly connected components (ngx_scc), as the reference's SccResult: number_components,
+        largest_component_size, component_sizes {size: number of components}; plus `component`, each vertex's
+        component named by its largest vertex."""
+        comp = np.zeros(max(self.n, 1), np.int32)
+        hist = np.zeros(self.n + 1, np.uint64)
+        count, largest = C.c_uint64(0), C.c_uint64(0)
+        _check(library().ngx_scc(self._handle, comp.ctypes.data, C.byref(count), C.byref(largest), hist.ctypes.data))
+        sizes = {int(k): int(hist[k]) for k in np.nonzero(hist)[0]}
+        return {"number_components": count.value, "largest_component_size": largest.value, "component_sizes": sizes,
+                "component": comp[: self.n]}
 
     def update_weights(self, w) -> None:
         """Replaces the arc weights in place (same arcs; no weight may change between zero and non-zero)."""

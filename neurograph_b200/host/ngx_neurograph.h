@@ -145,4 +145,23 @@ template <typename d_type>
     return sum / static_cast<double>(gpu.number_nodes());  // BetweennessCentrality.h:76-79
 }
 
+// StronglyConnectedComponents::compute_strongly_connected_components on the GPU (any SccAlgorithm gives this result).
+[[nodiscard]] inline SccResult compute_scc_gpu(const DistributedGraph& graph) {
+    const auto gpu = GpuGraph{ graph };
+    const auto n = static_cast<std::size_t>(gpu.number_nodes());
+    auto histogram = std::vector<std::uint64_t>(n + 1);
+    auto number = std::uint64_t{};
+    auto largest = std::uint64_t{};
+    check(ngx_scc(gpu.get(), nullptr, &number, &largest, histogram.data()));
+    auto out = SccResult{};
+    out.number_components = number;
+    out.largest_component_size = largest;
+    for (std::size_t size = 1; size <= n; ++size) {
+        if (histogram[size] != 0) {
+            out.component_sizes[size] = histogram[size];
+        }
+    }
+    return out;
+}
+
 }  // namespace ngx_neurograph

@@ -119,6 +119,8 @@ class Restatement:
         lib.ngxo_brandes.argtypes = [C.POINTER(_Graph), C.c_void_p, C.c_int64, _f64p]
         lib.ngxo_apsp_grad.argtypes = [C.POINTER(_Graph), C.c_void_p, C.c_int64, _f64p, _f64p, C.POINTER(_Totals)]
         lib.ngxo_exact_sum.argtypes = [_f64p, C.c_int64]
+        lib.ngxo_scc.argtypes = [C.POINTER(_Graph), C.c_void_p]
+        lib.ngxo_scc.restype = C.c_int64
         lib.ngxo_exact_sum.restype = C.c_double
         self.lib = lib
 
@@ -134,6 +136,18 @@ class Restatement:
     def exact_sum(self, x) -> float:
         x = np.ascontiguousarray(x, dtype=np.float64)
         return self.lib.ngxo_exact_sum(x, x.size)
+
+    def scc(self, g: Csr) -> dict:
+        """Tarjan's strongly connected components (ngxo_scc): the SccResult summary plus `component`, each vertex's
+        component named by its largest vertex."""
+        comp = np.zeros(max(g.n, 1), np.int32)
+        count = self.lib.ngxo_scc(C.byref(self._graph(g)), comp.ctypes.data)
+        if count < 0:
+            raise RuntimeError(f"ngxo_scc failed ({count})")
+        out = _scc_summary(comp[: g.n])
+        assert out["number_components"] == count
+        out["component"] = comp[: g.n]
+        return out
 
     def sssp(self, g: Csr, source: int, metric: int = METRIC_REGULAR) -> np.ndarray:
         dist = np.empty(max(g.n, 1), dtype=np.float64)
@@ -185,6 +199,14 @@ class Restatement:
         if rc != 0:
             raise ValueError(f"ngxo_apsp_grad failed ({rc})")
         return dcpl[: g.m], deff[: g.m], _totals_dict(totals)
+
+
+def _scc_summary(component: np.ndarray) -> dict:
+    """SccResult of the reference from per-vertex component names: number, largest size, {size: components}."""
+    _, sizes = np.unique(component, return_counts=True)
+    keys, counts = np.unique(sizes, return_counts=True)
+    return {"number_components": int(sizes.size), "largest_component_size": int(sizes.max()) if sizes.size else 0,
+            "component_sizes": {int(k): int(c) for k, c in zip(keys, counts)}}
 
 
 def _cluster_sizes(n: int, unreachable: np.ndarray) -> dict:
@@ -302,6 +324,16 @@ class RefGraph:
         self.ref._check(self.ref.lib.ngxref_diameter_approximation(self.handle, C.c_uint64(r), None if d is None else d.ctypes.data_as(C.c_void_p),
                                                                     C.c_int64(0 if d is None else d.size), C.c_uint(seed), C.byref(out)))
         return int(out.value)
+
+    def scc(self, algorithm: int = 3, tail_threshold: int = 0) -> dict:
+        """StronglyConnectedComponents::compute_strongly_connected_components (algorithm: 0 TarjanGathered,
+        1 ForwardBackward, 2 Coloring, 3 Multistep)."""
+        count, largest = C.c_uint64(), C.c_uint64()
+        sizes = np.zeros(self.n + 1, np.uint64)
+        self.ref._check(self.ref.lib.ngxref_scc(self.handle, int(algorithm), C.c_uint64(tail_threshold), C.byref(count), C.byref(largest),
+                                                sizes.ctypes.data_as(C.c_void_p), C.c_int64(sizes.size)))
+        return {"number_components": int(count.value), "largest_component_size": int(largest.value),
+                "component_sizes": {int(k): int(sizes[k]) for k in np.nonzero(sizes)[0]}}
 
     def betweenness(self, algorithm=0):
         bc = np.zeros(max(self.n, 1), np.float64)

@@ -3,13 +3,14 @@
  * code, go through the reference's AllPairsShortestPath / BetweennessCentrality and through the C++20 adapter
  * neurograph_b200/host/ngx_neurograph.h that a maintainer would call from those classes. The results
  * must agree: CPL, diameter, unreachable pairs and cluster sizes exactly, efficiency within the reference's rounding,
- * average betweenness within 1e-12 relative. Exit code 0 when every fixture agrees. Needs a B200.
+ * average betweenness within 1e-12 relative, strongly connected components exactly. Exit code 0 when every fixture agrees. Needs a B200.
  */
 #include "GraphTest.h"
 #include "Types.h"
 
 #include "metrics/paths/AllPairsShortestPath.h"
 #include "metrics/paths/BetweennessCentrality.h"
+#include "metrics/connectivity/StronglyConnectedComponents.h"
 
 #include "ngx_neurograph.h"
 
@@ -66,8 +67,12 @@ int main(int argc, char** argv) {
         const auto bc_ref = BetweennessCentrality::compute_average_betweenness_centrality(graph);
         const auto bc_gpu = ngx_neurograph::compute_average_betweenness_gpu(graph);
         const bool bc_ok = std::fabs(bc_gpu - bc_ref) <= 1e-12 * std::fmax(1.0, std::fabs(bc_ref));
-        std::printf("%-40s apsp %s  inverse %s  betweenness %s (%.17g vs %.17g)\n", name, apsp_ok ? "ok" : "MISMATCH", inv_ok ? "ok" : "MISMATCH",
-                    bc_ok ? "ok" : "MISMATCH", bc_gpu, bc_ref);
+        const auto scc_ref = StronglyConnectedComponents::compute_strongly_connected_components(graph);
+        const auto scc_gpu = ngx_neurograph::compute_scc_gpu(graph);
+        const bool scc_ok = scc_gpu.number_components == scc_ref.number_components && scc_gpu.largest_component_size == scc_ref.largest_component_size &&
+                            scc_gpu.component_sizes == scc_ref.component_sizes;
+        std::printf("%-40s apsp %s  inverse %s  betweenness %s (%.17g vs %.17g)  scc %s\n", name, apsp_ok ? "ok" : "MISMATCH", inv_ok ? "ok" : "MISMATCH",
+                    bc_ok ? "ok" : "MISMATCH", bc_gpu, bc_ref, scc_ok ? "ok" : "MISMATCH");
         if (!apsp_ok || !inv_ok) {
             std::printf("  regular: gpu cpl %.17g eff %.17g dia %llu unreach %llu clusters %zu | ref cpl %.17g eff %.17g dia %llu unreach %llu clusters %zu\n",
                         gpu.average_shortest_path_length, gpu.average_efficiency, static_cast<unsigned long long>(gpu.diameter),
@@ -77,7 +82,7 @@ int main(int argc, char** argv) {
             std::printf("  inverse: gpu cpl %.17g eff %.17g dia %.17g | ref cpl %.17g eff %.17g dia %.17g\n", gpu_inv.average_shortest_path_length,
                         gpu_inv.average_efficiency, gpu_inv.diameter, ref_inv.average_shortest_path_length, ref_inv.average_efficiency, ref_inv.diameter);
         }
-        failures += apsp_ok && inv_ok && bc_ok ? 0 : 1;
+        failures += apsp_ok && inv_ok && bc_ok && scc_ok ? 0 : 1;
     }
     mpiPP::MPIWrapper::finalize();
     return failures == 0 ? 0 : 1;

@@ -640,3 +640,79 @@ int ngxo_apsp_grad(const ngxo_graph* g, const int64_t* sources, int64_t k, doubl
     free(delta_g);
     return rc;
 }
+
+/* ------------------------------------------------------------------ strongly connected components (Tarjan 1972) */
+int64_t ngxo_scc(const ngxo_graph* g, int32_t* comp) {
+    if (!graph_valid(g) || comp == NULL) {
+        return -1;
+    }
+    const int64_t n = g->n;
+    int64_t* index = malloc(sizeof(int64_t) * (size_t)(n + 1));
+    int64_t* low = malloc(sizeof(int64_t) * (size_t)(n + 1));
+    int64_t* next_arc = malloc(sizeof(int64_t) * (size_t)(n + 1));
+    int64_t* call = malloc(sizeof(int64_t) * (size_t)(n + 1)); /* depth-first path */
+    int64_t* stack = malloc(sizeof(int64_t) * (size_t)(n + 1)); /* Tarjan's vertex stack */
+    uint8_t* on_stack = calloc((size_t)(n + 1), 1);
+    if (!index || !low || !next_arc || !call || !stack || !on_stack) {
+        free(index), free(low), free(next_arc), free(call), free(stack), free(on_stack);
+        return -2;
+    }
+    for (int64_t v = 0; v < n; ++v) {
+        index[v] = -1;
+    }
+    int64_t counter = 0, stack_top = 0, components = 0;
+    for (int64_t root = 0; root < n; ++root) {
+        if (index[root] >= 0) {
+            continue;
+        }
+        int64_t depth = 0;
+        call[depth++] = root;
+        index[root] = low[root] = counter++;
+        next_arc[root] = g->row_ptr[root];
+        stack[stack_top++] = root;
+        on_stack[root] = 1;
+        while (depth > 0) {
+            const int64_t v = call[depth - 1];
+            if (next_arc[v] < g->row_ptr[v + 1]) {
+                const int64_t e = next_arc[v]++;
+                const int64_t x = g->col[e];
+                if (g->w[e] == 0.0 || x == v) {
+                    continue; /* absent arc; self arcs join nothing */
+                }
+                if (index[x] < 0) {
+                    index[x] = low[x] = counter++;
+                    next_arc[x] = g->row_ptr[x];
+                    stack[stack_top++] = x;
+                    on_stack[x] = 1;
+                    call[depth++] = x;
+                } else if (on_stack[x] && index[x] < low[v]) {
+                    low[v] = index[x];
+                }
+                continue;
+            }
+            /* v is finished */
+            --depth;
+            if (low[v] == index[v]) {
+                int64_t top = stack_top, largest = -1;
+                do {
+                    const int64_t x = stack[--top];
+                    largest = x > largest ? x : largest;
+                } while (stack[top] != v);
+                for (int64_t i = top; i < stack_top; ++i) {
+                    comp[stack[i]] = (int32_t)largest;
+                    on_stack[stack[i]] = 0;
+                }
+                stack_top = top;
+                ++components;
+            }
+            if (depth > 0) {
+                const int64_t parent = call[depth - 1];
+                if (low[v] < low[parent]) {
+                    low[parent] = low[v];
+                }
+            }
+        }
+    }
+    free(index), free(low), free(next_arc), free(call), free(stack), free(on_stack);
+    return components;
+}

@@ -12,6 +12,7 @@
  *   APSP aggregation (R, CPL, efficiency)       source/metrics/paths/AllPairsShortestPath.h:110-163
  *   Brandes betweenness                         source/metrics/paths/BetweennessCentralityVariants/BrandesVariant.h:79-159
  *   distance histogram bin rule                 external/cpp-utility/data-structure/Histogram.hpp:143-180
+ *   strongly connected components (Tarjan)      source/metrics/connectivity/SccVariants/TarjanGatheredVariant.h:17-36
  * and adds the exactly rounded sums and the CPL / efficiency gradient that the reference does not have.
  *
  * Parity pin: on integer-weight graphs its distances, per-source summaries, APSP scalars and Brandes values are
@@ -87,6 +88,13 @@ int ngxo_brandes(const ngxo_graph* g, const int64_t* sources, int64_t k, double*
  * sources (NULL: all), normalised by R of those sources. dcpl, deff: m entries each, overwritten.
  */
 int ngxo_apsp_grad(const ngxo_graph* g, const int64_t* sources, int64_t k, double* dcpl, double* deff, ngxo_totals* totals);
+
+/*
+ * Strongly connected components by Tarjan's algorithm (iterative depth-first search; weights and self arcs ignored,
+ * zero-weight arcs absent). comp (n entries) receives each vertex's component, named by its largest vertex. Returns
+ * the number of components, or a negative error code.
+ */
+int64_t ngxo_scc(const ngxo_graph* g, int32_t* comp);
 
 #ifdef __cplusplus
 }

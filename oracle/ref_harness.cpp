@@ -25,12 +25,15 @@
 #include "metrics/paths/Dijkstra.h"
 #include "metrics/paths/BetweennessCentralityVariants/BrandesVariant.h"
 #include "metrics/paths/DiameterApproximation.h"
+#include "metrics/connectivity/StronglyConnectedComponents.h"
 #include "utility/RandomNumberGenerator.h"
 
 #include <mpi-wrapper/MPIWrapper.h>
 #include <mpi-wrapper/instrumentation/MPIProgress.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <stdexcept>
 #include <cstring>
 #include <exception>
 #include <functional>
@@ -320,6 +323,24 @@ int ngxref_diameter_approximation(void* handle, std::uint64_t r, const double* d
         } else {
             auto generator = DefaultRandomNumberGenerator{ seed };
             *out = DiameterApproximation::compute_approximation(graph, r, generator);
+        }
+    });
+}
+
+// StronglyConnectedComponents::compute_strongly_connected_components; sizes (n + 1 entries) receives component_sizes.
+int ngxref_scc(void* handle, int algorithm, std::uint64_t tail_threshold, std::uint64_t* number_components, std::uint64_t* largest, std::uint64_t* sizes,
+               std::int64_t capacity) {
+    return guarded([&] {
+        const auto& graph = static_cast<RefGraph*>(handle)->graph;
+        const auto result = StronglyConnectedComponents::compute_strongly_connected_components(graph, static_cast<SccAlgorithm>(algorithm), tail_threshold);
+        *number_components = result.number_components;
+        *largest = result.largest_component_size;
+        std::fill(sizes, sizes + capacity, std::uint64_t{ 0 });
+        for (const auto& [size, count] : result.component_sizes) {
+            if (static_cast<std::int64_t>(size) >= capacity) {
+                throw std::runtime_error("ngxref_scc: a component size beyond the output");
+            }
+            sizes[size] = count;
         }
     });
 }
