@@ -203,7 +203,7 @@ int ngx_batch_run(ngx_graph* g, const ngx_batch_opts* opts, ngx_apsp_result* res
     // graph table and sources (every vertex of every graph) for these options
     const std::vector<GraphDesc> descs = graph_table(g, opts->metric, opts->delta_scale);
     // every graph's sources in its locality order (per-source results are scattered back by vertex)
-    const std::vector<int32_t>& sources = g->source_order;
+    const auto& sources = g->source_order;
     NGX_CUDA_TRY(cudaMemcpyAsync(o.graphs, descs.data(), descs.size() * sizeof(GraphDesc), cudaMemcpyHostToDevice, g->stream));
     if (!sources.empty()) {
         NGX_CUDA_TRY(cudaMemcpyAsync(o.sources, sources.data(), sources.size() * 4, cudaMemcpyHostToDevice, g->stream));

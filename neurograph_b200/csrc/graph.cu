@@ -8,11 +8,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "ngx_common.cuh"
@@ -90,13 +93,16 @@ namespace {
 
 // Tiles of nearby sources: from each unassigned seed (in id order), the seed and its lightest unassigned out-neighbours,
 // then theirs (one hop at a time, lightest first, continuing from the 64 lightest), until a tile of 32 is full or the
-// search has looked at 256 vertices. Close sources reach most vertices at similar distances, so more of them are pending on a vertex when it is
-// expanded, and one pass over its arcs serves more of them. O(n * 256 * degree) at worst, on the host.
-void append_source_order(int64_t n, const int64_t* row_ptr, const Arc* arcs, std::vector<int32_t>& order) {
+// search has looked at 256 vertices. Close sources reach most vertices at similar distances, so more of them are
+// pending on a vertex when it is expanded, and one pass over its arcs serves more of them. Candidates are ordered by
+// (length, vertex), a strict order, and only the lightest ones a hop uses are selected and sorted: the unassigned ones
+// that fill the tile and, when the hop does not fill it, the 64 that continue the search. O(n * 256 * degree) at
+// worst, on the host.
+void append_source_order(int64_t n, const int64_t* row_ptr, const Arc* arcs, HostVector<int32_t>& order) {
     std::vector<uint8_t> assigned(static_cast<size_t>(n), 0);
     std::vector<int32_t> seen_stamp(static_cast<size_t>(n), -1);
     std::vector<int32_t> frontier, next;
-    std::vector<std::pair<double, int32_t>> cand;
+    std::vector<std::pair<double, int32_t>> cand, free_cand;
     int32_t stamp = 0;
     for (int64_t seed = 0; seed < n; ++seed) {
         if (assigned[static_cast<size_t>(seed)]) {
@@ -104,7 +110,7 @@ void append_source_order(int64_t n, const int64_t* row_ptr, const Arc* arcs, std
         }
         ++stamp;
         int taken = 0;
-        int looked = 1;
+        int64_t looked = 1;
         frontier.assign(1, static_cast<int32_t>(seed));
         seen_stamp[static_cast<size_t>(seed)] = stamp;
         assigned[static_cast<size_t>(seed)] = 1;
@@ -112,29 +118,38 @@ void append_source_order(int64_t n, const int64_t* row_ptr, const Arc* arcs, std
         ++taken;
         while (taken < kTile && !frontier.empty() && looked < 256) {
             cand.clear();
+            free_cand.clear();
             for (const int32_t u : frontier) {
                 for (int64_t e = row_ptr[u]; e < row_ptr[u + 1]; ++e) {
                     const int32_t v = arcs[e].col;
                     if (seen_stamp[static_cast<size_t>(v)] != stamp) {
                         seen_stamp[static_cast<size_t>(v)] = stamp;
                         cand.emplace_back(arcs[e].len, v);
+                        if (!assigned[static_cast<size_t>(v)]) {
+                            free_cand.emplace_back(arcs[e].len, v);
+                        }
                     }
                 }
             }
-            std::sort(cand.begin(), cand.end());
+            // the unassigned candidates, lightest first, fill the tile
+            const size_t need = static_cast<size_t>(kTile - taken);
+            const size_t take = std::min(need, free_cand.size());
+            std::partial_sort(free_cand.begin(), free_cand.begin() + static_cast<std::ptrdiff_t>(take), free_cand.end());
+            for (size_t i = 0; i < take; ++i) {
+                assigned[static_cast<size_t>(free_cand[i].second)] = 1;
+                order.push_back(free_cand[i].second);
+            }
+            taken += static_cast<int>(take);
+            if (taken == kTile) {
+                break;
+            }
+            // the hop looked at every candidate; the next one continues from the 64 lightest of them
+            looked += static_cast<int64_t>(cand.size());
+            const size_t keep = std::min<size_t>(64, cand.size());
+            std::partial_sort(cand.begin(), cand.begin() + static_cast<std::ptrdiff_t>(keep), cand.end());
             next.clear();
-            for (const auto& c : cand) {
-                ++looked;
-                if (next.size() < 64) {
-                    next.push_back(c.second);  // the next hop continues from the lightest candidates only
-                }
-                if (!assigned[static_cast<size_t>(c.second)]) {
-                    assigned[static_cast<size_t>(c.second)] = 1;
-                    order.push_back(c.second);
-                    if (++taken == kTile) {
-                        break;
-                    }
-                }
+            for (size_t i = 0; i < keep; ++i) {
+                next.push_back(cand[i].second);
             }
             frontier.swap(next);
         }
@@ -172,7 +187,8 @@ void release(ngx_graph* g) {
     delete g;
 }
 
-int validate(const ngx_csr* csr) {
+// Checks the sizes, pointers and row offsets of one CSR (the arcs are checked during the first pass over them).
+int validate_rows(const ngx_csr* csr) {
     if (csr == nullptr) {
         return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: csr is NULL");
     }
@@ -199,18 +215,352 @@ int validate(const ngx_csr* csr) {
             return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: row_ptr is not monotone at vertex " + std::to_string(u));
         }
     }
-    for (int64_t e = 0; e < csr->m; ++e) {
-        if (csr->col[e] < 0 || csr->col[e] >= csr->n) {
-            return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: arc " + std::to_string(e) + " has an out-of-range target");
-        }
-        if (!std::isfinite(csr->w[e])) {
-            return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: arc " + std::to_string(e) + " has a non-finite weight");
-        }
-    }
     return NGX_OK;
 }
 
+// Runs body(task) for every task in [0, tasks) on up to `threads` threads (the calling thread included).
+template <typename Body>
+void parallel_for(int64_t tasks, int threads, const Body& body) {
+    const int workers = static_cast<int>(std::min<int64_t>(tasks, threads));
+    if (workers <= 1) {
+        for (int64_t t = 0; t < tasks; ++t) {
+            body(t);
+        }
+        return;
+    }
+    std::atomic<int64_t> next{ 0 };
+    const auto run = [&] {
+        for (int64_t t = next.fetch_add(1); t < tasks; t = next.fetch_add(1)) {
+            body(t);
+        }
+    };
+    std::vector<std::thread> pool;
+    pool.reserve(static_cast<size_t>(workers - 1));
+    for (int i = 1; i < workers; ++i) {
+        pool.emplace_back(run);
+    }
+    run();
+    for (auto& worker : pool) {
+        worker.join();
+    }
+}
+
+// A vertex range of one graph, sized to about kChunkArcs caller arcs: the unit of the parallel passes over arcs.
+constexpr int64_t kChunkArcs = int64_t(1) << 20;
+struct Chunk {
+    int64_t graph = 0;
+    int64_t v0 = 0, v1 = 0;
+    int64_t bad_arc = -1;  // first arc with an out-of-range target or a non-finite weight
+    bool bad_target = false;
+    int64_t max_degree = 0;
+    double min_len = INFINITY, max_len = 0.0;
+};
+
 }  // namespace
+
+int build_host_graphs(const ngx_csr* csrs, int64_t count, int threads, HostGraphs* out) {
+    if (csrs == nullptr || count <= 0) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: no graphs");
+    }
+    if (threads <= 0) {
+        threads = static_cast<int>(std::min<unsigned>(32u, std::max(1u, std::thread::hardware_concurrency())));
+    }
+    HostGraphs& h = *out;
+    // rows of every graph first; the arcs of the graphs before the first bad one are checked by the first pass, so
+    // that the first error in graph order is the one reported
+    int64_t rows_ok = count;
+    int rows_rc = NGX_OK;
+    std::string rows_message;
+    int64_t n_total = 0, m_total = 0;
+    for (int64_t i = 0; i < count; ++i) {
+        if (const int rc = validate_rows(&csrs[i]); rc != NGX_OK) {
+            rows_ok = i;
+            rows_rc = rc;
+            rows_message = ngx_last_error();
+            break;
+        }
+        n_total += csrs[i].n;
+        m_total += csrs[i].m;
+    }
+    const auto graph_error = [&](int64_t i, int rc, const std::string& message) {
+        return count > 1 ? fail(rc, "graph " + std::to_string(i) + ": " + message) : fail(rc, message);
+    };
+    if (rows_ok == count && (n_total >= (int64_t(1) << 31) - 1 || m_total >= (int64_t(1) << 31) - 1)) {
+        return fail(NGX_UNSUPPORTED, "ngx_graph_create: total vertices and arcs must be below 2^31 - 1");
+    }
+    if (m_total < (int64_t(1) << 16)) {
+        threads = 1;  // not worth a thread
+    }
+    try {
+        // vertex and row offsets per graph
+        std::vector<int64_t> vertex_off(static_cast<size_t>(rows_ok) + 1, 0), row_off(static_cast<size_t>(rows_ok) + 1, 0),
+            user_off(static_cast<size_t>(rows_ok) + 1, 0);
+        for (int64_t i = 0; i < rows_ok; ++i) {
+            vertex_off[static_cast<size_t>(i) + 1] = vertex_off[static_cast<size_t>(i)] + csrs[i].n;
+            row_off[static_cast<size_t>(i) + 1] = row_off[static_cast<size_t>(i)] + csrs[i].n + 1;
+            user_off[static_cast<size_t>(i) + 1] = user_off[static_cast<size_t>(i)] + csrs[i].m;
+        }
+        std::vector<Chunk> chunks;
+        for (int64_t i = 0; i < rows_ok; ++i) {
+            const ngx_csr& c = csrs[i];
+            const int64_t pieces = std::max<int64_t>(1, std::min<int64_t>(c.n, (c.m + kChunkArcs - 1) / kChunkArcs));
+            int64_t v0 = 0;
+            for (int64_t p = 1; p <= pieces && c.n > 0; ++p) {
+                int64_t v1 = c.n;
+                if (p < pieces) {
+                    const int64_t target = p * c.m / pieces;
+                    v1 = std::max<int64_t>(v0, std::lower_bound(c.row_ptr, c.row_ptr + c.n, target) - c.row_ptr);
+                }
+                Chunk k;
+                k.graph = i;
+                k.v0 = v0;
+                k.v1 = v1;
+                chunks.push_back(k);
+                v0 = v1;
+            }
+        }
+        // pass 1: check the arcs, count the stored ones per vertex
+        std::vector<int64_t> kept(static_cast<size_t>(vertex_off.back()), 0);
+        parallel_for(static_cast<int64_t>(chunks.size()), threads, [&](int64_t t) {
+            Chunk& k = chunks[static_cast<size_t>(t)];
+            const ngx_csr& c = csrs[k.graph];
+            int64_t* kept_row = kept.data() + vertex_off[static_cast<size_t>(k.graph)];
+            for (int64_t u = k.v0; u < k.v1; ++u) {
+                int64_t stored = 0;
+                for (int64_t e = c.row_ptr[u]; e < c.row_ptr[u + 1]; ++e) {
+                    const int32_t v = c.col[e];
+                    const double w = c.w[e];
+                    if (k.bad_arc < 0 && (v < 0 || v >= c.n || !std::isfinite(w))) {
+                        k.bad_arc = e;
+                        k.bad_target = v < 0 || v >= c.n;
+                    }
+                    stored += w != 0.0 ? 1 : 0;
+                }
+                kept_row[u] = stored;
+                k.max_degree = std::max(k.max_degree, stored);
+            }
+        });
+        for (int64_t i = 0; i < rows_ok; ++i) {
+            int64_t bad = -1;
+            bool bad_target = false;
+            for (const Chunk& k : chunks) {
+                if (k.graph == i && k.bad_arc >= 0 && (bad < 0 || k.bad_arc < bad)) {
+                    bad = k.bad_arc;
+                    bad_target = k.bad_target;
+                }
+            }
+            if (bad >= 0) {
+                return graph_error(i, NGX_INVALID_ARGUMENT, "ngx_graph_create: arc " + std::to_string(bad) +
+                                                                (bad_target ? " has an out-of-range target" : " has a non-finite weight"));
+            }
+        }
+        if (rows_ok < count) {
+            return graph_error(rows_ok, rows_rc, rows_message);
+        }
+        // row offsets (global arc indices) and the parts
+        h.parts.assign(static_cast<size_t>(count), GraphPart{});
+        h.row_ptr.assign(static_cast<size_t>(row_off.back()), 0);
+        int64_t m = 0;
+        for (int64_t i = 0; i < count; ++i) {
+            GraphPart& part = h.parts[static_cast<size_t>(i)];
+            part.n = csrs[i].n;
+            part.m_user = csrs[i].m;
+            part.row_off = row_off[static_cast<size_t>(i)];
+            part.user_arc_off = user_off[static_cast<size_t>(i)];
+            part.vertex_off = vertex_off[static_cast<size_t>(i)];
+            int64_t* rows = h.row_ptr.data() + part.row_off;
+            const int64_t* kept_row = kept.data() + part.vertex_off;
+            rows[0] = m;
+            for (int64_t u = 0; u < part.n; ++u) {
+                m += kept_row[u];
+                rows[u + 1] = m;
+            }
+            part.m_stored = m - rows[0];
+            h.n_max = std::max(h.n_max, part.n);
+        }
+        kept = std::vector<int64_t>();
+        h.n_total = n_total;
+        h.m_user = m_total;
+        // pass 2: the stored arcs
+        h.regular.resize(static_cast<size_t>(m));
+        h.inverse.resize(static_cast<size_t>(m));
+        h.arc_src.resize(static_cast<size_t>(m));
+        h.stored_of_user.resize(static_cast<size_t>(m_total));  // every caller arc is written by its chunk
+        HostVector<int32_t> target(static_cast<size_t>(m));
+        parallel_for(static_cast<int64_t>(chunks.size()), threads, [&](int64_t t) {
+            Chunk& k = chunks[static_cast<size_t>(t)];
+            const ngx_csr& c = csrs[k.graph];
+            const GraphPart& part = h.parts[static_cast<size_t>(k.graph)];
+            int64_t pos = h.row_ptr[static_cast<size_t>(part.row_off + k.v0)];
+            for (int64_t u = k.v0; u < k.v1; ++u) {
+                for (int64_t e = c.row_ptr[u]; e < c.row_ptr[u + 1]; ++e) {
+                    const double a = std::fabs(c.w[e]);
+                    const int32_t id = static_cast<int32_t>(part.user_arc_off + e);
+                    if (a == 0.0) {
+                        h.stored_of_user[static_cast<size_t>(id)] = -1;
+                        continue;
+                    }
+                    const int32_t v = c.col[e];
+                    h.stored_of_user[static_cast<size_t>(id)] = static_cast<int32_t>(pos);
+                    h.regular[static_cast<size_t>(pos)] = Arc{ v, id, a };
+                    h.inverse[static_cast<size_t>(pos)] = Arc{ v, id, 1.0 / a };
+                    h.arc_src[static_cast<size_t>(pos)] = static_cast<int32_t>(u);
+                    target[static_cast<size_t>(pos)] = v;
+                    k.min_len = std::min(k.min_len, a);
+                    k.max_len = std::max(k.max_len, a);
+                    ++pos;
+                }
+            }
+        });
+        // The locality order needs only the forward arcs. A single graph's order is sequential (each tile depends on
+        // the ones before), so it runs on a thread of its own beside the remaining passes; a batch's graphs are
+        // ordered in parallel at the end.
+        std::vector<HostVector<int32_t>> orders(static_cast<size_t>(count));
+        const auto order_graph = [&](int64_t i) {
+            const GraphPart& part = h.parts[static_cast<size_t>(i)];
+            const int64_t first = h.row_ptr[static_cast<size_t>(part.row_off)];
+            std::vector<int64_t> local_rows(static_cast<size_t>(part.n) + 1);
+            for (int64_t v = 0; v <= part.n; ++v) {
+                local_rows[static_cast<size_t>(v)] = h.row_ptr[static_cast<size_t>(part.row_off + v)] - first;
+            }
+            orders[static_cast<size_t>(i)].reserve(static_cast<size_t>(part.n));
+            append_source_order(part.n, local_rows.data(), h.regular.data() + first, orders[static_cast<size_t>(i)]);
+        };
+        std::thread order_thread;
+        bool order_failed = false;
+        if (count == 1 && threads > 1) {
+            order_thread = std::thread([&] {
+                try {
+                    order_graph(0);
+                } catch (const std::bad_alloc&) {
+                    order_failed = true;
+                }
+            });
+            --threads;
+        }
+        // joins the order thread on every exit from here on
+        struct Joiner {
+            std::thread& t;
+            ~Joiner() {
+                if (t.joinable()) {
+                    t.join();
+                }
+            }
+        } joiner{ order_thread };
+        double min_regular = INFINITY, max_regular = 0.0;
+        for (const Chunk& k : chunks) {
+            h.max_out_degree = std::max(h.max_out_degree, k.max_degree);
+            min_regular = std::min(min_regular, k.min_len);
+            max_regular = std::max(max_regular, k.max_len);
+        }
+        // Two kinds of tasks run together: each graph's sums of lengths in arc order (the mean lengths; the graphs
+        // are then added in order, so the bits do not depend on the threads), and the in-degree counts of the
+        // reverse CSR, which is built by counting sort over targets, within a target in ascending stored order
+        // (= ascending source); a large graph's targets are split into ranges, each task scanning all its targets.
+        struct Range {
+            int64_t graph, t0, t1;
+        };
+        std::vector<Range> ranges;
+        for (int64_t i = 0; i < count; ++i) {
+            const GraphPart& part = h.parts[static_cast<size_t>(i)];
+            const int64_t pieces = part.m_stored >= (int64_t(1) << 21) ? std::min<int64_t>(threads, part.n) : 1;
+            for (int64_t r = 0; r < pieces; ++r) {
+                ranges.push_back(Range{ i, r * part.n / pieces, (r + 1) * part.n / pieces });
+            }
+        }
+        std::vector<double> part_regular(static_cast<size_t>(count), 0.0), part_inverse(static_cast<size_t>(count), 0.0);
+        std::vector<int64_t> cursor(static_cast<size_t>(n_total) + 1, 0);  // in-degree, then the next free slot
+        parallel_for(count + static_cast<int64_t>(ranges.size()), threads, [&](int64_t t) {
+            if (t < count) {
+                const GraphPart& part = h.parts[static_cast<size_t>(t)];
+                const int64_t first = h.row_ptr[static_cast<size_t>(part.row_off)];
+                double sr = 0.0, si = 0.0;
+                for (int64_t e = first; e < first + part.m_stored; ++e) {
+                    sr += h.regular[static_cast<size_t>(e)].len;
+                    si += h.inverse[static_cast<size_t>(e)].len;
+                }
+                part_regular[static_cast<size_t>(t)] = sr;
+                part_inverse[static_cast<size_t>(t)] = si;
+                return;
+            }
+            const Range& r = ranges[static_cast<size_t>(t - count)];
+            const GraphPart& part = h.parts[static_cast<size_t>(r.graph)];
+            const int64_t first = h.row_ptr[static_cast<size_t>(part.row_off)];
+            int64_t* degree = cursor.data() + part.vertex_off;
+            for (int64_t e = first; e < first + part.m_stored; ++e) {
+                const int32_t v = target[static_cast<size_t>(e)];
+                if (v >= r.t0 && v < r.t1) {
+                    ++degree[v];
+                }
+            }
+        });
+        double sum_regular = 0.0, sum_inverse = 0.0;
+        for (int64_t i = 0; i < count; ++i) {
+            GraphPart& part = h.parts[static_cast<size_t>(i)];
+            if (part.m_stored > 0) {
+                part.mean_len_regular = part_regular[static_cast<size_t>(i)] / static_cast<double>(part.m_stored);
+                part.mean_len_inverse = part_inverse[static_cast<size_t>(i)] / static_cast<double>(part.m_stored);
+            }
+            sum_regular += part_regular[static_cast<size_t>(i)];
+            sum_inverse += part_inverse[static_cast<size_t>(i)];
+        }
+        if (m > 0) {
+            h.mean_len_regular = sum_regular / static_cast<double>(m);
+            h.mean_len_inverse = sum_inverse / static_cast<double>(m);
+            h.min_len_regular = min_regular;
+            h.max_len_regular = max_regular;
+        }
+        h.rrow_ptr.assign(static_cast<size_t>(row_off.back()), 0);
+        for (int64_t i = 0; i < count; ++i) {
+            const GraphPart& part = h.parts[static_cast<size_t>(i)];
+            int64_t* rows = h.rrow_ptr.data() + part.row_off;
+            int64_t* slot = cursor.data() + part.vertex_off;
+            rows[0] = h.row_ptr[static_cast<size_t>(part.row_off)];
+            for (int64_t v = 0; v < part.n; ++v) {
+                rows[v + 1] = rows[v] + slot[v];
+                slot[v] = rows[v];
+            }
+        }
+        h.rarcs.resize(static_cast<size_t>(m));
+        parallel_for(static_cast<int64_t>(ranges.size()), threads, [&](int64_t t) {
+            const Range& r = ranges[static_cast<size_t>(t)];
+            const GraphPart& part = h.parts[static_cast<size_t>(r.graph)];
+            const int64_t first = h.row_ptr[static_cast<size_t>(part.row_off)];
+            int64_t* slot = cursor.data() + part.vertex_off;
+            for (int64_t e = first; e < first + part.m_stored; ++e) {
+                const int32_t v = target[static_cast<size_t>(e)];
+                if (v >= r.t0 && v < r.t1) {
+                    // the reverse record keeps the arc's index in the stored forward CSR (its caller index is regular[e].id)
+                    h.rarcs[static_cast<size_t>(slot[v]++)] = Arc{ h.arc_src[static_cast<size_t>(e)], static_cast<int32_t>(e), h.regular[static_cast<size_t>(e)].len };
+                }
+            }
+        });
+        target = HostVector<int32_t>();
+        cursor = std::vector<int64_t>();
+        if (order_thread.joinable()) {
+            order_thread.join();
+            if (order_failed) {
+                throw std::bad_alloc();
+            }
+        } else {
+            parallel_for(count, threads, order_graph);
+        }
+        if (count == 1) {
+            h.source_order = std::move(orders[0]);
+        } else {
+            h.source_order.clear();
+            h.source_order.reserve(static_cast<size_t>(n_total));
+            for (const auto& o : orders) {
+                h.source_order.insert(h.source_order.end(), o.begin(), o.end());
+            }
+        }
+    } catch (const std::bad_alloc&) {
+        return fail(NGX_OUT_OF_MEMORY, "ngx_graph_create: host allocation failed");
+    } catch (const std::system_error& e) {
+        return fail(NGX_OUT_OF_MEMORY, std::string("ngx_graph_create: cannot start host threads: ") + e.what());
+    }
+    return NGX_OK;
+}
 
 int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** out) {
     if (out == nullptr) {
@@ -220,16 +570,10 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
     if (csrs == nullptr || count <= 0) {
         return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: no graphs");
     }
-    int64_t n_total = 0, m_total = 0;
-    for (int64_t i = 0; i < count; ++i) {
-        if (const int rc = validate(&csrs[i]); rc != NGX_OK) {
-            return count > 1 ? fail(rc, "graph " + std::to_string(i) + ": " + ngx_last_error()) : rc;
-        }
-        n_total += csrs[i].n;
-        m_total += csrs[i].m;
-    }
-    if (n_total >= (int64_t(1) << 31) - 1 || m_total >= (int64_t(1) << 31) - 1) {
-        return fail(NGX_UNSUPPORTED, "ngx_graph_create: total vertices and arcs must be below 2^31 - 1");
+    // the input is checked (and laid out) before the device, so that a bad graph is reported as such anywhere
+    HostGraphs h;
+    if (const int rc = build_host_graphs(csrs, count, 0, &h); rc != NGX_OK) {
+        return rc;
     }
     int device_count = 0;
     NGX_CUDA_TRY(cudaGetDeviceCount(&device_count));
@@ -249,8 +593,18 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
     }
     g->device = device;
     g->sm_count = prop.multiProcessorCount;
-    g->n_total = n_total;
-    g->m_user = m_total;
+    g->n_total = h.n_total;
+    g->m_user = h.m_user;
+    g->n = h.n_max;
+    g->m_stored = static_cast<int64_t>(h.regular.size());
+    g->parts = std::move(h.parts);
+    g->stored_of_user = std::move(h.stored_of_user);
+    g->source_order = std::move(h.source_order);
+    g->max_out_degree = h.max_out_degree;
+    g->mean_len_regular = h.mean_len_regular;
+    g->mean_len_inverse = h.mean_len_inverse;
+    g->min_len_regular = h.min_len_regular;
+    g->max_len_regular = h.max_len_regular;
 
     const auto finish = [&](int rc) -> int {
         if (rc != NGX_OK) {
@@ -269,102 +623,8 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
     *g->h_abort = 0;
     g->stream = g->own_stream;
 
-    // Host compaction, graph after graph: drop zero-weight arcs, keep each arc's caller index (graphs numbered
-    // consecutively), precompute both metrics' lengths. Row offsets are global arc indices; targets stay graph-local.
-    std::vector<int64_t> row_ptr;
-    std::vector<int64_t> rrow_ptr;
-    std::vector<Arc> regular;
-    std::vector<Arc> inverse;
-    std::vector<int32_t> arc_src;
-    row_ptr.reserve(static_cast<size_t>(n_total + count));
-    rrow_ptr.reserve(static_cast<size_t>(n_total + count));
-    regular.reserve(static_cast<size_t>(m_total));
-    inverse.reserve(static_cast<size_t>(m_total));
-    std::vector<Arc> rarcs(static_cast<size_t>(m_total));
-    g->stored_of_user.assign(static_cast<size_t>(m_total), -1);
-    double sum_regular = 0.0, sum_inverse = 0.0;
-    double min_regular = INFINITY, max_regular = 0.0;
-    int64_t user_arc_off = 0, vertex_off = 0;
-    g->parts.resize(static_cast<size_t>(count));
-    for (int64_t gi = 0; gi < count; ++gi) {
-        const ngx_csr* csr = &csrs[gi];
-        const int64_t n = csr->n;
-        GraphPart& part = g->parts[static_cast<size_t>(gi)];
-        part.n = n;
-        part.m_user = csr->m;
-        part.row_off = static_cast<int64_t>(row_ptr.size());
-        part.user_arc_off = user_arc_off;
-        part.vertex_off = vertex_off;
-        const int64_t first_arc = static_cast<int64_t>(regular.size());
-        std::vector<int64_t> in_degree(static_cast<size_t>(n) + 1, 0);
-        double part_regular = 0.0, part_inverse = 0.0;
-        row_ptr.push_back(first_arc);
-        for (int64_t u = 0; u < n; ++u) {
-            for (int64_t e = csr->row_ptr[u]; e < csr->row_ptr[u + 1]; ++e) {
-                const double a = std::fabs(csr->w[e]);
-                if (a == 0.0) {
-                    continue;
-                }
-                const int32_t v = csr->col[e];
-                const int32_t id = static_cast<int32_t>(user_arc_off + e);
-                g->stored_of_user[static_cast<size_t>(id)] = static_cast<int32_t>(regular.size());
-                regular.push_back(Arc{ v, id, a });
-                arc_src.push_back(static_cast<int32_t>(u));
-                inverse.push_back(Arc{ v, id, 1.0 / a });
-                part_regular += a;
-                part_inverse += 1.0 / a;
-                min_regular = std::min(min_regular, a);
-                max_regular = std::max(max_regular, a);
-                in_degree[static_cast<size_t>(v) + 1] += 1;
-            }
-            row_ptr.push_back(static_cast<int64_t>(regular.size()));
-            g->max_out_degree = std::max(g->max_out_degree, row_ptr.back() - row_ptr[row_ptr.size() - 2]);
-        }
-        part.m_stored = static_cast<int64_t>(regular.size()) - first_arc;
-        if (part.m_stored > 0) {
-            part.mean_len_regular = part_regular / static_cast<double>(part.m_stored);
-            part.mean_len_inverse = part_inverse / static_cast<double>(part.m_stored);
-        }
-        sum_regular += part_regular;
-        sum_inverse += part_inverse;
-        // reverse CSR of this graph by counting sort over targets; within a target, ascending source order
-        const size_t rbase = rrow_ptr.size();
-        rrow_ptr.push_back(first_arc);
-        for (int64_t v = 0; v < n; ++v) {
-            rrow_ptr.push_back(rrow_ptr.back() + in_degree[static_cast<size_t>(v) + 1]);
-        }
-        std::vector<int64_t> fill(rrow_ptr.begin() + static_cast<std::ptrdiff_t>(rbase), rrow_ptr.end() - 1);
-        for (int64_t u = 0; u < n; ++u) {
-            for (int64_t e = row_ptr[static_cast<size_t>(part.row_off + u)]; e < row_ptr[static_cast<size_t>(part.row_off + u + 1)]; ++e) {
-                const Arc& a = regular[static_cast<size_t>(e)];
-                // the reverse record keeps the arc's index in the stored forward CSR (its caller index is arcs[e].id)
-                rarcs[static_cast<size_t>(fill[static_cast<size_t>(a.col)]++)] = Arc{ static_cast<int32_t>(u), static_cast<int32_t>(e), a.len };
-            }
-        }
-        // arcs of this graph's rows, with graph-local row offsets
-        {
-            std::vector<int64_t> local_rows(static_cast<size_t>(n) + 1);
-            for (int64_t v = 0; v <= n; ++v) {
-                local_rows[static_cast<size_t>(v)] = row_ptr[static_cast<size_t>(part.row_off + v)] - first_arc;
-            }
-            append_source_order(n, local_rows.data(), regular.data() + first_arc, g->source_order);
-        }
-        g->n = std::max(g->n, n);
-        user_arc_off += csr->m;
-        vertex_off += n;
-    }
-    const int64_t m = static_cast<int64_t>(regular.size());
-    rarcs.resize(static_cast<size_t>(m));
-    g->m_stored = m;
-    if (m > 0) {
-        g->mean_len_regular = sum_regular / static_cast<double>(m);
-        g->mean_len_inverse = sum_inverse / static_cast<double>(m);
-        g->min_len_regular = min_regular;
-        g->max_len_regular = max_regular;
-    }
-
     const auto upload = [&](auto** dst, const auto& src) -> int {
-        using T = std::remove_reference_t<decltype(src[0])>;
+        using T = std::remove_cv_t<std::remove_reference_t<decltype(src[0])>>;
         const size_t bytes = std::max<size_t>(1, src.size()) * sizeof(T);
         NGX_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(dst), bytes));
         if (!src.empty()) {
@@ -372,12 +632,12 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
         }
         return NGX_OK;
     };
-    int rc = upload(&g->d_row_ptr, row_ptr);
-    if (rc == NGX_OK) rc = upload(&g->d_arcs_regular, regular);
-    if (rc == NGX_OK) rc = upload(&g->d_arcs_inverse, inverse);
-    if (rc == NGX_OK) rc = upload(&g->d_rrow_ptr, rrow_ptr);
-    if (rc == NGX_OK) rc = upload(&g->d_rarcs, rarcs);
-    if (rc == NGX_OK) rc = upload(&g->d_arc_src, arc_src);
+    int rc = upload(&g->d_row_ptr, h.row_ptr);
+    if (rc == NGX_OK) rc = upload(&g->d_arcs_regular, h.regular);
+    if (rc == NGX_OK) rc = upload(&g->d_arcs_inverse, h.inverse);
+    if (rc == NGX_OK) rc = upload(&g->d_rrow_ptr, h.rrow_ptr);
+    if (rc == NGX_OK) rc = upload(&g->d_rarcs, h.rarcs);
+    if (rc == NGX_OK) rc = upload(&g->d_arc_src, h.arc_src);
     if (rc == NGX_OK) {
         const cudaError_t err = cudaStreamSynchronize(g->stream);
         if (err != cudaSuccess) {

@@ -4,11 +4,35 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "ngx_common.cuh"
 
 namespace ngx {
+// Allocator whose element construction without arguments leaves trivial types uninitialized: large host arrays that a
+// parallel pass fills completely are then first touched (and paged in) by the threads that fill them.
+template <typename T>
+struct DefaultInitAllocator : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = DefaultInitAllocator<U>;
+    };
+    using std::allocator<T>::allocator;
+    template <typename U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible_v<U>) {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U* p, Args&&... args) {
+        ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+    }
+};
+template <typename T>
+using HostVector = std::vector<T, DefaultInitAllocator<T>>;
+
 // Host view of one graph of a handle (a single-graph handle holds one; a batch handle holds many, concatenated).
 struct GraphPart {
     int64_t n = 0;
@@ -79,10 +103,10 @@ struct ngx_graph {
     // bucket width per size class (floor(log2 n)), as a multiple of each graph's mean arc length (ngx_batch_autotune)
     double class_scale[64] = {};
     // stored forward index of each caller arc (-1 for zero weights), for ngx_graph_update_weights
-    std::vector<int32_t> stored_of_user;
+    ngx::HostVector<int32_t> stored_of_user;
     // all-sources processing order of each graph (graph-local ids, graph after graph): clusters of nearby vertices,
     // so that the 32 sources of a tile reach most vertices in the same phases and share arc passes
-    std::vector<int32_t> source_order;
+    ngx::HostVector<int32_t> source_order;
 
     ngx::DeviceCsr csr(int metric) const {
         return ngx::DeviceCsr{ n, m_stored, d_row_ptr, metric == NGX_METRIC_INVERSE ? d_arcs_inverse : d_arcs_regular };
@@ -91,6 +115,31 @@ struct ngx_graph {
 };
 
 namespace ngx {
+
+// Host form of a handle's graphs, concatenated graph after graph, before the upload.
+struct HostGraphs {
+    std::vector<GraphPart> parts;
+    HostVector<int64_t> row_ptr;   // n + 1 global arc offsets per graph (graph i's at parts[i].row_off)
+    HostVector<int64_t> rrow_ptr;  // the same for the reverse CSR
+    HostVector<Arc> regular;       // stored arcs (zero weights dropped) with |w|, in caller order within each row
+    HostVector<Arc> inverse;       // the same arcs with 1/|w|
+    HostVector<Arc> rarcs;         // in-arcs per target, ascending source; col = source, id = stored forward index
+    HostVector<int32_t> arc_src;   // graph-local source of each stored arc
+    HostVector<int32_t> stored_of_user;  // stored index of each caller arc, -1 for zero weights
+    HostVector<int32_t> source_order;    // locality order of each graph, graph after graph
+    int64_t n_max = 0;
+    int64_t n_total = 0;
+    int64_t m_user = 0;
+    int64_t max_out_degree = 0;
+    double mean_len_regular = 1.0;
+    double mean_len_inverse = 1.0;
+    double min_len_regular = 1.0;
+    double max_len_regular = 1.0;
+};
+
+// Validates `count` CSRs and builds their host form on up to `threads` host threads (0: the machine's cores). No
+// CUDA calls. The result does not depend on the number of threads.
+int build_host_graphs(const ngx_csr* csrs, int64_t count, int threads, HostGraphs* out);
 
 // Validates and uploads `count` CSRs into one handle (concatenated device CSR + reverse CSR).
 int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** out);
