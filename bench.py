@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import argparse
 import contextlib
+import gc
 import json
 import math
 import os
@@ -49,6 +50,13 @@ WORKLOAD = {
 HIST_BINS = 1024
 SLOTS_PER_WAVE = 296  # 148 SMs x 2 resident CTAs
 DEFAULT_SOURCES_PER_STEP = SLOTS_PER_WAVE * 32
+
+
+def pause_gc():
+    """Collects now and pauses Python's cyclic garbage collector for a timed region (as timeit does): a full
+    collection over the interpreter's objects takes tens of milliseconds and would otherwise land in a random step."""
+    gc.collect()
+    gc.disable()
 
 
 def log(*a):
@@ -327,6 +335,7 @@ def run_uneven_batch(args, ngx, torch, rank, world, barrier, max_over_ranks, sum
     for _ in range(args.warmup):
         b.run(**run)
     clocks = ClockSampler(local_rank)
+    pause_gc()
     clocks.start()
     clocks.wait_first_sample()
     barrier()
@@ -340,6 +349,7 @@ def run_uneven_batch(args, ngx, torch, rank, world, barrier, max_over_ranks, sum
     ev1.record(stream)
     barrier()
     clock_info = clocks.stop()
+    gc.enable()
     elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     value = sum_over_ranks(float(arcs)) / elapsed / 1e9
     reached = 0
@@ -356,11 +366,13 @@ def run_uneven_batch(args, ngx, torch, rank, world, barrier, max_over_ranks, sum
                    torch.from_numpy(w).pin_memory().numpy()) for n, rp, c, w in graphs]
         h2d = sum(rp.nbytes + c.nbytes + w.nbytes for _, rp, c, w in pinned)
         barrier()
+        pause_gc()
         t1 = time.perf_counter()
         with ngx.Batch(pinned, device=local_rank) as be:
             res, extra = be.run(task="brandes", hist_bins=HIST_BINS, hist_max=UNEVEN_BATCH["hist_max"])
         barrier()
         e2e_elapsed = max_over_ranks(time.perf_counter() - t1)
+        gc.enable()
         d2h = sum(x.nbytes for x in extra) + sum(r.hist.nbytes for r in res)
         e2e = {"value": sum_over_ranks(float(sum(r.traversed_arcs for r in res))) / e2e_elapsed / 1e9, "unit": "GTEPS",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
@@ -415,6 +427,7 @@ def run_scc(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ran
     for _ in range(args.warmup):
         first = g.scc()
     clocks = ClockSampler(local_rank)
+    pause_gc()
     clocks.start()
     clocks.wait_first_sample()
     barrier()
@@ -425,6 +438,7 @@ def run_scc(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ran
     ev1.record(stream)
     barrier()
     clock_info = clocks.stop()
+    gc.enable()
     elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
     arcs = int(c.m)
     value = sum_over_ranks(float(arcs * args.steps)) / elapsed / 1e9
@@ -439,11 +453,13 @@ def run_scc(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ran
     if not args.no_e2e:
         pinned = [torch.from_numpy(x).pin_memory().numpy() for x in (c.row_ptr, c.col, c.w)]
         barrier()
+        pause_gc()
         t1 = time.perf_counter()
         with ngx.Graph(c.n, *pinned, device=local_rank) as ge:
             res = ge.scc()
         barrier()
         e2e_elapsed = max_over_ranks(time.perf_counter() - t1)
+        gc.enable()
         e2e = {"value": sum_over_ranks(float(arcs)) / e2e_elapsed / 1e9, "unit": "G arcs/s",
                "h2d_bytes_per_step": int(sum(x.nbytes for x in pinned)), "d2h_bytes_per_step": int(res["component"].nbytes + 8 * (c.n + 3)),
                "timing": "wall clock, synchronized; graph handle created from pinned host CSR arrays, one ngx_scc call, "
@@ -565,6 +581,7 @@ def main():
         r, _ = step(g, batches[i], hist_max)
         hist_max = r.hist_max if r.hist_max > 0 else hist_max
     clocks = ClockSampler(local_rank)
+    pause_gc()
     clocks.start()
     clocks.wait_first_sample()
     barrier()
@@ -592,6 +609,7 @@ def main():
     ev1.record(stream)
     barrier()
     clock_info = clocks.stop()
+    gc.enable()
     elapsed = ev0.elapsed_time(ev1) / 1e3
     prev = ev0
     for k, (e, kms) in enumerate(zip(step_events, step_kernel_ms)):
@@ -635,6 +653,7 @@ def main():
         h2d = graph_bytes / args.steps + batches[0].nbytes
         d2h = 0
         barrier()
+        pause_gc()
         t1 = time.perf_counter()
         e2e_arcs = 0
         with ngx.Graph(c.n, pinned["row_ptr"], pinned["col"], pinned["w"], device=local_rank) as ge:
@@ -645,6 +664,7 @@ def main():
                     sum(a.nbytes for a in (r.per_source or {}).values())
         barrier()
         e2e_elapsed = max_over_ranks(time.perf_counter() - t1)
+        gc.enable()
         e2e = {"value": sum_over_ranks(float(e2e_arcs)) / e2e_elapsed / 1e9, "unit": "GTEPS", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
                "timing": f"wall clock, synchronized; graph created from the pinned host CSR once for the {args.steps}-step job, "
