@@ -12,6 +12,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <exception>
+#include <mutex>
 #include <new>
 #include <string>
 #include <system_error>
@@ -218,7 +220,9 @@ int validate_rows(const ngx_csr* csr) {
     return NGX_OK;
 }
 
-// Runs body(task) for every task in [0, tasks) on up to `threads` threads (the calling thread included).
+// Runs body(task) for every task in [0, tasks) on up to `threads` threads (the calling thread included). A thread that
+// cannot be started leaves its share to the others; the first exception a task throws is rethrown here once every
+// thread has stopped (the remaining tasks are skipped).
 template <typename Body>
 void parallel_for(int64_t tasks, int threads, const Body& body) {
     const int workers = static_cast<int>(std::min<int64_t>(tasks, threads));
@@ -229,19 +233,36 @@ void parallel_for(int64_t tasks, int threads, const Body& body) {
         return;
     }
     std::atomic<int64_t> next{ 0 };
+    std::exception_ptr failure;
+    std::mutex failure_lock;
     const auto run = [&] {
         for (int64_t t = next.fetch_add(1); t < tasks; t = next.fetch_add(1)) {
-            body(t);
+            try {
+                body(t);
+            } catch (...) {
+                const std::lock_guard<std::mutex> hold(failure_lock);
+                if (!failure) {
+                    failure = std::current_exception();
+                }
+                next.store(tasks);
+            }
         }
     };
     std::vector<std::thread> pool;
     pool.reserve(static_cast<size_t>(workers - 1));
     for (int i = 1; i < workers; ++i) {
-        pool.emplace_back(run);
+        try {
+            pool.emplace_back(run);
+        } catch (const std::system_error&) {
+            break;  // fewer threads
+        }
     }
     run();
     for (auto& worker : pool) {
         worker.join();
+    }
+    if (failure) {
+        std::rethrow_exception(failure);
     }
 }
 
@@ -427,16 +448,20 @@ int build_host_graphs(const ngx_csr* csrs, int64_t count, int threads, HostGraph
             append_source_order(part.n, local_rows.data(), h.regular.data() + first, orders[static_cast<size_t>(i)]);
         };
         std::thread order_thread;
-        bool order_failed = false;
+        std::exception_ptr order_failure;
         if (count == 1 && threads > 1) {
-            order_thread = std::thread([&] {
-                try {
-                    order_graph(0);
-                } catch (const std::bad_alloc&) {
-                    order_failed = true;
-                }
-            });
-            --threads;
+            try {
+                order_thread = std::thread([&] {
+                    try {
+                        order_graph(0);
+                    } catch (...) {
+                        order_failure = std::current_exception();
+                    }
+                });
+                --threads;
+            } catch (const std::system_error&) {
+                // no thread for it: ordered at the end like a batch's graphs
+            }
         }
         // joins the order thread on every exit from here on
         struct Joiner {
@@ -539,8 +564,8 @@ int build_host_graphs(const ngx_csr* csrs, int64_t count, int threads, HostGraph
         cursor = std::vector<int64_t>();
         if (order_thread.joinable()) {
             order_thread.join();
-            if (order_failed) {
-                throw std::bad_alloc();
+            if (order_failure) {
+                std::rethrow_exception(order_failure);
             }
         } else {
             parallel_for(count, threads, order_graph);
@@ -556,8 +581,8 @@ int build_host_graphs(const ngx_csr* csrs, int64_t count, int threads, HostGraph
         }
     } catch (const std::bad_alloc&) {
         return fail(NGX_OUT_OF_MEMORY, "ngx_graph_create: host allocation failed");
-    } catch (const std::system_error& e) {
-        return fail(NGX_OUT_OF_MEMORY, std::string("ngx_graph_create: cannot start host threads: ") + e.what());
+    } catch (const std::exception& e) {
+        return fail(NGX_OUT_OF_MEMORY, std::string("ngx_graph_create: host build failed: ") + e.what());
     }
     return NGX_OK;
 }
