@@ -119,374 +119,382 @@ using namespace ngx;
 extern "C" {
 
 int ngx_batch_create(const ngx_csr* graphs, int64_t count, int device, ngx_graph** out) {
-    const int rc = create_graphs(graphs, count, device, out);
-    if (rc != NGX_OK) {
-        return rc;
-    }
-    const int rc2 = build_items(*out);
-    if (rc2 != NGX_OK) {
-        ngx_graph_destroy(*out);
-        *out = nullptr;
-    }
-    return rc2;
+    return guard_host("ngx_batch_create", [&]() -> int {
+        const int rc = create_graphs(graphs, count, device, out);
+        if (rc != NGX_OK) {
+            return rc;
+        }
+        const int rc2 = build_items(*out);
+        if (rc2 != NGX_OK) {
+            ngx_graph_destroy(*out);
+            *out = nullptr;
+        }
+        return rc2;
+    });
 }
 
 int ngx_batch_run(ngx_graph* g, const ngx_batch_opts* opts, ngx_apsp_result* results, double* bc, double* dcpl, double* deff) {
-    if (g == nullptr || opts == nullptr || results == nullptr) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_batch_run: batch, opts or results is NULL");
-    }
-    const int mode = task_mode(opts->task);
-    if (mode < 0) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_batch_run: unknown task");
-    }
-    if (mode != kModeApsp && opts->metric != NGX_METRIC_REGULAR) {
-        return fail(NGX_UNSUPPORTED, "ngx_batch_run: betweenness and the gradient are defined for the regular metric");
-    }
-    if (opts->hist_bins < 0 || opts->hist_bins > kMaxHistBins || (opts->hist_bins > 0 && !(opts->hist_max > 0.0))) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_batch_run: hist_bins must be in [0, 16384] with hist_max > 0");
-    }
-    if (g->d_items == nullptr) {
-        if (const int rc = build_items(g); rc != NGX_OK) {
-            return rc;
+    return guard_host("ngx_batch_run", [&]() -> int {
+        if (g == nullptr || opts == nullptr || results == nullptr) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_batch_run: batch, opts or results is NULL");
         }
-    }
-    NGX_CUDA_TRY(cudaSetDevice(g->device));
-    *g->h_abort = 0;
-    ngx_apsp_opts aopts{};
-    aopts.metric = opts->metric;
-    aopts.mode = NGX_MODE_BATCHED;
-    aopts.block_threads = opts->block_threads;
-    aopts.max_iterations = opts->max_iterations;
-    if (const int rc = check_opts(g, &aopts); rc != NGX_OK) {
-        return rc;
-    }
-    const int64_t count = static_cast<int64_t>(g->parts.size());
-    const int64_t hist_bins = opts->hist_bins;
-    const double hist_max = opts->hist_max;
-
-    // persistent outputs: the run's block, then the betweenness / gradient fixed-point sums and the sigma flag
-    const size_t n_total = static_cast<size_t>(g->n_total);
-    const size_t m_total = static_cast<size_t>(g->m_user);
-    const size_t dag_words = 1 + (mode == kModeBrandes ? 2 * n_total : 0) + (mode == kModeGrad ? 4 * m_total : 0);
-    RunOutputs o;
-    if (const int rc = alloc_outputs(g, count, g->n_total, hist_bins, false, o, true); rc != NGX_OK) {
-        return rc;
-    }
-    const size_t run_bytes = (o.bytes + 255) & ~size_t(255);
-    if (run_bytes + dag_words * 8 > g->persistent_bytes) {
-        NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        if (g->graph_exec != nullptr) {
-            cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g->graph_exec));
-            g->graph_exec = nullptr;
-            g->graph_key = 0;
+        const int mode = task_mode(opts->task);
+        if (mode < 0) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_batch_run: unknown task");
         }
-        cudaFree(g->d_persistent);
-        g->d_persistent = nullptr;
-        g->persistent_bytes = 0;
-        NGX_CUDA_TRY(cudaMalloc(&g->d_persistent, run_bytes + dag_words * 8));
-        g->persistent_bytes = run_bytes + dag_words * 8;
-        if (const int rc = alloc_outputs(g, count, g->n_total, hist_bins, false, o, true); rc != NGX_OK) {
-            return rc;
+        if (mode != kModeApsp && opts->metric != NGX_METRIC_REGULAR) {
+            return fail(NGX_UNSUPPORTED, "ngx_batch_run: betweenness and the gradient are defined for the regular metric");
         }
-    }
-    auto* dag_block = reinterpret_cast<unsigned long long*>(static_cast<char*>(g->d_persistent) + run_bytes);
-    DagOutputs extra;
-    extra.sigma_inexact = reinterpret_cast<int*>(dag_block);
-    if (mode == kModeBrandes) {
-        extra.bc = dag_block + 1;
-    }
-    if (mode == kModeGrad) {
-        extra.grad_cpl = dag_block + 1;
-        extra.grad_eff = dag_block + 1 + 2 * m_total;
-    }
-
-    // graph table and sources (every vertex of every graph) for these options
-    const std::vector<GraphDesc> descs = graph_table(g, opts->metric, opts->delta_scale);
-    // every graph's sources in its locality order (per-source results are scattered back by vertex)
-    const auto& sources = g->source_order;
-    NGX_CUDA_TRY(cudaMemcpyAsync(o.graphs, descs.data(), descs.size() * sizeof(GraphDesc), cudaMemcpyHostToDevice, g->stream));
-    if (!sources.empty()) {
-        NGX_CUDA_TRY(cudaMemcpyAsync(o.sources, sources.data(), sources.size() * 4, cudaMemcpyHostToDevice, g->stream));
-    }
-    NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    TileJob job;
-    job.num_graphs = count;
-    job.num_items = g->num_items;
-    job.d_items = static_cast<const WorkItem*>(g->d_items);
-    job.num_sources = g->n_total;
-    job.n_max = g->n;
-    job.plain_delta = 1.0;
-
-    const uint64_t key = options_key(opts, g);
-    cudaEvent_t start, stop;
-    NGX_CUDA_TRY(cudaEventCreate(&start));
-    NGX_CUDA_TRY(cudaEventCreate(&stop));
-    int rc = NGX_OK;
-    cudaEventRecord(start, g->stream);
-    if (opts->use_cuda_graph && g->graph_exec != nullptr && g->graph_key == key) {
-        const cudaError_t err = cudaGraphLaunch(static_cast<cudaGraphExec_t>(g->graph_exec), g->stream);
-        rc = err == cudaSuccess ? NGX_OK : cuda_fail(err, "replaying the captured batch run");
-    } else {
-        rc = enqueue_run(g, aopts, mode, job, hist_bins, hist_max, o, &extra, dag_block, dag_words * 8);
-    }
-    cudaEventRecord(stop, g->stream);
-    cudaError_t err = cudaEventSynchronize(stop);
-    float ms = 0.0f;
-    if (err == cudaSuccess) {
-        cudaEventElapsedTime(&ms, start, stop);
-    } else if (rc == NGX_OK) {
-        rc = cuda_fail(err, "batch run");
-    }
-    cudaEventDestroy(start);
-    cudaEventDestroy(stop);
-    if (rc == NGX_OK) {
-        int code = 0;
-        NGX_CUDA_TRY(cudaMemcpy(&code, o.error, sizeof(int), cudaMemcpyDeviceToHost));
-        rc = device_error_status(code);
-    }
-    int inexact = 0;
-    if (rc == NGX_OK && mode != kModeApsp) {
-        NGX_CUDA_TRY(cudaMemcpy(&inexact, extra.sigma_inexact, sizeof(int), cudaMemcpyDeviceToHost));
-        if (inexact != 0) {
-            // some path count reached 2^53: rerun with the order-defined pull form for sigma (not captured)
-            extra.sigma_pull = 1;
-            rc = enqueue_run(g, aopts, mode, job, hist_bins, hist_max, o, &extra, dag_block, dag_words * 8);
-            if (rc == NGX_OK) {
-                err = cudaStreamSynchronize(g->stream);
-                rc = err == cudaSuccess ? NGX_OK : cuda_fail(err, "batch rerun");
-            }
-            extra.sigma_pull = 0;
+        if (opts->hist_bins < 0 || opts->hist_bins > kMaxHistBins || (opts->hist_bins > 0 && !(opts->hist_max > 0.0))) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_batch_run: hist_bins must be in [0, 16384] with hist_max > 0");
         }
-    }
-    // capture the run for later replays (after a plain run has sized the workspace; nothing executes here)
-    if (rc == NGX_OK && opts->use_cuda_graph && inexact == 0 && (g->graph_exec == nullptr || g->graph_key != key)) {
-        if (g->graph_exec != nullptr) {
-            cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g->graph_exec));
-            g->graph_exec = nullptr;
-            g->graph_key = 0;
-        }
-        // The workspace was sized by the run above, so the capture allocates nothing. A capture that fails anyway
-        // leaves the handle without a graph; the results of the run above stand and later calls launch normally.
-        cudaGraph_t graph = nullptr;
-        if (cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-            const int crc = enqueue_run(g, aopts, mode, job, hist_bins, hist_max, o, &extra, dag_block, dag_words * 8);
-            const cudaError_t cerr = cudaStreamEndCapture(g->stream, &graph);
-            cudaGraphExec_t exec = nullptr;
-            if (crc == NGX_OK && cerr == cudaSuccess && graph != nullptr && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
-                g->graph_exec = exec;
-                g->graph_key = key;
-            }
-            if (graph != nullptr) {
-                cudaGraphDestroy(graph);
-            }
-        }
-        cudaGetLastError();
-        set_last_error("");
-    }
-    if (rc != NGX_OK) {
-        return rc;
-    }
-
-    // per-graph results
-    std::vector<unsigned long long> acc, counters;
-    if ((rc = read_totals(g, o, acc, counters)) != NGX_OK) {
-        return rc;
-    }
-    for (int64_t gi = 0; gi < count; ++gi) {
-        ngx_apsp_result* r = &results[gi];
-        clear_result_totals(r);
-        const GraphPart& part = g->parts[static_cast<size_t>(gi)];
-        if ((rc = collect_graph(g, o, acc.data(), counters.data(), gi, part.vertex_off, part.n, hist_bins, hist_max, r,
-                                g->source_order.data() + part.vertex_off)) != NGX_OK) {
-            return rc;
-        }
-        r->kernel_ms = ms;
-    }
-    if (mode == kModeBrandes && bc != nullptr) {
-        std::vector<unsigned long long> fixed(2 * n_total);
-        NGX_CUDA_TRY(cudaMemcpyAsync(fixed.data(), extra.bc, fixed.size() * 8, cudaMemcpyDeviceToHost, g->stream));
-        NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        for (size_t v = 0; v < n_total; ++v) {
-            bc[v] = fixed_value(fixed[2 * v], fixed[2 * v + 1]);
-        }
-    }
-    if (mode == kModeGrad && (dcpl != nullptr || deff != nullptr)) {
-        std::vector<unsigned long long> fixed(4 * m_total);
-        NGX_CUDA_TRY(cudaMemcpyAsync(fixed.data(), extra.grad_cpl, fixed.size() * 8, cudaMemcpyDeviceToHost, g->stream));
-        NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        for (int64_t gi = 0; gi < count; ++gi) {
-            const GraphPart& part = g->parts[static_cast<size_t>(gi)];
-            const double r = static_cast<double>(results[gi].reached_pairs);
-            for (int64_t e = 0; e < part.m_user; ++e) {
-                const size_t i = static_cast<size_t>(part.user_arc_off + e);
-                if (dcpl != nullptr) dcpl[i] = fixed_value(fixed[2 * i], fixed[2 * i + 1]) / r;
-                if (deff != nullptr) deff[i] = -fixed_value(fixed[2 * m_total + 2 * i], fixed[2 * m_total + 2 * i + 1]) / r;
-            }
-        }
-    }
-    NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    return NGX_OK;
-}
-
-int ngx_batch_autotune(ngx_graph* g, int task, double* class_scales) {
-    if (g == nullptr) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_batch_autotune: batch is NULL");
-    }
-    const int mode = task_mode(task);
-    if (mode < 0) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_batch_autotune: unknown task");
-    }
-    NGX_CUDA_TRY(cudaSetDevice(g->device));
-    *g->h_abort = 0;
-    static const double kScales[] = { 0.125, 0.25, 0.5, 1.0, 2.0, 4.0 };
-    ngx_apsp_opts aopts{};
-    aopts.metric = NGX_METRIC_REGULAR;
-    aopts.mode = NGX_MODE_BATCHED;
-    for (int c = 0; c < NGX_SIZE_CLASSES; ++c) {
-        std::vector<int32_t> members;
-        for (size_t i = 0; i < g->parts.size(); ++i) {
-            if (size_class(g->parts[i].n) == c && g->parts[i].n > 0) {
-                members.push_back(static_cast<int32_t>(i));
-            }
-        }
-        if (class_scales != nullptr) {
-            class_scales[c] = 0.0;
-        }
-        if (members.empty()) {
-            continue;
-        }
-        std::sort(members.begin(), members.end(), [&](int32_t a, int32_t b) { return g->parts[static_cast<size_t>(a)].n < g->parts[static_cast<size_t>(b)].n; });
-        const int32_t gi = members[members.size() / 2];
-        const GraphPart& part = g->parts[static_cast<size_t>(gi)];
-        // one wave of the graph's source tiles (at most 2 x SMs tiles)
-        const int64_t tiles = std::min<int64_t>((part.n + kTile - 1) / kTile, 2 * g->sm_count);
-        std::vector<WorkItem> items(static_cast<size_t>(tiles));
-        for (int64_t t = 0; t < tiles; ++t) {
-            items[static_cast<size_t>(t)] = WorkItem{ 0, static_cast<int32_t>(t) };
-        }
-        // the graph's sources in the order a run takes them
-        const std::vector<int32_t> sources(g->source_order.begin() + part.vertex_off, g->source_order.begin() + part.vertex_off + part.n);
-        WorkItem* d_items = nullptr;
-        NGX_CUDA_TRY(cudaMalloc(&d_items, items.size() * sizeof(WorkItem)));
-        NGX_CUDA_TRY(cudaMemcpy(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
-        double best_rate = -1.0, best_scale = 1.0;
-        for (const double scale : kScales) {
-            RunOutputs o;
-            int rc = alloc_outputs(g, 1, part.n, 0, false, o, false);
-            DagOutputs extra;
-            unsigned long long* dag = nullptr;
-            const size_t dag_words = 1 + (mode == kModeBrandes ? 2 * static_cast<size_t>(g->n_total) : 0) +
-                                     (mode == kModeGrad ? 4 * static_cast<size_t>(g->m_user) : 0);
-            if (rc == NGX_OK && mode != kModeApsp) {
-                rc = grow_buffer(g, &g->d_call_dag, &g->call_dag_bytes, dag_words * 8);
-                if (rc == NGX_OK) {
-                    dag = static_cast<unsigned long long*>(g->d_call_dag);
-                    cudaMemsetAsync(dag, 0, dag_words * 8, g->stream);
-                    extra.sigma_inexact = reinterpret_cast<int*>(dag);
-                    if (mode == kModeBrandes) extra.bc = dag + 1;
-                    if (mode == kModeGrad) {
-                        extra.grad_cpl = dag + 1;
-                        extra.grad_eff = dag + 1 + 2 * static_cast<size_t>(g->m_user);
-                    }
-                }
-            }
-            if (rc == NGX_OK) {
-                const GraphDesc desc{ part.n, part.m_stored, part.row_off, 0, part.n, part.vertex_off, pick_delta(part.mean_len_regular, 0.0, scale) };
-                cudaMemsetAsync(o.block, 0, o.zeroed_bytes, g->stream);
-                cudaMemcpyAsync(o.graphs, &desc, sizeof(desc), cudaMemcpyHostToDevice, g->stream);
-                cudaMemcpyAsync(o.sources, sources.data(), sources.size() * 4, cudaMemcpyHostToDevice, g->stream);
-                TileJob job;
-                job.num_graphs = 1;
-                job.num_items = tiles;
-                job.d_items = d_items;
-                job.num_sources = part.n;
-                job.n_max = g->n;
-                float ms = 0.0f;
-                rc = launch_tiles(g, &aopts, mode, job, 0, 0.0, o, mode != kModeApsp ? &extra : nullptr, &ms, true);
-                if (rc == NGX_OK) {
-                    std::vector<unsigned long long> acc, counters;
-                    rc = read_totals(g, o, acc, counters);
-                    if (rc == NGX_OK && ms > 0.0f) {
-                        const double rate = static_cast<double>(counters[kTraversedArcs]) / ms;
-                        if (rate > best_rate) {
-                            best_rate = rate;
-                            best_scale = scale;
-                        }
-                    }
-                }
-            }
-            free_outputs(g, o);
-            cudaStreamSynchronize(g->stream);
-            if (rc != NGX_OK) {
-                cudaFree(d_items);
+        if (g->d_items == nullptr) {
+            if (const int rc = build_items(g); rc != NGX_OK) {
                 return rc;
             }
         }
-        cudaFree(d_items);
-        g->class_scale[c] = best_scale;
-        if (class_scales != nullptr) {
-            class_scales[c] = best_scale;
+        NGX_CUDA_TRY(cudaSetDevice(g->device));
+        *g->h_abort = 0;
+        ngx_apsp_opts aopts{};
+        aopts.metric = opts->metric;
+        aopts.mode = NGX_MODE_BATCHED;
+        aopts.block_threads = opts->block_threads;
+        aopts.max_iterations = opts->max_iterations;
+        if (const int rc = check_opts(g, &aopts); rc != NGX_OK) {
+            return rc;
         }
-    }
-    return NGX_OK;
+        const int64_t count = static_cast<int64_t>(g->parts.size());
+        const int64_t hist_bins = opts->hist_bins;
+        const double hist_max = opts->hist_max;
+
+        // persistent outputs: the run's block, then the betweenness / gradient fixed-point sums and the sigma flag
+        const size_t n_total = static_cast<size_t>(g->n_total);
+        const size_t m_total = static_cast<size_t>(g->m_user);
+        const size_t dag_words = 1 + (mode == kModeBrandes ? 2 * n_total : 0) + (mode == kModeGrad ? 4 * m_total : 0);
+        RunOutputs o;
+        if (const int rc = alloc_outputs(g, count, g->n_total, hist_bins, false, o, true); rc != NGX_OK) {
+            return rc;
+        }
+        const size_t run_bytes = (o.bytes + 255) & ~size_t(255);
+        if (run_bytes + dag_words * 8 > g->persistent_bytes) {
+            NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            if (g->graph_exec != nullptr) {
+                cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g->graph_exec));
+                g->graph_exec = nullptr;
+                g->graph_key = 0;
+            }
+            cudaFree(g->d_persistent);
+            g->d_persistent = nullptr;
+            g->persistent_bytes = 0;
+            NGX_CUDA_TRY(cudaMalloc(&g->d_persistent, run_bytes + dag_words * 8));
+            g->persistent_bytes = run_bytes + dag_words * 8;
+            if (const int rc = alloc_outputs(g, count, g->n_total, hist_bins, false, o, true); rc != NGX_OK) {
+                return rc;
+            }
+        }
+        auto* dag_block = reinterpret_cast<unsigned long long*>(static_cast<char*>(g->d_persistent) + run_bytes);
+        DagOutputs extra;
+        extra.sigma_inexact = reinterpret_cast<int*>(dag_block);
+        if (mode == kModeBrandes) {
+            extra.bc = dag_block + 1;
+        }
+        if (mode == kModeGrad) {
+            extra.grad_cpl = dag_block + 1;
+            extra.grad_eff = dag_block + 1 + 2 * m_total;
+        }
+
+        // graph table and sources (every vertex of every graph) for these options
+        const std::vector<GraphDesc> descs = graph_table(g, opts->metric, opts->delta_scale);
+        // every graph's sources in its locality order (per-source results are scattered back by vertex)
+        const auto& sources = g->source_order;
+        NGX_CUDA_TRY(cudaMemcpyAsync(o.graphs, descs.data(), descs.size() * sizeof(GraphDesc), cudaMemcpyHostToDevice, g->stream));
+        if (!sources.empty()) {
+            NGX_CUDA_TRY(cudaMemcpyAsync(o.sources, sources.data(), sources.size() * 4, cudaMemcpyHostToDevice, g->stream));
+        }
+        NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        TileJob job;
+        job.num_graphs = count;
+        job.num_items = g->num_items;
+        job.d_items = static_cast<const WorkItem*>(g->d_items);
+        job.num_sources = g->n_total;
+        job.n_max = g->n;
+        job.plain_delta = 1.0;
+
+        const uint64_t key = options_key(opts, g);
+        cudaEvent_t start, stop;
+        NGX_CUDA_TRY(cudaEventCreate(&start));
+        NGX_CUDA_TRY(cudaEventCreate(&stop));
+        int rc = NGX_OK;
+        cudaEventRecord(start, g->stream);
+        if (opts->use_cuda_graph && g->graph_exec != nullptr && g->graph_key == key) {
+            const cudaError_t err = cudaGraphLaunch(static_cast<cudaGraphExec_t>(g->graph_exec), g->stream);
+            rc = err == cudaSuccess ? NGX_OK : cuda_fail(err, "replaying the captured batch run");
+        } else {
+            rc = enqueue_run(g, aopts, mode, job, hist_bins, hist_max, o, &extra, dag_block, dag_words * 8);
+        }
+        cudaEventRecord(stop, g->stream);
+        cudaError_t err = cudaEventSynchronize(stop);
+        float ms = 0.0f;
+        if (err == cudaSuccess) {
+            cudaEventElapsedTime(&ms, start, stop);
+        } else if (rc == NGX_OK) {
+            rc = cuda_fail(err, "batch run");
+        }
+        cudaEventDestroy(start);
+        cudaEventDestroy(stop);
+        if (rc == NGX_OK) {
+            int code = 0;
+            NGX_CUDA_TRY(cudaMemcpy(&code, o.error, sizeof(int), cudaMemcpyDeviceToHost));
+            rc = device_error_status(code);
+        }
+        int inexact = 0;
+        if (rc == NGX_OK && mode != kModeApsp) {
+            NGX_CUDA_TRY(cudaMemcpy(&inexact, extra.sigma_inexact, sizeof(int), cudaMemcpyDeviceToHost));
+            if (inexact != 0) {
+                // some path count reached 2^53: rerun with the order-defined pull form for sigma (not captured)
+                extra.sigma_pull = 1;
+                rc = enqueue_run(g, aopts, mode, job, hist_bins, hist_max, o, &extra, dag_block, dag_words * 8);
+                if (rc == NGX_OK) {
+                    err = cudaStreamSynchronize(g->stream);
+                    rc = err == cudaSuccess ? NGX_OK : cuda_fail(err, "batch rerun");
+                }
+                extra.sigma_pull = 0;
+            }
+        }
+        // capture the run for later replays (after a plain run has sized the workspace; nothing executes here)
+        if (rc == NGX_OK && opts->use_cuda_graph && inexact == 0 && (g->graph_exec == nullptr || g->graph_key != key)) {
+            if (g->graph_exec != nullptr) {
+                cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(g->graph_exec));
+                g->graph_exec = nullptr;
+                g->graph_key = 0;
+            }
+            // The workspace was sized by the run above, so the capture allocates nothing. A capture that fails anyway
+            // leaves the handle without a graph; the results of the run above stand and later calls launch normally.
+            cudaGraph_t graph = nullptr;
+            if (cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                const int crc = enqueue_run(g, aopts, mode, job, hist_bins, hist_max, o, &extra, dag_block, dag_words * 8);
+                const cudaError_t cerr = cudaStreamEndCapture(g->stream, &graph);
+                cudaGraphExec_t exec = nullptr;
+                if (crc == NGX_OK && cerr == cudaSuccess && graph != nullptr && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+                    g->graph_exec = exec;
+                    g->graph_key = key;
+                }
+                if (graph != nullptr) {
+                    cudaGraphDestroy(graph);
+                }
+            }
+            cudaGetLastError();
+            set_last_error("");
+        }
+        if (rc != NGX_OK) {
+            return rc;
+        }
+
+        // per-graph results
+        std::vector<unsigned long long> acc, counters;
+        if ((rc = read_totals(g, o, acc, counters)) != NGX_OK) {
+            return rc;
+        }
+        for (int64_t gi = 0; gi < count; ++gi) {
+            ngx_apsp_result* r = &results[gi];
+            clear_result_totals(r);
+            const GraphPart& part = g->parts[static_cast<size_t>(gi)];
+            if ((rc = collect_graph(g, o, acc.data(), counters.data(), gi, part.vertex_off, part.n, hist_bins, hist_max, r,
+                                    g->source_order.data() + part.vertex_off)) != NGX_OK) {
+                return rc;
+            }
+            r->kernel_ms = ms;
+        }
+        if (mode == kModeBrandes && bc != nullptr) {
+            std::vector<unsigned long long> fixed(2 * n_total);
+            NGX_CUDA_TRY(cudaMemcpyAsync(fixed.data(), extra.bc, fixed.size() * 8, cudaMemcpyDeviceToHost, g->stream));
+            NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            for (size_t v = 0; v < n_total; ++v) {
+                bc[v] = fixed_value(fixed[2 * v], fixed[2 * v + 1]);
+            }
+        }
+        if (mode == kModeGrad && (dcpl != nullptr || deff != nullptr)) {
+            std::vector<unsigned long long> fixed(4 * m_total);
+            NGX_CUDA_TRY(cudaMemcpyAsync(fixed.data(), extra.grad_cpl, fixed.size() * 8, cudaMemcpyDeviceToHost, g->stream));
+            NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            for (int64_t gi = 0; gi < count; ++gi) {
+                const GraphPart& part = g->parts[static_cast<size_t>(gi)];
+                const double r = static_cast<double>(results[gi].reached_pairs);
+                for (int64_t e = 0; e < part.m_user; ++e) {
+                    const size_t i = static_cast<size_t>(part.user_arc_off + e);
+                    if (dcpl != nullptr) dcpl[i] = fixed_value(fixed[2 * i], fixed[2 * i + 1]) / r;
+                    if (deff != nullptr) deff[i] = -fixed_value(fixed[2 * m_total + 2 * i], fixed[2 * m_total + 2 * i + 1]) / r;
+                }
+            }
+        }
+        NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        return NGX_OK;
+    });
+}
+
+int ngx_batch_autotune(ngx_graph* g, int task, double* class_scales) {
+    return guard_host("ngx_batch_autotune", [&]() -> int {
+        if (g == nullptr) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_batch_autotune: batch is NULL");
+        }
+        const int mode = task_mode(task);
+        if (mode < 0) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_batch_autotune: unknown task");
+        }
+        NGX_CUDA_TRY(cudaSetDevice(g->device));
+        *g->h_abort = 0;
+        static const double kScales[] = { 0.125, 0.25, 0.5, 1.0, 2.0, 4.0 };
+        ngx_apsp_opts aopts{};
+        aopts.metric = NGX_METRIC_REGULAR;
+        aopts.mode = NGX_MODE_BATCHED;
+        for (int c = 0; c < NGX_SIZE_CLASSES; ++c) {
+            std::vector<int32_t> members;
+            for (size_t i = 0; i < g->parts.size(); ++i) {
+                if (size_class(g->parts[i].n) == c && g->parts[i].n > 0) {
+                    members.push_back(static_cast<int32_t>(i));
+                }
+            }
+            if (class_scales != nullptr) {
+                class_scales[c] = 0.0;
+            }
+            if (members.empty()) {
+                continue;
+            }
+            std::sort(members.begin(), members.end(), [&](int32_t a, int32_t b) { return g->parts[static_cast<size_t>(a)].n < g->parts[static_cast<size_t>(b)].n; });
+            const int32_t gi = members[members.size() / 2];
+            const GraphPart& part = g->parts[static_cast<size_t>(gi)];
+            // one wave of the graph's source tiles (at most 2 x SMs tiles)
+            const int64_t tiles = std::min<int64_t>((part.n + kTile - 1) / kTile, 2 * g->sm_count);
+            std::vector<WorkItem> items(static_cast<size_t>(tiles));
+            for (int64_t t = 0; t < tiles; ++t) {
+                items[static_cast<size_t>(t)] = WorkItem{ 0, static_cast<int32_t>(t) };
+            }
+            // the graph's sources in the order a run takes them
+            const std::vector<int32_t> sources(g->source_order.begin() + part.vertex_off, g->source_order.begin() + part.vertex_off + part.n);
+            WorkItem* d_items = nullptr;
+            NGX_CUDA_TRY(cudaMalloc(&d_items, items.size() * sizeof(WorkItem)));
+            NGX_CUDA_TRY(cudaMemcpy(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
+            double best_rate = -1.0, best_scale = 1.0;
+            for (const double scale : kScales) {
+                RunOutputs o;
+                int rc = alloc_outputs(g, 1, part.n, 0, false, o, false);
+                DagOutputs extra;
+                unsigned long long* dag = nullptr;
+                const size_t dag_words = 1 + (mode == kModeBrandes ? 2 * static_cast<size_t>(g->n_total) : 0) +
+                                         (mode == kModeGrad ? 4 * static_cast<size_t>(g->m_user) : 0);
+                if (rc == NGX_OK && mode != kModeApsp) {
+                    rc = grow_buffer(g, &g->d_call_dag, &g->call_dag_bytes, dag_words * 8);
+                    if (rc == NGX_OK) {
+                        dag = static_cast<unsigned long long*>(g->d_call_dag);
+                        cudaMemsetAsync(dag, 0, dag_words * 8, g->stream);
+                        extra.sigma_inexact = reinterpret_cast<int*>(dag);
+                        if (mode == kModeBrandes) extra.bc = dag + 1;
+                        if (mode == kModeGrad) {
+                            extra.grad_cpl = dag + 1;
+                            extra.grad_eff = dag + 1 + 2 * static_cast<size_t>(g->m_user);
+                        }
+                    }
+                }
+                if (rc == NGX_OK) {
+                    const GraphDesc desc{ part.n, part.m_stored, part.row_off, 0, part.n, part.vertex_off, pick_delta(part.mean_len_regular, 0.0, scale) };
+                    cudaMemsetAsync(o.block, 0, o.zeroed_bytes, g->stream);
+                    cudaMemcpyAsync(o.graphs, &desc, sizeof(desc), cudaMemcpyHostToDevice, g->stream);
+                    cudaMemcpyAsync(o.sources, sources.data(), sources.size() * 4, cudaMemcpyHostToDevice, g->stream);
+                    TileJob job;
+                    job.num_graphs = 1;
+                    job.num_items = tiles;
+                    job.d_items = d_items;
+                    job.num_sources = part.n;
+                    job.n_max = g->n;
+                    float ms = 0.0f;
+                    rc = launch_tiles(g, &aopts, mode, job, 0, 0.0, o, mode != kModeApsp ? &extra : nullptr, &ms, true);
+                    if (rc == NGX_OK) {
+                        std::vector<unsigned long long> acc, counters;
+                        rc = read_totals(g, o, acc, counters);
+                        if (rc == NGX_OK && ms > 0.0f) {
+                            const double rate = static_cast<double>(counters[kTraversedArcs]) / ms;
+                            if (rate > best_rate) {
+                                best_rate = rate;
+                                best_scale = scale;
+                            }
+                        }
+                    }
+                }
+                free_outputs(g, o);
+                cudaStreamSynchronize(g->stream);
+                if (rc != NGX_OK) {
+                    cudaFree(d_items);
+                    return rc;
+                }
+            }
+            cudaFree(d_items);
+            g->class_scale[c] = best_scale;
+            if (class_scales != nullptr) {
+                class_scales[c] = best_scale;
+            }
+        }
+        return NGX_OK;
+    });
 }
 
 int ngx_graph_update_weights(ngx_graph* g, const double* w) {
-    if (g == nullptr || (w == nullptr && g->m_user > 0)) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_update_weights: graph or w is NULL");
-    }
-    NGX_CUDA_TRY(cudaSetDevice(g->device));
-    const size_t m = static_cast<size_t>(g->m_stored);
-    std::vector<Arc> regular(m), inverse(m), rarcs(m);
-    NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    NGX_CUDA_TRY(cudaMemcpy(regular.data(), g->d_arcs_regular, m * sizeof(Arc), cudaMemcpyDeviceToHost));
-    NGX_CUDA_TRY(cudaMemcpy(rarcs.data(), g->d_rarcs, m * sizeof(Arc), cudaMemcpyDeviceToHost));
-    for (int64_t e = 0; e < g->m_user; ++e) {
-        const int32_t stored = g->stored_of_user[static_cast<size_t>(e)];
-        const double a = std::fabs(w[e]);
-        if (!std::isfinite(w[e]) || (stored < 0) != (a == 0.0)) {
-            return fail(NGX_INVALID_ARGUMENT, "ngx_graph_update_weights: arc " + std::to_string(e) + " is non-finite or changes between zero and non-zero");
+    return guard_host("ngx_graph_update_weights", [&]() -> int {
+        if (g == nullptr || (w == nullptr && g->m_user > 0)) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_graph_update_weights: graph or w is NULL");
         }
-        if (stored >= 0) {
-            regular[static_cast<size_t>(stored)].len = a;
-        }
-    }
-    double sum_regular = 0.0, sum_inverse = 0.0, min_regular = INFINITY, max_regular = 0.0;
-    for (size_t e = 0; e < m; ++e) {
-        inverse[e] = regular[e];
-        inverse[e].len = 1.0 / regular[e].len;
-        sum_regular += regular[e].len;
-        sum_inverse += inverse[e].len;
-        min_regular = std::min(min_regular, regular[e].len);
-        max_regular = std::max(max_regular, regular[e].len);
-    }
-    for (size_t r = 0; r < m; ++r) {
-        rarcs[r].len = regular[static_cast<size_t>(rarcs[r].id)].len;
-    }
-    for (GraphPart& part : g->parts) {
-        double sr = 0.0, si = 0.0;
-        for (int64_t e = 0; e < part.m_user; ++e) {
-            const int32_t stored = g->stored_of_user[static_cast<size_t>(part.user_arc_off + e)];
+        NGX_CUDA_TRY(cudaSetDevice(g->device));
+        const size_t m = static_cast<size_t>(g->m_stored);
+        std::vector<Arc> regular(m), inverse(m), rarcs(m);
+        NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+        NGX_CUDA_TRY(cudaMemcpy(regular.data(), g->d_arcs_regular, m * sizeof(Arc), cudaMemcpyDeviceToHost));
+        NGX_CUDA_TRY(cudaMemcpy(rarcs.data(), g->d_rarcs, m * sizeof(Arc), cudaMemcpyDeviceToHost));
+        for (int64_t e = 0; e < g->m_user; ++e) {
+            const int32_t stored = g->stored_of_user[static_cast<size_t>(e)];
+            const double a = std::fabs(w[e]);
+            if (!std::isfinite(w[e]) || (stored < 0) != (a == 0.0)) {
+                return fail(NGX_INVALID_ARGUMENT, "ngx_graph_update_weights: arc " + std::to_string(e) + " is non-finite or changes between zero and non-zero");
+            }
             if (stored >= 0) {
-                sr += regular[static_cast<size_t>(stored)].len;
-                si += inverse[static_cast<size_t>(stored)].len;
+                regular[static_cast<size_t>(stored)].len = a;
             }
         }
-        if (part.m_stored > 0) {
-            part.mean_len_regular = sr / static_cast<double>(part.m_stored);
-            part.mean_len_inverse = si / static_cast<double>(part.m_stored);
+        double sum_regular = 0.0, sum_inverse = 0.0, min_regular = INFINITY, max_regular = 0.0;
+        for (size_t e = 0; e < m; ++e) {
+            inverse[e] = regular[e];
+            inverse[e].len = 1.0 / regular[e].len;
+            sum_regular += regular[e].len;
+            sum_inverse += inverse[e].len;
+            min_regular = std::min(min_regular, regular[e].len);
+            max_regular = std::max(max_regular, regular[e].len);
         }
-    }
-    if (m > 0) {
-        g->mean_len_regular = sum_regular / static_cast<double>(m);
-        g->mean_len_inverse = sum_inverse / static_cast<double>(m);
-        g->min_len_regular = min_regular;
-        g->max_len_regular = max_regular;
-        NGX_CUDA_TRY(cudaMemcpy(g->d_arcs_regular, regular.data(), m * sizeof(Arc), cudaMemcpyHostToDevice));
-        NGX_CUDA_TRY(cudaMemcpy(g->d_arcs_inverse, inverse.data(), m * sizeof(Arc), cudaMemcpyHostToDevice));
-        NGX_CUDA_TRY(cudaMemcpy(g->d_rarcs, rarcs.data(), m * sizeof(Arc), cudaMemcpyHostToDevice));
-    }
-    return NGX_OK;
+        for (size_t r = 0; r < m; ++r) {
+            rarcs[r].len = regular[static_cast<size_t>(rarcs[r].id)].len;
+        }
+        for (GraphPart& part : g->parts) {
+            double sr = 0.0, si = 0.0;
+            for (int64_t e = 0; e < part.m_user; ++e) {
+                const int32_t stored = g->stored_of_user[static_cast<size_t>(part.user_arc_off + e)];
+                if (stored >= 0) {
+                    sr += regular[static_cast<size_t>(stored)].len;
+                    si += inverse[static_cast<size_t>(stored)].len;
+                }
+            }
+            if (part.m_stored > 0) {
+                part.mean_len_regular = sr / static_cast<double>(part.m_stored);
+                part.mean_len_inverse = si / static_cast<double>(part.m_stored);
+            }
+        }
+        if (m > 0) {
+            g->mean_len_regular = sum_regular / static_cast<double>(m);
+            g->mean_len_inverse = sum_inverse / static_cast<double>(m);
+            g->min_len_regular = min_regular;
+            g->max_len_regular = max_regular;
+            NGX_CUDA_TRY(cudaMemcpy(g->d_arcs_regular, regular.data(), m * sizeof(Arc), cudaMemcpyHostToDevice));
+            NGX_CUDA_TRY(cudaMemcpy(g->d_arcs_inverse, inverse.data(), m * sizeof(Arc), cudaMemcpyHostToDevice));
+            NGX_CUDA_TRY(cudaMemcpy(g->d_rarcs, rarcs.data(), m * sizeof(Arc), cudaMemcpyHostToDevice));
+        }
+        return NGX_OK;
+    });
 }
 
 }  // extern "C"

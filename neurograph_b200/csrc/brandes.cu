@@ -122,17 +122,21 @@ using namespace ngx;
 extern "C" {
 
 int ngx_brandes(ngx_graph* graph, const ngx_apsp_opts* opts, double* bc, ngx_apsp_result* result) {
-    if (graph == nullptr || opts == nullptr || (bc == nullptr && graph->n > 0)) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_brandes: graph, opts or bc is NULL");
-    }
-    return dag_run(graph, opts, kModeBrandes, result, bc, nullptr, nullptr);
+    return guard_host("ngx_brandes", [&]() -> int {
+        if (graph == nullptr || opts == nullptr || (bc == nullptr && graph->n > 0)) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_brandes: graph, opts or bc is NULL");
+        }
+        return dag_run(graph, opts, kModeBrandes, result, bc, nullptr, nullptr);
+    });
 }
 
 int ngx_apsp_grad(ngx_graph* graph, const ngx_apsp_opts* opts, double* dcpl, double* deff, ngx_apsp_result* result) {
-    if (graph == nullptr || opts == nullptr || ((dcpl == nullptr || deff == nullptr) && graph->m_user > 0)) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_apsp_grad: graph, opts, dcpl or deff is NULL");
-    }
-    return dag_run(graph, opts, kModeGrad, result, nullptr, dcpl, deff);
+    return guard_host("ngx_apsp_grad", [&]() -> int {
+        if (graph == nullptr || opts == nullptr || ((dcpl == nullptr || deff == nullptr) && graph->m_user > 0)) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_apsp_grad: graph, opts, dcpl or deff is NULL");
+        }
+        return dag_run(graph, opts, kModeGrad, result, nullptr, dcpl, deff);
+    });
 }
 
 }  // extern "C"

@@ -17,12 +17,16 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
+#include <memory>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
 
 #include "ngx_common.cuh"
 #include "ngx_network.h"
+#include "ngx_threads.h"
 
 
 namespace ngx {
@@ -231,21 +235,15 @@ void parse_arcs(const std::string& text, const RankInfo& info, bool out, int thr
     }
     const size_t first = parts.size();
     parts.resize(first + static_cast<size_t>(pieces));
-    std::vector<std::thread> pool;
-    for (int i = 0; i < pieces; ++i) {
-        pool.emplace_back([&, i] {
-            std::vector<RawArc>& mine = parts[first + static_cast<size_t>(i)];
-            for_each_line(cut[static_cast<size_t>(i)], cut[static_cast<size_t>(i) + 1], [&](const char* p, const char* e) {
-                RawArc arc{};
-                if (parse_arc(p, e, info, out, arc)) {
-                    mine.push_back(arc);
-                }
-            });
+    parallel_for(pieces, pieces, [&](int64_t i) {
+        std::vector<RawArc>& mine = parts[first + static_cast<size_t>(i)];
+        for_each_line(cut[static_cast<size_t>(i)], cut[static_cast<size_t>(i) + 1], [&](const char* p, const char* e) {
+            RawArc arc{};
+            if (parse_arc(p, e, info, out, arc)) {
+                mine.push_back(arc);
+            }
         });
-    }
-    for (auto& t : pool) {
-        t.join();
-    }
+    });
 }
 
 // Rows of (target, summed weight) per source, targets ascending and unique; weights summed in 32-bit two's
@@ -272,29 +270,23 @@ void merge_rows(int64_t n, const std::vector<std::vector<RawArc>>& parts, int th
     }
     // sort each row by target, merge repeats (rows split over the threads)
     std::vector<int64_t> kept(static_cast<size_t>(n), 0);
-    std::vector<std::thread> pool;
     const int workers = std::max(1, threads);
-    for (int t = 0; t < workers; ++t) {
-        pool.emplace_back([&, t] {
-            for (int64_t v = t; v < n; v += workers) {
-                auto* b = entries.data() + count[static_cast<size_t>(v)];
-                auto* e = entries.data() + count[static_cast<size_t>(v + 1)];
-                std::stable_sort(b, e, [](const auto& x, const auto& y) { return x.first < y.first; });
-                int64_t out = 0;
-                for (auto* q = b; q < e; ++q) {
-                    if (out > 0 && b[out - 1].first == q->first) {
-                        b[out - 1].second = static_cast<int32_t>(static_cast<uint32_t>(b[out - 1].second) + static_cast<uint32_t>(q->second));
-                    } else {
-                        b[out++] = *q;
-                    }
+    parallel_for(workers, workers, [&](int64_t t) {
+        for (int64_t v = t; v < n; v += workers) {
+            auto* b = entries.data() + count[static_cast<size_t>(v)];
+            auto* e = entries.data() + count[static_cast<size_t>(v + 1)];
+            std::stable_sort(b, e, [](const auto& x, const auto& y) { return x.first < y.first; });
+            int64_t out = 0;
+            for (auto* q = b; q < e; ++q) {
+                if (out > 0 && b[out - 1].first == q->first) {
+                    b[out - 1].second = static_cast<int32_t>(static_cast<uint32_t>(b[out - 1].second) + static_cast<uint32_t>(q->second));
+                } else {
+                    b[out++] = *q;
                 }
-                kept[static_cast<size_t>(v)] = out;
             }
-        });
-    }
-    for (auto& th : pool) {
-        th.join();
-    }
+            kept[static_cast<size_t>(v)] = out;
+        }
+    });
     row_ptr.assign(static_cast<size_t>(n) + 1, 0);
     for (int64_t v = 0; v < n; ++v) {
         row_ptr[static_cast<size_t>(v + 1)] = row_ptr[static_cast<size_t>(v)] + kept[static_cast<size_t>(v)];
@@ -337,7 +329,8 @@ using namespace ngx;
 
 extern "C" {
 
-int ngx_network_load(const char* directory, int32_t number_ranks, const char* file_prefix, int flags, int threads, ngx_network** out) {
+namespace {
+int load_network(const char* directory, int32_t number_ranks, const char* file_prefix, int flags, int threads, ngx_network** out) {
     if (directory == nullptr || out == nullptr || number_ranks < 1) {
         return fail(NGX_INVALID_ARGUMENT, "ngx_network_load: directory or out is NULL, or number_ranks < 1");
     }
@@ -348,14 +341,13 @@ int ngx_network_load(const char* directory, int32_t number_ranks, const char* fi
     const int workers = threads > 0 ? threads : std::max(1u, std::thread::hardware_concurrency());
     const std::string dir(directory);
     const std::string prefix = file_prefix != nullptr ? file_prefix : "";
-    auto net = new ngx_network();
+    auto net = std::make_unique<ngx_network>();
     // vertices per rank, then global numbering
     net->rank_nodes.resize(static_cast<size_t>(number_ranks));
     for (int r = 0; r < number_ranks; ++r) {
         std::string text;
         const std::string path = dir + "/positions/" + rank_prefix(r, number_ranks) + "_positions.txt";
         if (!read_file(path, text)) {
-            delete net;
             return fail(NGX_INVALID_ARGUMENT, "ngx_network_load: cannot read " + path);
         }
         net->rank_nodes[static_cast<size_t>(r)] = count_nodes(text);
@@ -366,7 +358,6 @@ int ngx_network_load(const char* directory, int32_t number_ranks, const char* fi
     }
     net->n = rank_prefix_sum.back();
     if (net->n >= (int64_t(1) << 31)) {
-        delete net;
         return fail(NGX_UNSUPPORTED, "ngx_network_load: more than 2^31 - 1 vertices");
     }
     const bool undirected = (flags & NGX_LOAD_UNDIRECTED) != 0;
@@ -378,7 +369,6 @@ int ngx_network_load(const char* directory, int32_t number_ranks, const char* fi
             std::string text;
             const std::string path = dir + "/network/" + rank_prefix(r, number_ranks) + prefix + (out_arcs ? "_out_network.txt" : "_in_network.txt");
             if (!read_file(path, text)) {
-                delete net;
                 return fail(NGX_INVALID_ARGUMENT, "ngx_network_load: cannot read " + path);
             }
             parse_arcs(text, info, out_arcs, workers, out_arcs ? out_parts : in_parts);
@@ -452,8 +442,19 @@ int ngx_network_load(const char* directory, int32_t number_ranks, const char* fi
         }
         net->row_ptr[static_cast<size_t>(v + 1)] = static_cast<int64_t>(net->col.size());
     }
-    *out = net;
+    *out = net.release();
     return NGX_OK;
+}
+}  // namespace
+
+int ngx_network_load(const char* directory, int32_t number_ranks, const char* file_prefix, int flags, int threads, ngx_network** out) {
+    try {
+        return load_network(directory, number_ranks, file_prefix, flags, threads, out);
+    } catch (const std::bad_alloc&) {
+        return fail(NGX_OUT_OF_MEMORY, "ngx_network_load: host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(NGX_OUT_OF_MEMORY, std::string("ngx_network_load: ") + e.what());
+    }
 }
 
 int ngx_network_size(const ngx_network* net, int64_t* n, int64_t* m) {

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <exception>
+#include <new>
 #include <string>
 
 #include "ngx_b200.h"
@@ -224,6 +226,21 @@ struct Error {
 void set_last_error(const std::string& message);
 int fail(int status, const std::string& message);
 int cuda_fail(cudaError_t err, const char* what);
+
+// Runs the body of a C entry point and turns a host exception (an allocation that failed) into a status, so that no
+// exception crosses the C ABI.
+template <typename Body>
+int guard_host(const char* entry, const Body& body) noexcept {
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        return fail(NGX_OUT_OF_MEMORY, std::string(entry) + ": host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(NGX_OUT_OF_MEMORY, std::string(entry) + ": " + e.what());
+    } catch (...) {
+        return fail(NGX_OUT_OF_MEMORY, std::string(entry) + ": host failure");
+    }
+}
 
 }  // namespace ngx
 

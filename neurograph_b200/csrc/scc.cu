@@ -165,99 +165,101 @@ using namespace ngx;
 extern "C" {
 
 int ngx_scc(ngx_graph* g, int32_t* component, uint64_t* number_components, uint64_t* largest_component, uint64_t* size_histogram) {
-    if (g == nullptr || number_components == nullptr || largest_component == nullptr) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_scc: graph or outputs are NULL");
-    }
-    if (g->parts.size() != 1) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_scc: this handle holds a batch of graphs");
-    }
-    const int64_t n = g->n;
-    *number_components = 0;
-    *largest_component = 0;
-    if (size_histogram != nullptr) {
-        std::fill(size_histogram, size_histogram + n + 1, uint64_t(0));
-    }
-    if (n == 0) {
-        return NGX_OK;
-    }
-    NGX_CUDA_TRY(cudaSetDevice(g->device));
-    const size_t words = static_cast<size_t>(n);
-    // device layout: comp i32[n] | color i32[n] | sizes u64[n] | visited u8[n] | flags i32[2], each 256-byte aligned
-    const size_t off_color = align256(words * 4);
-    const size_t off_sizes = off_color + align256(words * 4);
-    const size_t off_visited = off_sizes + align256(words * 8);
-    const size_t off_flags = off_visited + align256(words);
-    const size_t bytes = off_flags + 256;
-    if (const int rc = grow_buffer(g, &g->d_call_out, &g->call_out_bytes, bytes); rc != NGX_OK) {
-        return rc;
-    }
-    char* base = static_cast<char*>(g->d_call_out);
-    auto* comp = reinterpret_cast<int32_t*>(base);
-    auto* color = reinterpret_cast<int32_t*>(base + off_color);
-    auto* sizes = reinterpret_cast<unsigned long long*>(base + off_sizes);
-    auto* visited = reinterpret_cast<uint8_t*>(base + off_visited);
-    auto* flags = reinterpret_cast<int*>(base + off_flags);
-    NGX_CUDA_TRY(cudaMemsetAsync(comp, 0xFF, words * 4, g->stream));  // -1: no component yet
-    int h_flag = 0;
-    const int vgrid = static_cast<int>(std::min<int64_t>((n + kSccBlock - 1) / kSccBlock, 8 * int64_t(g->sm_count)));
-    const int wgrid = static_cast<int>(std::min<int64_t>((n * 32 + kSccBlock - 1) / kSccBlock, 32 * int64_t(g->sm_count)));
-    const int64_t* row_ptr = g->d_row_ptr;
-    const Arc* arcs = g->d_arcs_regular;
-    const int64_t* rrow_ptr = g->d_rrow_ptr;
-    const Arc* rarcs = g->d_rarcs;
-    // every round assigns at least the largest unassigned vertex (its own colour's root)
-    bool done = false;
-    for (int64_t round = 0; round <= n && !done; ++round) {
-        int rc = until_stable(g, flags, &h_flag, n, [&] {
-            scc_trim_kernel<<<wgrid, kSccBlock, 0, g->stream>>>(n, row_ptr, arcs, rrow_ptr, rarcs, comp, flags);
-        });
-        if (rc != NGX_OK) {
+    return guard_host("ngx_scc", [&]() -> int {
+        if (g == nullptr || number_components == nullptr || largest_component == nullptr) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_scc: graph or outputs are NULL");
+        }
+        if (g->parts.size() != 1) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_scc: this handle holds a batch of graphs");
+        }
+        const int64_t n = g->n;
+        *number_components = 0;
+        *largest_component = 0;
+        if (size_histogram != nullptr) {
+            std::fill(size_histogram, size_histogram + n + 1, uint64_t(0));
+        }
+        if (n == 0) {
+            return NGX_OK;
+        }
+        NGX_CUDA_TRY(cudaSetDevice(g->device));
+        const size_t words = static_cast<size_t>(n);
+        // device layout: comp i32[n] | color i32[n] | sizes u64[n] | visited u8[n] | flags i32[2], each 256-byte aligned
+        const size_t off_color = align256(words * 4);
+        const size_t off_sizes = off_color + align256(words * 4);
+        const size_t off_visited = off_sizes + align256(words * 8);
+        const size_t off_flags = off_visited + align256(words);
+        const size_t bytes = off_flags + 256;
+        if (const int rc = grow_buffer(g, &g->d_call_out, &g->call_out_bytes, bytes); rc != NGX_OK) {
             return rc;
         }
-        scc_color_init_kernel<<<vgrid, kSccBlock, 0, g->stream>>>(n, comp, color, visited);
-        NGX_CUDA_TRY(cudaGetLastError());
-        rc = until_stable(g, flags, &h_flag, n, [&] { scc_color_kernel<<<wgrid, kSccBlock, 0, g->stream>>>(n, rrow_ptr, rarcs, comp, color, flags); });
-        if (rc != NGX_OK) {
-            return rc;
+        char* base = static_cast<char*>(g->d_call_out);
+        auto* comp = reinterpret_cast<int32_t*>(base);
+        auto* color = reinterpret_cast<int32_t*>(base + off_color);
+        auto* sizes = reinterpret_cast<unsigned long long*>(base + off_sizes);
+        auto* visited = reinterpret_cast<uint8_t*>(base + off_visited);
+        auto* flags = reinterpret_cast<int*>(base + off_flags);
+        NGX_CUDA_TRY(cudaMemsetAsync(comp, 0xFF, words * 4, g->stream));  // -1: no component yet
+        int h_flag = 0;
+        const int vgrid = static_cast<int>(std::min<int64_t>((n + kSccBlock - 1) / kSccBlock, 8 * int64_t(g->sm_count)));
+        const int wgrid = static_cast<int>(std::min<int64_t>((n * 32 + kSccBlock - 1) / kSccBlock, 32 * int64_t(g->sm_count)));
+        const int64_t* row_ptr = g->d_row_ptr;
+        const Arc* arcs = g->d_arcs_regular;
+        const int64_t* rrow_ptr = g->d_rrow_ptr;
+        const Arc* rarcs = g->d_rarcs;
+        // every round assigns at least the largest unassigned vertex (its own colour's root)
+        bool done = false;
+        for (int64_t round = 0; round <= n && !done; ++round) {
+            int rc = until_stable(g, flags, &h_flag, n, [&] {
+                scc_trim_kernel<<<wgrid, kSccBlock, 0, g->stream>>>(n, row_ptr, arcs, rrow_ptr, rarcs, comp, flags);
+            });
+            if (rc != NGX_OK) {
+                return rc;
+            }
+            scc_color_init_kernel<<<vgrid, kSccBlock, 0, g->stream>>>(n, comp, color, visited);
+            NGX_CUDA_TRY(cudaGetLastError());
+            rc = until_stable(g, flags, &h_flag, n, [&] { scc_color_kernel<<<wgrid, kSccBlock, 0, g->stream>>>(n, rrow_ptr, rarcs, comp, color, flags); });
+            if (rc != NGX_OK) {
+                return rc;
+            }
+            scc_roots_kernel<<<vgrid, kSccBlock, 0, g->stream>>>(n, comp, color, visited);
+            NGX_CUDA_TRY(cudaGetLastError());
+            rc = until_stable(g, flags, &h_flag, n,
+                              [&] { scc_backward_kernel<<<wgrid, kSccBlock, 0, g->stream>>>(n, row_ptr, arcs, comp, color, visited, flags); });
+            if (rc != NGX_OK) {
+                return rc;
+            }
+            NGX_CUDA_TRY(cudaMemsetAsync(flags + 1, 0, sizeof(int), g->stream));
+            scc_assign_kernel<<<vgrid, kSccBlock, 0, g->stream>>>(n, comp, color, visited, flags + 1);
+            NGX_CUDA_TRY(cudaGetLastError());
+            int remaining = 0;
+            NGX_CUDA_TRY(cudaMemcpyAsync(&remaining, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+            NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+            done = remaining == 0;
         }
-        scc_roots_kernel<<<vgrid, kSccBlock, 0, g->stream>>>(n, comp, color, visited);
-        NGX_CUDA_TRY(cudaGetLastError());
-        rc = until_stable(g, flags, &h_flag, n,
-                          [&] { scc_backward_kernel<<<wgrid, kSccBlock, 0, g->stream>>>(n, row_ptr, arcs, comp, color, visited, flags); });
-        if (rc != NGX_OK) {
-            return rc;
+        if (!done) {
+            return fail(NGX_TIMEOUT, "ngx_scc: components did not converge");
         }
-        NGX_CUDA_TRY(cudaMemsetAsync(flags + 1, 0, sizeof(int), g->stream));
-        scc_assign_kernel<<<vgrid, kSccBlock, 0, g->stream>>>(n, comp, color, visited, flags + 1);
+        // component sizes: a component is named by its largest vertex, so sizes[] is indexed by vertex
+        NGX_CUDA_TRY(cudaMemsetAsync(sizes, 0, words * 8, g->stream));
+        scc_count_kernel<<<vgrid, kSccBlock, 0, g->stream>>>(n, comp, sizes);
         NGX_CUDA_TRY(cudaGetLastError());
-        int remaining = 0;
-        NGX_CUDA_TRY(cudaMemcpyAsync(&remaining, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+        std::vector<unsigned long long> host(words);
+        NGX_CUDA_TRY(cudaMemcpyAsync(host.data(), sizes, words * 8, cudaMemcpyDeviceToHost, g->stream));
+        if (component != nullptr) {
+            NGX_CUDA_TRY(cudaMemcpyAsync(component, comp, words * 4, cudaMemcpyDeviceToHost, g->stream));
+        }
         NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
-        done = remaining == 0;
-    }
-    if (!done) {
-        return fail(NGX_TIMEOUT, "ngx_scc: components did not converge");
-    }
-    // component sizes: a component is named by its largest vertex, so sizes[] is indexed by vertex
-    NGX_CUDA_TRY(cudaMemsetAsync(sizes, 0, words * 8, g->stream));
-    scc_count_kernel<<<vgrid, kSccBlock, 0, g->stream>>>(n, comp, sizes);
-    NGX_CUDA_TRY(cudaGetLastError());
-    std::vector<unsigned long long> host(words);
-    NGX_CUDA_TRY(cudaMemcpyAsync(host.data(), sizes, words * 8, cudaMemcpyDeviceToHost, g->stream));
-    if (component != nullptr) {
-        NGX_CUDA_TRY(cudaMemcpyAsync(component, comp, words * 4, cudaMemcpyDeviceToHost, g->stream));
-    }
-    NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
-    for (size_t v = 0; v < words; ++v) {
-        if (host[v] != 0) {
-            *number_components += 1;
-            *largest_component = std::max<uint64_t>(*largest_component, host[v]);
-            if (size_histogram != nullptr) {
-                size_histogram[host[v]] += 1;
+        for (size_t v = 0; v < words; ++v) {
+            if (host[v] != 0) {
+                *number_components += 1;
+                *largest_component = std::max<uint64_t>(*largest_component, host[v]);
+                if (size_histogram != nullptr) {
+                    size_histogram[host[v]] += 1;
+                }
             }
         }
-    }
-    return NGX_OK;
+        return NGX_OK;
+    });
 }
 
 }  // extern "C"

@@ -604,15 +604,19 @@ using namespace ngx;
 
 extern "C" {
 
-int ngx_apsp(ngx_graph* graph, const ngx_apsp_opts* opts, ngx_apsp_result* result) { return run_apsp(graph, opts, result, nullptr, kModeApsp, nullptr); }
+int ngx_apsp(ngx_graph* graph, const ngx_apsp_opts* opts, ngx_apsp_result* result) {
+    return guard_host("ngx_apsp", [&]() -> int { return run_apsp(graph, opts, result, nullptr, kModeApsp, nullptr); });
+}
 
 int ngx_sssp_rows(ngx_graph* graph, const ngx_apsp_opts* opts, double* rows) {
-    if (rows == nullptr || opts == nullptr) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_sssp_rows: opts or rows is NULL");
-    }
-    ngx_apsp_opts o = *opts;
-    o.hist_bins = 0;
-    return run_apsp(graph, &o, nullptr, rows, kModeApsp, nullptr);
+    return guard_host("ngx_sssp_rows", [&]() -> int {
+        if (rows == nullptr || opts == nullptr) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_sssp_rows: opts or rows is NULL");
+        }
+        ngx_apsp_opts o = *opts;
+        o.hist_bins = 0;
+        return run_apsp(graph, &o, nullptr, rows, kModeApsp, nullptr);
+    });
 }
 
 }  // extern "C"
