@@ -211,64 +211,157 @@ def profiled_traffic_per_arc(mode):
 _WORKER = {}
 
 
-def cpu_worker_init(directory):
-    """Maps the CSR read-only (shared page cache across the worker processes)."""
+def cpu_worker_init(directory, count=1):
+    """Maps the CSRs (graph 0 .. count-1) read-only (shared page cache across the worker processes)."""
     sys.path.insert(0, ROOT)
     import oracle
 
-    row_ptr = np.load(os.path.join(directory, "row_ptr.npy"), mmap_mode="r")
-    col = np.load(os.path.join(directory, "col.npy"), mmap_mode="r")
-    w = np.load(os.path.join(directory, "w.npy"), mmap_mode="r")
-    _WORKER["graph"] = oracle.Csr(int(row_ptr.size - 1), row_ptr, col, w)
+    _WORKER["graphs"] = []
+    for i in range(count):
+        row_ptr, col, w = (np.load(os.path.join(directory, f"g{i}_{name}.npy"), mmap_mode="r") for name in ("row_ptr", "col", "w"))
+        _WORKER["graphs"].append(oracle.Csr(int(row_ptr.size - 1), row_ptr, col, w))
     _WORKER["oracle"] = oracle.Restatement()
 
 
-def cpu_worker(sources):
-    g, r = _WORKER["graph"], _WORKER["oracle"]
+def cpu_worker(task):
+    """task: sources of graph 0, or (graph index, sources)."""
+    gi, sources = task if isinstance(task, tuple) else (0, task)
+    g, r = _WORKER["graphs"][gi], _WORKER["oracle"]
     t0 = time.perf_counter()
     a = r.apsp(g, sources=sources, bins=HIST_BINS, hist_max=64.0)
     r.brandes(g, sources=sources)
     return int(a["traversed_arcs"]), time.perf_counter() - t0
 
 
-def run_reference(args, rank, world):
-    """The reference arm: CPU restatement of the reference's Dijkstra + Brandes over all host cores."""
-    if rank != 0:
-        return
+def save_graphs(directory, graphs):
+    for i, (_, row_ptr, col, w) in enumerate(graphs):
+        for name, arr in (("row_ptr", row_ptr), ("col", col), ("w", w)):
+            np.save(os.path.join(directory, f"g{i}_{name}.npy"), arr)
+
+
+def remove_graphs(directory, count):
+    for i in range(count):
+        for name in ("row_ptr", "col", "w"):
+            os.unlink(os.path.join(directory, f"g{i}_{name}.npy"))
+    os.rmdir(directory)
+
+
+def host_cores():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+def time_reference_pool(args, directory, count, tasks_per_step):
+    """W + K steps of the restatement over a spawned process pool (one process per host core); each step maps one
+    task per process. Returns (timed seconds, traversed arcs) of the K timed steps."""
     import multiprocessing as mp
 
-    c = make_graph(args.n, args.degree, args.length_scale, args.sigma)
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-    directory = tempfile.mkdtemp(prefix="ngx_ref_")
-    for name, arr in (("row_ptr", c.row_ptr), ("col", c.col), ("w", c.w)):
-        np.save(os.path.join(directory, f"{name}.npy"), arr)
-    batches = source_batches(c.n, cores, args.warmup + args.steps, 0, 1)
+    cores = host_cores()
     ctx = mp.get_context("spawn")
     times, arcs = [], []
-    with ctx.Pool(cores, initializer=cpu_worker_init, initargs=(directory,)) as pool:
-        pool.map(cpu_worker, [np.zeros(0, np.int64)] * cores)  # start every worker and map the graph before timing
-        for i, batch in enumerate(batches):
+    with ctx.Pool(cores, initializer=cpu_worker_init, initargs=(directory, count)) as pool:
+        pool.map(cpu_worker, [(0, np.zeros(0, np.int64))] * cores)  # start every worker and map the graphs before timing
+        for i in range(args.warmup + args.steps):
             t0 = time.perf_counter()
-            res = pool.map(cpu_worker, [batch[j:j + 1] for j in range(len(batch))], chunksize=1)
+            res = pool.map(cpu_worker, tasks_per_step(i), chunksize=1)
             dt = time.perf_counter() - t0
             if i >= args.warmup:
                 times.append(dt)
                 arcs.append(sum(r[0] for r in res))
-    for name in ("row_ptr", "col", "w"):
-        os.unlink(os.path.join(directory, f"{name}.npy"))
-    os.rmdir(directory)
-    total = sum(times)
-    value = sum(arcs) / total / 1e9
-    line = {
-        "impl": "reference", "metric": "APSP+Brandes GTEPS (batched single graph)", "value": value, "unit": "GTEPS",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(WORKLOAD, sources_per_step=cores, parallelism=f"{cores} host processes x 1 thread"),
-        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": "port",
-                         "sample": f"{cores} sources per step (one per process), APSP summaries + histogram + Brandes, "
-                                   "CPU restatement of the reference Dijkstra/Brandes (the reference build reads int32 weights only)"},
-        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    return sum(times), sum(arcs)
+
+
+def reference_line(args, metric, unit, value, total_s, config, cores, kind, sample):
+    return {
+        "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if unit == "GTEPS" else "int32", "data": "synthetic", "config": config,
+        "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+
+
+def run_reference(args, rank, world):
+    """The reference arm on the host cores (rank 0 only): the reference's algorithm for the selected workload."""
+    if rank != 0:
+        return
+    if args.workload == "scc":
+        run_reference_scc(args)
+        return
+    if args.workload == "uneven-batch":
+        run_reference_uneven_batch(args)
+        return
+    c = make_graph(args.n, args.degree, args.length_scale, args.sigma)
+    cores = host_cores()
+    directory = tempfile.mkdtemp(prefix="ngx_ref_")
+    save_graphs(directory, [(c.n, c.row_ptr, c.col, c.w)])
+    batches = source_batches(c.n, cores, args.warmup + args.steps, 0, 1)
+    total, arcs = time_reference_pool(args, directory, 1, lambda i: [(0, batches[i][j:j + 1]) for j in range(len(batches[i]))])
+    remove_graphs(directory, 1)
+    value = arcs / total / 1e9
+    line = reference_line(args, "APSP+Brandes GTEPS (batched single graph)", "GTEPS", value, total,
+                          dict(WORKLOAD, **workload_overrides(args), n=c.n, arcs=int(c.m), sources_per_step=cores,
+                               parallelism=f"{cores} host processes x 1 thread"), cores, "port",
+                          f"{cores} sources per step (one per process), APSP summaries + histogram + Brandes, CPU restatement "
+                          "of the reference Dijkstra/Brandes (the reference build reads int32 weights only)")
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_uneven_batch(args, sample_graphs=8):
+    """The uneven batch on the host cores: every step four sources per process, round-robin over a seeded sample of the
+    batch's graphs (the CPU rate per traversed arc hardly depends on the graph, and generating all 512 graphs on the
+    host takes over half an hour)."""
+    indices = list(range(0, UNEVEN_BATCH["graphs"], UNEVEN_BATCH["graphs"] // sample_graphs))[:sample_graphs]
+    graphs = uneven_batch_graphs(indices=indices)
+    cores = host_cores()
+    directory = tempfile.mkdtemp(prefix="ngx_ref_")
+    save_graphs(directory, graphs)
+    rng = np.random.default_rng(12345)
+
+    per_step = 4 * cores
+
+    def tasks(i):
+        out = []
+        for j in range(per_step):
+            gi = (i * per_step + j) % len(graphs)
+            out.append((gi, np.array([int(rng.integers(0, graphs[gi][0]))], np.int64)))
+        return out
+
+    total, arcs = time_reference_pool(args, directory, len(graphs), tasks)
+    remove_graphs(directory, len(graphs))
+    value = arcs / total / 1e9
+    line = reference_line(args, "APSP+Brandes GTEPS (uneven multi-graph batch)", "GTEPS", value, total,
+                          dict(UNEVEN_BATCH, workload="uneven batch: 512 connectomes, N ~ U{500..20000}, out-degree ~ U[5,60]; "
+                               f"host arm on graphs {indices}", parallelism=f"{cores} host processes x 1 thread"), cores, "port",
+                          f"{per_step} sources per step ({per_step // cores} per process) over {len(graphs)} of the batch's graphs, APSP summaries + "
+                          "histogram + Brandes, CPU restatement of the reference Dijkstra/Brandes")
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_scc(args):
+    """The reference's own StronglyConnectedComponents (Multistep, its default) built from source, once per step."""
+    import oracle
+
+    config = {**WORKLOAD, **workload_overrides(args), "workload": "strongly connected components of the synthetic connectome "
+              f"N={args.n} (reference StronglyConnectedComponents, Multistep, one rank)"}
+    if not oracle.Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "the reference build (oracle/_ref) is not present; build it with "
+                          "__graft_entry__.build() where the reference sources are", "config": config}), flush=True)
+        return
+    c = make_graph(args.n, args.degree, args.length_scale, args.sigma)
+    ref = oracle.Reference()
+    with stdout_to_stderr():
+        rg = ref.graph(c.n, c.row_ptr, c.col, np.ones(c.m, np.int32))  # SCC ignores the weights
+        total = 0.0
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            rg.scc(3)
+            if i >= args.warmup:
+                total += time.perf_counter() - t0
+    value = c.m * args.steps / total / 1e9
+    line = reference_line(args, "SCC arcs per second (strongly connected components of one graph)", "G arcs/s", value, total,
+                          dict(config, n=c.n, arcs=int(c.m)), 1, "reference",
+                          "the whole graph once per step, reference StronglyConnectedComponents (Multistep) built from source, "
+                          "one rank x one thread")
     print(json.dumps(line), flush=True)
 
 
@@ -298,8 +391,8 @@ UNEVEN_BATCH = {"graphs": 512, "n_min": 500, "n_max": 20000, "degree_min": 5.0, 
                 "weights": "45% integer U{1..10}, 45% log-normal(0,1), 10% unit", "seed": 3, "hist_max": 200.0}
 
 
-def uneven_batch_graphs(rank=0, world=1):
-    """The uneven-batch workload: 512 seeded connectomes (rank r builds graphs r, r + world, ...)."""
+def uneven_batch_graphs(rank=0, world=1, indices=None):
+    """The uneven-batch workload: 512 seeded connectomes (rank r builds graphs r, r + world, ...; or only `indices`)."""
     from neurograph_b200 import synth
 
     cfg = UNEVEN_BATCH
@@ -312,10 +405,15 @@ def uneven_batch_graphs(rank=0, world=1):
         kind = "int" if u < 0.45 else ("lognormal" if u < 0.9 else "unit")
         specs.append((n, deg, kind))
     graphs = []
-    for i in range(rank, cfg["graphs"], world):
+    use_gpu = True
+    if indices is not None:
+        import torch
+
+        use_gpu = torch.cuda.is_available()  # a sample for the host arm: the CPU sampler where there is no GPU
+    for i in (range(rank, cfg["graphs"], world) if indices is None else indices):
         n, deg, kind = specs[i]
         # the dense sampler on the GPU: its O(n^2) CPU form takes over half an hour for the 512 graphs
-        c = synth.connectome(n, deg, cfg["length_scale"], weights=kind, seed=10_000 + i, use_gpu=True)
+        c = synth.connectome(n, deg, cfg["length_scale"], weights=kind, seed=10_000 + i, use_gpu=use_gpu)
         graphs.append((c.n, c.row_ptr, c.col, c.w))
     return graphs
 
@@ -490,10 +588,10 @@ def run_scc(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ran
         "metric": "SCC arcs per second (strongly connected components of one graph)", "value": value, "unit": "G arcs/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": dict(WORKLOAD, **workload_overrides(args), workload=f"strongly connected components of the synthetic connectome "
-                       f"N={c.n}, {c.m} arcs (ngx_scc per step, every rank on its own replica)",
-                       components=out["number_components"], largest=out["largest_component_size"],
-                       l2="graph arrays (both CSRs, ~16 B per arc each) exceed the 126 MB L2 at this size; no flush"),
+        "config": {**WORKLOAD, **workload_overrides(args), "workload": f"strongly connected components of the synthetic connectome "
+                   f"N={c.n}, {c.m} arcs (ngx_scc per step, every rank on its own replica)", "n": c.n, "arcs": int(c.m),
+                   "components": out["number_components"], "largest": out["largest_component_size"],
+                   "l2": "graph arrays (both CSRs, ~16 B per arc each) exceed the 126 MB L2 at this size; no flush"},
         "gpu_launches": None,
         "clocks": clock_info,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
