@@ -12,6 +12,7 @@
 // per arc u -> v, the arc centre(u) -> centre(v) of weight w + d(u) + d(v), the last arc in CSR order winning when
 // several map to the same pair. Its exact diameter plus 2r is the approximation.
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <limits>
@@ -90,6 +91,9 @@ int ngx_diameter_contract(const ngx_csr* csr, uint64_t r, const double* draws, i
         const uint64_t two_r = 2 * r;
         const auto last_iteration = static_cast<uint64_t>(std::ceil(std::log2(static_cast<double>(n))));
         std::vector<Offer> offers;
+        std::vector<int64_t> changed_list;                               // vertices changed by the last round
+        std::vector<uint64_t> changed_mark(static_cast<size_t>(n), 0);  // == stamp: already in changed_list
+        uint64_t stamp = 1;
         for (uint64_t iteration = 0; iteration < last_iteration; ++iteration) {
             // mark_as_centers
             const double threshold = std::pow(2.0, static_cast<double>(iteration)) / static_cast<double>(n);
@@ -111,10 +115,18 @@ int ngx_diameter_contract(const ngx_csr* csr, uint64_t r, const double* draws, i
             if (!has_center) {
                 continue;
             }
-            // perform_growing_step: rounds of offers built from the round's starting state, then applied in order
+            // perform_growing_step: rounds of offers built from the round's starting state, then applied in order. The
+            // first round of an iteration hears every vertex with a centre (the distance bound grows with the iteration);
+            // a later round only the vertices changed by the round before: an unchanged vertex's offers were rejected, or
+            // accepted and so no longer smaller, and target distances only decrease, so none of them could be accepted.
+            // The offers keep their order (vertices ascending, arcs in CSR order), so the results are the same.
+            bool first_round = true;
+            changed_list.clear();
             for (;;) {
                 offers.clear();
-                for (int64_t u = 0; u < n; ++u) {
+                const int64_t heard = first_round ? n : static_cast<int64_t>(changed_list.size());
+                for (int64_t h = 0; h < heard; ++h) {
+                    const int64_t u = first_round ? h : changed_list[static_cast<size_t>(h)];
                     if (center[static_cast<size_t>(u)] < 0) {
                         continue;
                     }
@@ -139,7 +151,8 @@ int ngx_diameter_contract(const ngx_csr* csr, uint64_t r, const double* draws, i
                         offers.push_back(Offer{ v, center[static_cast<size_t>(u)], nd, gu });
                     }
                 }
-                bool changed = false;
+                first_round = false;
+                changed_list.clear();
                 for (const Offer& o : offers) {
                     if (distance[static_cast<size_t>(o.target)] <= o.distance) {
                         continue;
@@ -148,11 +161,16 @@ int ngx_diameter_contract(const ngx_csr* csr, uint64_t r, const double* draws, i
                     distance[static_cast<size_t>(o.target)] = o.distance;
                     generation[static_cast<size_t>(o.target)] = o.generation;
                     stable[static_cast<size_t>(o.target)] = 0;
-                    changed = true;
+                    if (changed_mark[static_cast<size_t>(o.target)] != stamp) {
+                        changed_mark[static_cast<size_t>(o.target)] = stamp;
+                        changed_list.push_back(o.target);
+                    }
                 }
-                if (!changed) {
+                if (changed_list.empty()) {
                     break;
                 }
+                std::sort(changed_list.begin(), changed_list.end());  // heard in vertex order
+                ++stamp;
             }
             // stabilize_nodes, check_all_stable
             bool all_stable = true;

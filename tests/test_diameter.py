@@ -90,6 +90,23 @@ def test_against_the_reference(restatement):
     assert agreed_values >= 24  # most cases reach every vertex, so values (not just failures) are compared
 
 
+def test_against_the_reference_on_larger_graphs(restatement):
+    """Thousands of vertices: growing steps of many rounds, where the rounds after the first hear only the vertices the
+    round before changed."""
+    if not oracle.Reference.available():
+        pytest.skip("the reference build (oracle/_ref) is not here")
+    ref = oracle.Reference()
+    agreed_values = 0
+    for n, degree, seed in ((3000, 4, 5), (6000, 8, 3)):
+        n, rp, c, w = symmetric_graph(n, degree, seed=seed)
+        g = ref.graph(n, rp, c, w.astype(np.int32))
+        n, rp, c, w = g.csr()
+        for r in (1, 2, 3):
+            for s in (1, 2, 3):
+                agreed_values += _agree(restatement, g, n, rp, c, w.astype(np.float64), r, None, s)
+    assert agreed_values >= 12
+
+
 def symmetric_graph(n, degree, seed):
     """A connectome with every arc mirrored and weights 1..3, so that balls can reach every vertex."""
     cg = synth.connectome(n, degree, 0.2, weights="int", seed=seed, use_gpu=False)
