@@ -70,7 +70,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ngx", "reference"], default="ngx")
     ap.add_argument("--sources-per-step", type=int, default=DEFAULT_SOURCES_PER_STEP)
-    ap.add_argument("--n", type=int, default=WORKLOAD["n"])
+    ap.add_argument("--n", "--vertices", dest="n", type=int, default=WORKLOAD["n"],
+                    help="vertices of the connectome (--vertices also passes through torchrun, whose own options --n abbreviates)")
     ap.add_argument("--degree", type=float, default=WORKLOAD["mean_degree"])
     ap.add_argument("--length-scale", type=float, default=WORKLOAD["length_scale"])
     ap.add_argument("--sigma", type=float, default=1.0, help="log-normal sigma of the weights")

@@ -17,8 +17,8 @@ KEYS = {"impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_
         "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"}
 
 
-def run_bench(*args):
-    proc = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", *args], cwd=ROOT,
+def run_bench(*args, launcher=()):
+    proc = subprocess.run([sys.executable, *launcher, os.path.join(ROOT, "bench.py"), "--impl", "reference", *args], cwd=ROOT,
                           capture_output=True, text=True, timeout=600)
     assert proc.returncode == 0, proc.stderr[-2000:]
     lines = [line for line in proc.stdout.splitlines() if line.strip()]
@@ -46,3 +46,17 @@ def test_reference_arm_scc_workload():
     line = run_bench("--workload", "scc", "--n", "1500", "--degree", "10", "--steps", "1", "--warmup", "3")
     check_line(line, "SCC", "G arcs/s")
     assert line["cpu_baseline"]["kind"] == "reference" and line["config"]["n"] == 1500
+
+
+def test_reference_arm_under_torchrun():
+    """Launched like the multi-GPU arm (one process per GPU): rank 0 alone runs and prints; the other ranks exit 0."""
+    import socket
+
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    launcher = ("-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr", "127.0.0.1",
+                "--master-port", str(port))
+    line = run_bench("--gpus", "2", "--vertices", "1500", "--degree", "10", "--steps", "1", "--warmup", "3", launcher=launcher)
+    check_line(line, "APSP+Brandes", "GTEPS")
+    assert line["n_gpus"] == 2
