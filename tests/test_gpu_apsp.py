@@ -202,3 +202,26 @@ def test_graph_from_network_files(tmp_path, restatement):
     with ngx.Graph(n, rp, c, w) as g2:
         again = g2.apsp()
     assert again.sum_distances == got.sum_distances and again.diameter == got.diameter
+
+
+@pytest.mark.parametrize("kind", ["signed_and_zero", "heavy", "self_and_repeated", "components"])
+def test_graph_families_against_oracle(restatement, kind):
+    """The families the oracle is pinned on against the live reference (tests/test_oracle.py): signed and zero weights,
+    weights up to the int32 limit, self and repeated arcs, many small components; both metrics, both forms, and
+    betweenness."""
+    import zlib
+
+    from test_oracle import _family
+
+    rng = np.random.default_rng(zlib.crc32(kind.encode()) + 1)
+    for _ in range(2):
+        n, row_ptr, col, w = _family(kind, rng)
+        w = w.astype(np.float64)
+        csr = oracle.Csr.from_arrays(n, row_ptr, col, w)
+        with gpu_graph(n, row_ptr, col, w) as gg:
+            for metric in ("regular", "inverse"):
+                for mode in MODES:
+                    check_against_oracle(gg, csr, restatement, metric=metric, mode=mode, bins=32, hist_max=4.0e9 if kind == "heavy" else 64.0)
+            bc, _ = gg.brandes()
+        want = restatement.brandes(csr)
+        assert np.allclose(bc, want, rtol=1e-12, atol=1e-12 * max(1.0, float(np.abs(want).mean()))), kind

@@ -7,6 +7,7 @@ where its sources and the shim build are present (oracle/_ref), the live referen
 from __future__ import annotations
 
 import math
+import zlib
 
 import numpy as np
 import pytest
@@ -180,6 +181,52 @@ def test_restatement_matches_live_reference_on_random_graphs(restatement):
         for epoch in range(4):  # PushBruteForce, PushCheck, PushShortLong, PushInnerShort
             da = rg.apsp_delta_stepping(3, epoch)
             assert da["cpl"] == ra["cpl"] and da["diameter"] == ra["diameter"]
+
+
+def _family(kind, rng):
+    """Random integer graphs with what the reference's loader and Dijkstra must handle."""
+    n = 220
+    degrees = rng.poisson(4.0, n)
+    row_ptr = np.concatenate([[0], np.cumsum(degrees)]).astype(np.int64)
+    m = int(row_ptr[-1])
+    col = rng.integers(0, n, m).astype(np.int32)
+    if kind == "signed_and_zero":  # lengths are |w|; zero weights are absent arcs
+        w = rng.integers(-6, 7, m)
+    elif kind == "heavy":  # weights up to the int32 limit: sums far above 2^32, still exact in FP64 here
+        w = rng.integers(1, 2**31 - 1, m)
+    elif kind == "self_and_repeated":  # self arcs, and arcs repeated within a row
+        src = np.repeat(np.arange(n), degrees)
+        col = np.where(rng.random(m) < 0.1, src, col).astype(np.int32)
+        dup = np.nonzero(np.diff(row_ptr) >= 2)[0]
+        col[row_ptr[dup] + 1] = col[row_ptr[dup]]
+        w = rng.integers(1, 9, m)
+    else:  # "components": arcs only inside blocks of 11 vertices
+        src = np.repeat(np.arange(n), degrees)
+        col = ((src // 11) * 11 + rng.integers(0, 11, m)).clip(0, n - 1).astype(np.int32)
+        w = rng.integers(1, 9, m)
+    return n, row_ptr, col, w.astype(np.int32)
+
+
+@pytest.mark.skipif(not oracle.Reference.available(), reason="reference shim build not present")
+@pytest.mark.parametrize("kind", ["signed_and_zero", "heavy", "self_and_repeated", "components"])
+def test_restatement_matches_live_reference_on_graph_families(restatement, kind):
+    ref = oracle.Reference()
+    rng = np.random.default_rng(zlib.crc32(kind.encode()))
+    for _ in range(2):
+        n, row_ptr, col, w = _family(kind, rng)
+        rg = ref.graph(n, row_ptr, col, w)
+        n2, rp2, col2, w2 = rg.csr()  # the reference's stored arcs (zero weights dropped) in its order
+        g = oracle.Csr.from_arrays(n2, rp2, col2, w2.astype(np.float64))
+        for inverse in (False, True):
+            ra = rg.apsp(inverse=inverse)
+            oa = restatement.apsp(g, metric=oracle.METRIC_INVERSE if inverse else oracle.METRIC_REGULAR)
+            assert ra["cpl"] == oa["sum_distances_sequential"] / oa["reached_pairs"], (kind, inverse)
+            assert ra["efficiency"] == oa["sum_inverse_sequential"] / oa["reached_pairs"], (kind, inverse)
+            assert ra["diameter"] == oa["diameter"] and ra["cluster_sizes"] == oa["cluster_sizes"], (kind, inverse)
+            assert ra["unreachable"] == oa["unreachable"], (kind, inverse)
+        bc_ref, _ = rg.betweenness()
+        bc = restatement.brandes(g)
+        assert np.allclose(bc, bc_ref, rtol=1e-12, atol=1e-12 * max(1.0, float(np.abs(bc_ref).mean()))), kind
 
 
 @pytest.mark.skipif(not oracle.Reference.available(), reason="reference shim build not present")
