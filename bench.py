@@ -29,7 +29,6 @@ import argparse
 import contextlib
 import gc
 import json
-import math
 import os
 import statistics
 import subprocess
