@@ -28,6 +28,14 @@
  *  - ngx_brandes             BetweennessCentrality::compute_average_betweenness_centrality with BrandesVariant
  *                            (BetweennessCentrality.h:46-80, BetweennessCentralityVariants/BrandesVariant.h:50-159)
  *  - ngx_apsp_grad           no reference counterpart: gradient of CPL and efficiency w.r.t. every arc length
+ *  - ngx_exact_*             the sequential double sums of AllPairsShortestPath.h:146-158, made exact across ranks
+ *  - ngx_batch_*             the per-graph loop of source/neurograph.cpp:139-416, for many graphs in one launch
+ *  - ngx_network_*           DistributedGraph::construct_graph's loading (DistributedGraph.cpp:68-127,
+ *                            FileLoader.cpp:96-327, ArcTransformer.cpp:21-69), one process reading every rank's files
+ *  - ngx_diameter_*          DiameterApproximation::compute_approximation (metrics/paths/DiameterApproximation.h:54-126)
+ *  - ngx_scc                 StronglyConnectedComponents::compute_strongly_connected_components
+ *                            (metrics/connectivity/StronglyConnectedComponents.h:17-36)
+ *  - ngx_apsp_noalloc, ngx_graph_source_order, ngx_graph_update_weights: no counterpart (see their comments)
  */
 #ifndef NGX_B200_H
 #define NGX_B200_H
@@ -272,9 +280,11 @@ NGX_API int ngx_graph_create_from_network(const ngx_network* network, int device
 NGX_API void ngx_network_destroy(ngx_network* network);
 
 /* ------------------------------------------------------------------------------------------------------------------
- * Diameter approximation. Replaces DiameterApproximation::compute_approximation (metrics/paths/DiameterApproximation.h):
- * balls of radius r grown around random centres, the graph contracted to its balls (arc weight w + d(u) + d(v), the
- * last arc of a centre pair in CSR order winning), and the exact diameter of the contracted graph, plus 2r. Centres
+ * Diameter approximation. Replaces DiameterApproximation::compute_approximation
+ * (source/metrics/paths/DiameterApproximation.h:54-126; mark_as_centers :154-179, perform_growing_step :204-284,
+ * contract :297-): balls of radius r grown around random centres, the graph contracted to its balls (arc weight
+ * w + d(u) + d(v), the last arc of a centre pair in CSR order winning), and the exact diameter of the contracted
+ * graph, plus 2r. Centres
  * are drawn from std::mt19937 seeded with `seed` through std::uniform_real_distribution<double>(0, 1) (the reference's
  * DefaultRandomNumberGenerator, seeded there with the MPI rank: 0 for one rank), or, when draws != NULL, from
  * draws[0], draws[1], ... (the last one repeating). Weights must be positive integers below 2^31 (zeros are absent
