@@ -46,7 +46,14 @@ WORKLOAD = {
                 "log-normal(0,1) FP64 weights; APSP summaries + 1024-bin histogram + Brandes per source batch",
     "n": 100000, "mean_degree": 100.0, "length_scale": 0.08, "weights": "lognormal(0,1)", "seed": 2,
 }
+# The plain small configuration: the one the reference itself can load (integer weights), all sources per step.
+WORKLOAD_C1 = {
+    "workload": "plain small graph: synthetic connectome N=5000, out-degree Poisson(6), kernel exp(-d/0.1), integer weights "
+                "U{1..10} stored FP64; all-sources APSP summaries + 1024-bin histogram + Brandes per step",
+    "n": 5000, "mean_degree": 6.0, "length_scale": 0.1, "weights": "int U{1..10}", "seed": 1,
+}
 HIST_BINS = 1024
+L2_BYTES = 126 << 20
 SLOTS_PER_WAVE = 296  # 148 SMs x 2 resident CTAs
 DEFAULT_SOURCES_PER_STEP = SLOTS_PER_WAVE * 32
 
@@ -74,9 +81,11 @@ def parse():
     ap.add_argument("--degree", type=float, default=WORKLOAD["mean_degree"])
     ap.add_argument("--length-scale", type=float, default=WORKLOAD["length_scale"])
     ap.add_argument("--sigma", type=float, default=1.0, help="log-normal sigma of the weights")
-    ap.add_argument("--workload", choices=["single", "uneven-batch", "scc"], default="single",
+    ap.add_argument("--workload", choices=["single", "uneven-batch", "scc", "c1"], default="single",
                     help="single: one connectome (the headline); uneven-batch: 512 connectomes of 500-20000 vertices in one "
-                         "handle; scc: strongly connected components of the connectome (ngx_scc) beside the reference's SCC")
+                         "handle; scc: strongly connected components of the connectome (ngx_scc) beside the reference's SCC; "
+                         "c1: the plain small integer-weight connectome (N=5000), all sources per step, beside the reference "
+                         "itself built from source")
     ap.add_argument("--delta", type=float, default=0.25)
     ap.add_argument("--mode", choices=["brandes", "apsp", "grad", "plain"], default="brandes",
                     help="what one step runs: APSP+Brandes (the headline), APSP only, APSP+gradient, or the plain per-source form")
@@ -85,17 +94,28 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the plain/batched APSP comparison runs")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.workload == "c1":
+        # every step is the whole all-sources job of the small graph; the bucket width follows the integer weights
+        args.n, args.degree, args.length_scale = WORKLOAD_C1["n"], WORKLOAD_C1["mean_degree"], WORKLOAD_C1["length_scale"]
+        args.sources_per_step = WORKLOAD_C1["n"]
+        args.delta = 0.0
+    return args
 
 
-def make_graph(n, degree, length_scale=WORKLOAD["length_scale"], sigma=1.0):
+def make_graph(n, degree, length_scale=WORKLOAD["length_scale"], sigma=1.0, workload="single"):
     from neurograph_b200 import synth
 
+    if workload == "c1":
+        return synth.connectome(WORKLOAD_C1["n"], WORKLOAD_C1["mean_degree"], WORKLOAD_C1["length_scale"], weights="int",
+                                seed=WORKLOAD_C1["seed"], use_gpu=False)
     return synth.connectome(n, degree, length_scale, weights="lognormal", mu=0.0, sigma=sigma, seed=WORKLOAD["seed"])
 
 
 def workload_overrides(args):
     """Config keys that differ from the default connectome (other generator parameters on the same code path)."""
+    if args.workload == "c1":
+        return dict(WORKLOAD_C1)
     if (args.n, args.degree, args.length_scale, args.sigma) == (WORKLOAD["n"], WORKLOAD["mean_degree"], WORKLOAD["length_scale"], 1.0):
         return {}
     return {"workload": f"single graph: synthetic connectome N={args.n}, out-degree Poisson({args.degree:g}), kernel "
@@ -290,6 +310,9 @@ def run_reference(args, rank, world):
     if args.workload == "uneven-batch":
         run_reference_uneven_batch(args)
         return
+    if args.workload == "c1":
+        run_reference_c1(args)
+        return
     c = make_graph(args.n, args.degree, args.length_scale, args.sigma)
     cores = host_cores()
     directory = tempfile.mkdtemp(prefix="ngx_ref_")
@@ -365,6 +388,92 @@ def run_reference_scc(args):
     print(json.dumps(line), flush=True)
 
 
+_REF_WORKER = {}
+
+
+def ref_worker_init(directory):
+    """One reference graph per worker process, built by the reference's own in-memory DistributedGraph construction
+    from the saved integer CSR; what the reference prints goes to stderr."""
+    sys.path.insert(0, ROOT)
+    import oracle
+
+    os.dup2(2, 1)
+    n = int(np.load(os.path.join(directory, "g0_row_ptr.npy")).size - 1)
+    row_ptr, col, w = (np.load(os.path.join(directory, f"g0_{name}.npy")) for name in ("row_ptr", "col", "w"))
+    _REF_WORKER["graph"] = oracle.Reference().graph(n, row_ptr, col, w.astype(np.int32))
+
+
+def ref_worker(_):
+    """One whole all-sources job in the reference: AllPairsShortestPath::compute_apsp with PriorityQueue Dijkstra
+    (AllPairsShortestPath.h:54-57) and BrandesVariant::accumulate_betweenness (BrandesVariant.h:50-74)."""
+    g = _REF_WORKER["graph"]
+    t0 = time.perf_counter()
+    g.apsp(inverse=False, queue=0)
+    g.betweenness(0)
+    return time.perf_counter() - t0
+
+
+def c1_traversed_arcs(c):
+    """Traversed arcs of one all-sources pass (sum over sources of the out-degrees of the reached vertices)."""
+    import oracle
+
+    return int(oracle.Restatement().apsp(oracle.Csr.from_arrays(c.n, c.row_ptr, c.col, c.w))["traversed_arcs"])
+
+
+def run_reference_c1(args):
+    """The plain small configuration on the host cores through the reference itself (built from source against
+    single-rank shims): each step runs one whole all-sources APSP + Brandes job in every host process at once (the
+    reference's hot path is single-threaded per rank and this one-rank build cannot split sources across processes)."""
+    import multiprocessing as mp
+
+    import oracle
+
+    config = dict(WORKLOAD_C1)
+    if not oracle.Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "the reference build (oracle/_ref) is not present; build it with "
+                          "__graft_entry__.build() where the reference sources are", "config": config}), flush=True)
+        return
+    c = make_graph(0, 0, workload="c1")
+    arcs_per_job = c1_traversed_arcs(c)
+    cores = host_cores()
+    directory = tempfile.mkdtemp(prefix="ngx_ref_")
+    save_graphs(directory, [(c.n, c.row_ptr, c.col, c.w)])
+    total = 0.0
+    with mp.get_context("spawn").Pool(cores, initializer=ref_worker_init, initargs=(directory,)) as pool:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            pool.map(ref_worker, range(cores), chunksize=1)
+            if i >= args.warmup:
+                total += time.perf_counter() - t0
+    remove_graphs(directory, 1)
+    value = cores * arcs_per_job * args.steps / total / 1e9
+    line = reference_line(args, "APSP+Brandes GTEPS (plain small graph, all sources)", "GTEPS", value, total,
+                          dict(config, n=c.n, arcs=int(c.m), sources_per_step=c.n * cores,
+                               parallelism=f"{cores} host processes x 1 rank x 1 thread, one whole job each per step"),
+                          cores, "reference",
+                          f"every step {cores} concurrent whole jobs (all {c.n} sources: compute_apsp with PriorityQueue Dijkstra + "
+                          "BrandesVariant::accumulate_betweenness), the reference built from source, 1 rank x 1 thread each")
+    print(json.dumps(line), flush=True)
+
+
+def reference_single_core_c1(c):
+    """The reference itself on one core: one whole all-sources APSP + Brandes job of the plain small graph."""
+    import oracle
+
+    if not oracle.Reference.available():
+        return None
+    arcs = c1_traversed_arcs(c)
+    with stdout_to_stderr():
+        g = oracle.Reference().graph(c.n, c.row_ptr, c.col, c.w.astype(np.int32))
+        t0 = time.perf_counter()
+        g.apsp(inverse=False, queue=0)
+        g.betweenness(0)
+        dt = time.perf_counter() - t0
+    return {"value": arcs / dt / 1e9, "unit": "GTEPS", "cores": 1, "kind": "reference",
+            "sample": f"one whole all-sources job ({c.n} sources, APSP with PriorityQueue Dijkstra + Brandes), {dt:.2f} s, "
+                      "the reference built from source, 1 rank x 1 thread"}
+
+
 def cpu_baseline_single_core(c, sources, budget_s=12.0):
     """The CPU restatement on one core, source after source, until about `budget_s` seconds of work are done."""
     import oracle
@@ -391,10 +500,8 @@ UNEVEN_BATCH = {"graphs": 512, "n_min": 500, "n_max": 20000, "degree_min": 5.0, 
                 "weights": "45% integer U{1..10}, 45% log-normal(0,1), 10% unit", "seed": 3, "hist_max": 200.0}
 
 
-def uneven_batch_graphs(rank=0, world=1, indices=None):
-    """The uneven-batch workload: 512 seeded connectomes (rank r builds graphs r, r + world, ...; or only `indices`)."""
-    from neurograph_b200 import synth
-
+def uneven_batch_specs():
+    """(n, mean degree, weight kind) of each of the uneven batch's 512 seeded connectomes."""
     cfg = UNEVEN_BATCH
     rng = np.random.default_rng(cfg["seed"])
     specs = []
@@ -404,6 +511,15 @@ def uneven_batch_graphs(rank=0, world=1, indices=None):
         u = rng.random()
         kind = "int" if u < 0.45 else ("lognormal" if u < 0.9 else "unit")
         specs.append((n, deg, kind))
+    return specs
+
+
+def uneven_batch_graphs(rank=0, world=1, indices=None):
+    """The uneven-batch workload: 512 seeded connectomes (rank r builds graphs r, r + world, ...; or only `indices`)."""
+    from neurograph_b200 import synth
+
+    cfg = UNEVEN_BATCH
+    specs = uneven_batch_specs()
     graphs = []
     use_gpu = True
     if indices is not None:
@@ -516,8 +632,13 @@ def run_scc(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ran
     on its own replica; the reference's StronglyConnectedComponents (Multistep, its default, and TarjanGathered) on the
     host beside it."""
     t0 = time.perf_counter()
-    c = make_graph(args.n, args.degree, args.length_scale, args.sigma)
+    c = make_graph(args.n, args.degree, args.length_scale, args.sigma, args.workload)
     log(f"[bench] graph n={c.n} m={c.m} generated in {time.perf_counter() - t0:.1f}s")
+    # a graph whose CSR + reverse CSR fit in L2 is timed step by step with L2 flushed between the steps (outside the
+    # timed intervals); larger graphs and their workspaces exceed L2 by themselves
+    graph_bytes = 2 * 16 * c.m + 2 * 8 * (c.n + 1)
+    flush = graph_bytes < L2_BYTES
+    flush_buf = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=f"cuda:{local_rank}") if flush else None
     torch.cuda.empty_cache()
     stream = torch.cuda.Stream()
     g = ngx.Graph(c.n, c.row_ptr, c.col, c.w, device=local_rank)
@@ -648,8 +769,13 @@ def main():
         return
 
     t0 = time.perf_counter()
-    c = make_graph(args.n, args.degree, args.length_scale, args.sigma)
+    c = make_graph(args.n, args.degree, args.length_scale, args.sigma, args.workload)
     log(f"[bench] graph n={c.n} m={c.m} generated in {time.perf_counter() - t0:.1f}s")
+    # a graph whose CSR + reverse CSR fit in L2 is timed step by step with L2 flushed between the steps (outside the
+    # timed intervals); larger graphs and their workspaces exceed L2 by themselves
+    graph_bytes = 2 * 16 * c.m + 2 * 8 * (c.n + 1)
+    flush = graph_bytes < L2_BYTES
+    flush_buf = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=f"cuda:{local_rank}") if flush else None
     torch.cuda.empty_cache()  # the generator's cached blocks would otherwise shrink the library's workspace budget
     stream = torch.cuda.Stream()
     g = ngx.Graph(c.n, c.row_ptr, c.col, c.w, device=local_rank)
@@ -690,7 +816,13 @@ def main():
     kernel_ms = 0.0
     step_events = []
     step_kernel_ms = []
+    step_starts = []
     for i in range(args.warmup, args.warmup + args.steps):
+        if flush:
+            with torch.cuda.stream(stream):
+                flush_buf.fill_(i)  # writes twice the L2 capacity
+            step_starts.append(torch.cuda.Event(enable_timing=True))
+            step_starts[-1].record(stream)
         t_host = time.perf_counter()
         r, _ = step(g, batches[i], hist_max)
         log(f"[bench] host call {1e3 * (time.perf_counter() - t_host):.1f} ms")
@@ -713,6 +845,9 @@ def main():
     for k, (e, kms) in enumerate(zip(step_events, step_kernel_ms)):
         log(f"[bench] step {k}: {prev.elapsed_time(e):.1f} ms, kernel {kms:.1f} ms")
         prev = e
+    if flush:
+        # the timed region is the steps alone: the flushes between them are not counted
+        elapsed = sum(a.elapsed_time(b) for a, b in zip(step_starts, step_events)) / 1e3
     elapsed_max = max_over_ranks(elapsed)
     arcs_total = sum_over_ranks(float(arcs))
     value = arcs_total / elapsed_max / 1e9
@@ -770,7 +905,7 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_single_core(c, batches[0])
+        cpu = reference_single_core_c1(c) if args.workload == "c1" else cpu_baseline_single_core(c, batches[0])
 
     if dist is not None:
         dist.barrier()
@@ -779,13 +914,18 @@ def main():
         return
     metric = {"brandes": "APSP+Brandes GTEPS (batched single graph)", "apsp": "APSP GTEPS (batched single graph)",
               "grad": "APSP+gradient GTEPS (batched single graph)", "plain": "APSP GTEPS (plain per-source form)"}[args.mode]
+    if args.workload == "c1":
+        metric = metric.replace("batched single graph", "plain small graph, all sources")
     line = {
         "metric": metric, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": dict(WORKLOAD, **workload_overrides(args), n=c.n, arcs=c.m, mode=args.mode, sources_per_step=args.sources_per_step, delta=args.delta, hist_bins=HIST_BINS,
                        hist_max=hist_max, parallelism=f"sources sharded over {world} GPU(s), no data-path collective",
-                       l2="graph (320 MB CSR + reverse CSR) and workspaces (GBs) exceed the 126 MB L2; no flush needed"),
+                       l2=(f"graph ({graph_bytes / 1e6:.1f} MB CSR + reverse CSR) fits in L2: L2 flushed between steps by a "
+                           f"{2 * L2_BYTES >> 20} MiB write outside the timed intervals") if flush else
+                          (f"graph ({graph_bytes / 1e6:.0f} MB CSR + reverse CSR) and workspaces (GBs) exceed the 126 MB L2; "
+                           "no flush needed")),
         "gpu_launches": gpu_launches,
         "clocks": clock_info,
         "roofline": roofline,

@@ -28,6 +28,8 @@
  *  - ngx_brandes             BetweennessCentrality::compute_average_betweenness_centrality with BrandesVariant
  *                            (BetweennessCentrality.h:46-80, BetweennessCentralityVariants/BrandesVariant.h:50-159)
  *  - ngx_apsp_grad           no reference counterpart: gradient of CPL and efficiency w.r.t. every arc length
+ *  - ngx_*_fixed, ngx_fixed_to_double  the per-rank betweenness vectors and their reduce_componentwise_sum
+ *                            (BetweennessCentrality.h:74), made exact across ranks
  *  - ngx_exact_*             the sequential double sums of AllPairsShortestPath.h:146-158, made exact across ranks
  *  - ngx_batch_*             the per-graph loop of source/neurograph.cpp:139-416, for many graphs in one launch
  *  - ngx_network_*           DistributedGraph::construct_graph's loading (DistributedGraph.cpp:68-127,
@@ -194,18 +196,35 @@ NGX_API int ngx_brandes(ngx_graph* graph, const ngx_apsp_opts* opts, double* bc,
  */
 NGX_API int ngx_apsp_grad(ngx_graph* graph, const ngx_apsp_opts* opts, double* dcpl, double* deff, ngx_apsp_result* result);
 
+/*
+ * The same runs with the sums left unconverted, for combining the runs of several ranks exactly (the reference reduces
+ * its per-rank betweenness vectors, BetweennessCentrality.h:74, reduce_componentwise_sum). Each value is a 128-bit
+ * unsigned fixed-point number value * 2^64 in two words (low, high): bc_fixed holds 2 n words, the sum over the
+ * requested sources of the pair dependencies; dcpl_fixed and deff_fixed hold 2 m words each, the gradient sums before
+ * the division by R (the reached pairs in result) and, for deff, before the sign. The sums of disjoint source sets add
+ * as 128-bit integers (modulo 2^128) to the sum of their union, and ngx_fixed_to_double turns a sum into the doubles
+ * ngx_brandes / ngx_apsp_grad return: bc = to_double(bc_fixed, 1, +1), dcpl = to_double(dcpl_fixed, R, +1),
+ * deff = to_double(deff_fixed, R, -1), with R summed over the same source sets.
+ */
+NGX_API int ngx_brandes_fixed(ngx_graph* graph, const ngx_apsp_opts* opts, uint64_t* bc_fixed, ngx_apsp_result* result);
+NGX_API int ngx_apsp_grad_fixed(ngx_graph* graph, const ngx_apsp_opts* opts, uint64_t* dcpl_fixed, uint64_t* deff_fixed,
+                                ngx_apsp_result* result);
+/* out[i] = sign * value(words[2i], words[2i+1]) / divisor, as the library converts its own sums. Host-only. */
+NGX_API int ngx_fixed_to_double(const uint64_t* words, int64_t count, double divisor, double sign, double* out);
+
 /* ------------------------------------------------------------------------------------------------------------------
  * APSP without device allocation. No counterpart in the reference.
  *
  * For callers that cannot allocate device memory while they run: a process whose caching allocator already holds
  * nearly all of the GPU (a cudaMalloc there fails or empties the cache), or a loop with a latency bound (cudaFree
- * synchronizes the device). Same inputs, outputs and results as ngx_apsp in the batched form, but every device
- * buffer comes from one fixed array of NGX_NOALLOC_SCRATCH_BYTES per device inside the library, and nothing is
- * allocated. Limits, rejected with NGX_INVALID_ARGUMENT: n <= NGX_NOALLOC_MAX_VERTICES, num_sources <=
- * NGX_NOALLOC_MAX_SOURCES, hist_max > 0 whenever hist_bins > 0 (no automatic bound); the plain form is rejected with
- * NGX_UNSUPPORTED. kernel_ms is not measured (0). The first call on each device resolves the array's address
- * (cudaGetSymbolAddress, which may load the library's device code): make that first call before any stream capture
- * begins. Calls that overlap on the same device share the array and race: serialize them.
+ * synchronizes the device). Same inputs and results as ngx_apsp in the batched form, but every device buffer comes
+ * from one fixed array of NGX_NOALLOC_SCRATCH_BYTES per device inside the library: no device memory is allocated, and
+ * host memory only to build an error message. Differences from ngx_apsp: result must not be NULL; limits, rejected with
+ * NGX_INVALID_ARGUMENT: n <= NGX_NOALLOC_MAX_VERTICES, num_sources <= NGX_NOALLOC_MAX_SOURCES, hist_max > 0 whenever
+ * hist_bins > 0 (no automatic bound); the plain form is rejected with NGX_UNSUPPORTED; kernel_ms is not measured (0).
+ * Every call looks up the array's address (cudaGetSymbolAddress, which may load the library's device code on the
+ * first call) and synchronizes the graph's stream, so the call can never be made while that stream is being captured.
+ * Calls that overlap on the same device share the array and race: serialize them.
  */
 #define NGX_NOALLOC_SCRATCH_BYTES (32u << 20)
 #define NGX_NOALLOC_MAX_VERTICES 32768

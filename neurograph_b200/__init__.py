@@ -113,6 +113,9 @@ def library() -> C.CDLL:
             lib.ngx_brandes.argtypes = [C.c_void_p, C.POINTER(_Opts), C.c_void_p, C.POINTER(_Result)]
         if hasattr(lib, "ngx_apsp_grad"):
             lib.ngx_apsp_grad.argtypes = [C.c_void_p, C.POINTER(_Opts), C.c_void_p, C.c_void_p, C.POINTER(_Result)]
+        lib.ngx_brandes_fixed.argtypes = [C.c_void_p, C.POINTER(_Opts), C.c_void_p, C.POINTER(_Result)]
+        lib.ngx_apsp_grad_fixed.argtypes = [C.c_void_p, C.POINTER(_Opts), C.c_void_p, C.c_void_p, C.POINTER(_Result)]
+        lib.ngx_fixed_to_double.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_void_p]
         lib.ngx_batch_create.argtypes = [C.POINTER(_Csr), C.c_int64, C.c_int, C.POINTER(C.c_void_p)]
         lib.ngx_batch_run.argtypes = [C.c_void_p, C.POINTER(_BatchOpts), C.POINTER(_Result), C.c_void_p, C.c_void_p, C.c_void_p]
         lib.ngx_batch_autotune.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
@@ -342,19 +345,37 @@ class Graph:
         return rows
 
     def brandes(self, sources=None, delta=0.0, hist_bins=0, hist_max=0.0, per_source=False, block_threads=0,
-                ctas_per_sm=0, max_iterations=0):
+                ctas_per_sm=0, max_iterations=0, fixed=False, exact=False):
+        """Betweenness (sum of pair dependencies over the sources) and the run's APSP result. fixed=True returns the
+        unconverted sums instead (ngx_brandes_fixed): an (n, 2) uint64 array of 128-bit fixed-point words."""
         opts, srcs, k = self._opts(sources, "regular", "batched", delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations)
-        r, hist, per = self._result_struct(hist_bins, per_source, k)
-        bc = np.zeros(max(self.n, 1), np.float64)
-        _check(library().ngx_brandes(self._handle, C.byref(opts), bc.ctypes.data, C.byref(r)))
-        return bc[: self.n], self._result(r, hist, per, k)
+        r, hist, per = self._result_struct(hist_bins, per_source, k, exact)
+        if fixed:
+            words = np.zeros((max(self.n, 1), 2), np.uint64)
+            _check(library().ngx_brandes_fixed(self._handle, C.byref(opts), words.ctypes.data, C.byref(r)))
+            bc = words[: self.n]
+        else:
+            bc = np.zeros(max(self.n, 1), np.float64)
+            _check(library().ngx_brandes(self._handle, C.byref(opts), bc.ctypes.data, C.byref(r)))
+            bc = bc[: self.n]
+        out = self._result(r, hist, per, k)
+        if exact:
+            out.acc_digits = r._digits
+        return bc, out
 
-    def apsp_grad(self, sources=None, delta=0.0, block_threads=0, ctas_per_sm=0, max_iterations=0):
+    def apsp_grad(self, sources=None, delta=0.0, block_threads=0, ctas_per_sm=0, max_iterations=0, fixed=False):
+        """Gradients of CPL and efficiency w.r.t. every arc length, and the run's APSP result. fixed=True returns the
+        unconverted sums instead (ngx_apsp_grad_fixed): two (m, 2) uint64 arrays, before the division by R."""
         opts, srcs, k = self._opts(sources, "regular", "batched", delta, 0, 0.0, block_threads, ctas_per_sm, max_iterations)
         r, hist, per = self._result_struct(0, False, k)
-        dcpl = np.zeros(max(self.m, 1), np.float64)
-        deff = np.zeros(max(self.m, 1), np.float64)
-        _check(library().ngx_apsp_grad(self._handle, C.byref(opts), dcpl.ctypes.data, deff.ctypes.data, C.byref(r)))
+        if fixed:
+            dcpl = np.zeros((max(self.m, 1), 2), np.uint64)
+            deff = np.zeros((max(self.m, 1), 2), np.uint64)
+            _check(library().ngx_apsp_grad_fixed(self._handle, C.byref(opts), dcpl.ctypes.data, deff.ctypes.data, C.byref(r)))
+        else:
+            dcpl = np.zeros(max(self.m, 1), np.float64)
+            deff = np.zeros(max(self.m, 1), np.float64)
+            _check(library().ngx_apsp_grad(self._handle, C.byref(opts), dcpl.ctypes.data, deff.ctypes.data, C.byref(r)))
         return dcpl[: self.m], deff[: self.m], self._result(r, hist, per, k)
 
 
@@ -525,6 +546,15 @@ def exact_accumulate(values, digits=None) -> np.ndarray:
         raise ValueError("digits must be a contiguous uint64 array of ACC_DIGITS words")
     _check(library().ngx_exact_accumulate(v.ctypes.data if v.size else None, v.size, d.ctypes.data))
     return d
+
+
+def fixed_to_double(words, divisor: float = 1.0, sign: float = 1.0) -> np.ndarray:
+    """Converts (count, 2) 128-bit fixed-point words (as ngx_brandes_fixed / ngx_apsp_grad_fixed return them, or their
+    merged sums) to doubles the way the library converts its own sums: sign * value / divisor."""
+    w = np.ascontiguousarray(words, dtype=np.uint64).reshape(-1, 2)
+    out = np.zeros(max(w.shape[0], 1), np.float64)
+    _check(library().ngx_fixed_to_double(w.ctypes.data, w.shape[0], float(divisor), float(sign), out.ctypes.data))
+    return out[: w.shape[0]]
 
 
 def exact_round(digits) -> float:

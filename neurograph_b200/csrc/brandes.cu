@@ -40,9 +40,19 @@ int convert_fixed(ngx_graph* g, const unsigned long long* sums, int64_t count, d
     return NGX_OK;
 }
 
-// One Brandes (bc != nullptr) or adjoint (dcpl, deff != nullptr) run of a single-graph handle. The fixed-point sums
-// are converted on the device and copied straight into the caller's arrays.
-int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_result* result, double* bc, double* dcpl, double* deff) {
+// Output arrays of one Brandes / adjoint run: converted doubles, or the unconverted 128-bit fixed-point words.
+struct DagHostOut {
+    double* bc = nullptr;
+    double* dcpl = nullptr;
+    double* deff = nullptr;
+    uint64_t* bc_fixed = nullptr;    // 2 n words
+    uint64_t* dcpl_fixed = nullptr;  // 2 m words
+    uint64_t* deff_fixed = nullptr;  // 2 m words
+};
+
+// One Brandes or adjoint run of a single-graph handle. The fixed-point sums are either converted on the device and
+// copied straight into the caller's double arrays, or copied out as words (for exact merging across ranks).
+int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_result* result, const DagHostOut& out) {
     if (const int rc = check_opts(g, opts); rc != NGX_OK) {
         return rc;
     }
@@ -95,14 +105,25 @@ int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_res
         }
     }
     if (rc == NGX_OK && g->n > 0) {
-        if (tile_mode == kModeBrandes) {
-            rc = convert_fixed(g, extra.bc, static_cast<int64_t>(n), 1.0, 1.0, d_out, bc);
+        const auto copy_words = [&](uint64_t* dst, const unsigned long long* src, size_t count) -> int {
+            NGX_CUDA_TRY(cudaMemcpyAsync(dst, src, 2 * count * 8, cudaMemcpyDeviceToHost, g->stream));
+            return NGX_OK;
+        };
+        if (tile_mode == kModeBrandes && out.bc_fixed != nullptr) {
+            rc = copy_words(out.bc_fixed, extra.bc, n);
+        } else if (tile_mode == kModeBrandes) {
+            rc = convert_fixed(g, extra.bc, static_cast<int64_t>(n), 1.0, 1.0, d_out, out.bc);
+        } else if (out.dcpl_fixed != nullptr) {
+            rc = copy_words(out.dcpl_fixed, extra.grad_cpl, m);
+            if (rc == NGX_OK) {
+                rc = copy_words(out.deff_fixed, extra.grad_eff, m);
+            }
         } else {
             // dCPL/dw = c / R and dE/dw = -f / R over the R reached ordered pairs (0 / 0 = NaN without any)
             const double reached = static_cast<double>(r->reached_pairs);
-            rc = convert_fixed(g, extra.grad_cpl, static_cast<int64_t>(m), reached, 1.0, d_out, dcpl);
+            rc = convert_fixed(g, extra.grad_cpl, static_cast<int64_t>(m), reached, 1.0, d_out, out.dcpl);
             if (rc == NGX_OK) {
-                rc = convert_fixed(g, extra.grad_eff, static_cast<int64_t>(m), reached, -1.0, d_out + m, deff);
+                rc = convert_fixed(g, extra.grad_eff, static_cast<int64_t>(m), reached, -1.0, d_out + m, out.deff);
             }
         }
         const cudaError_t err = cudaStreamSynchronize(g->stream);
@@ -126,7 +147,20 @@ int ngx_brandes(ngx_graph* graph, const ngx_apsp_opts* opts, double* bc, ngx_aps
         if (graph == nullptr || opts == nullptr || (bc == nullptr && graph->n > 0)) {
             return fail(NGX_INVALID_ARGUMENT, "ngx_brandes: graph, opts or bc is NULL");
         }
-        return dag_run(graph, opts, kModeBrandes, result, bc, nullptr, nullptr);
+        DagHostOut out;
+        out.bc = bc;
+        return dag_run(graph, opts, kModeBrandes, result, out);
+    });
+}
+
+int ngx_brandes_fixed(ngx_graph* graph, const ngx_apsp_opts* opts, uint64_t* bc_fixed, ngx_apsp_result* result) {
+    return guard_host("ngx_brandes_fixed", [&]() -> int {
+        if (graph == nullptr || opts == nullptr || (bc_fixed == nullptr && graph->n > 0)) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_brandes_fixed: graph, opts or bc_fixed is NULL");
+        }
+        DagHostOut out;
+        out.bc_fixed = bc_fixed;
+        return dag_run(graph, opts, kModeBrandes, result, out);
     });
 }
 
@@ -135,7 +169,36 @@ int ngx_apsp_grad(ngx_graph* graph, const ngx_apsp_opts* opts, double* dcpl, dou
         if (graph == nullptr || opts == nullptr || ((dcpl == nullptr || deff == nullptr) && graph->m_user > 0)) {
             return fail(NGX_INVALID_ARGUMENT, "ngx_apsp_grad: graph, opts, dcpl or deff is NULL");
         }
-        return dag_run(graph, opts, kModeGrad, result, nullptr, dcpl, deff);
+        DagHostOut out;
+        out.dcpl = dcpl;
+        out.deff = deff;
+        return dag_run(graph, opts, kModeGrad, result, out);
+    });
+}
+
+int ngx_apsp_grad_fixed(ngx_graph* graph, const ngx_apsp_opts* opts, uint64_t* dcpl_fixed, uint64_t* deff_fixed, ngx_apsp_result* result) {
+    return guard_host("ngx_apsp_grad_fixed", [&]() -> int {
+        if (graph == nullptr || opts == nullptr || ((dcpl_fixed == nullptr || deff_fixed == nullptr) && graph->m_user > 0)) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_apsp_grad_fixed: graph, opts, dcpl_fixed or deff_fixed is NULL");
+        }
+        DagHostOut out;
+        out.dcpl_fixed = dcpl_fixed;
+        out.deff_fixed = deff_fixed;
+        return dag_run(graph, opts, kModeGrad, result, out);
+    });
+}
+
+int ngx_fixed_to_double(const uint64_t* words, int64_t count, double divisor, double sign, double* out) {
+    return guard_host("ngx_fixed_to_double", [&]() -> int {
+        if (count < 0 || (count > 0 && (words == nullptr || out == nullptr))) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_fixed_to_double: negative count or NULL array");
+        }
+        for (int64_t i = 0; i < count; ++i) {
+            // the same expression as fixed_to_double_kernel, so a merged sum converts to the bits of a single run
+            const double v = fixed_value(words[2 * i], words[2 * i + 1]);
+            out[i] = divisor == 1.0 ? sign * v : sign * v / divisor;
+        }
+        return NGX_OK;
     });
 }
 

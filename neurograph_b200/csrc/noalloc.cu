@@ -5,16 +5,20 @@
 // and loops with a latency bound, where cudaFree would synchronize the whole device. For them this entry point runs
 // the batched APSP tile kernel (the one ngx_apsp uses) with every device buffer - outputs, sources and the per-slot
 // delta-stepping workspace - carved from one fixed array of NGX_NOALLOC_SCRATCH_BYTES defined in this file. The graph
-// handle itself was allocated when it was created; this call allocates nothing further, on the device or the host.
+// handle itself was allocated when it was created; this call allocates no device memory, and host memory only to build
+// an error message.
 //
 // Because there is one array per device, calls that overlap on the same device (two host threads, or two handles on
 // one device used at once) race on it and corrupt each other's results: serialize them.
+//
+// The array's device address is looked up on every call, with the graph's device current: the lookup allocates
+// nothing, and a cached address would go stale if the caller reset the device (cudaDeviceReset) and the library's
+// device code were loaded again at another address.
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "ngx_common.cuh"
@@ -25,45 +29,29 @@ namespace ngx {
 namespace {
 
 constexpr size_t kScratchBytes = NGX_NOALLOC_SCRATCH_BYTES;
-constexpr int kMaxDevices = 64;
 constexpr int64_t kChunk = 4096;  // sources staged per host -> device copy
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-std::mutex g_setup_mutex;
-void* g_scratch_ptr[kMaxDevices] = {};
-
 size_t align256(size_t bytes) { return (bytes + 255) & ~size_t(255); }
 
-// The device address of this device's scratch array, resolved once per device (the current device must be `device`).
-int scratch_for_device(int device, void** out) {
-    if (device < 0 || device >= kMaxDevices) {
-        return fail(NGX_UNSUPPORTED, "ngx_apsp_noalloc: device ordinal " + std::to_string(device) + " is beyond the supported 64 devices");
+// The device address of the current device's scratch array.
+int scratch_address(void** out) {
+    void* ptr = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&ptr, g_scratch);
+    if (err != cudaSuccess) {
+        return cuda_fail(err, "ngx_apsp_noalloc: cudaGetSymbolAddress of the scratch array");
     }
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (g_scratch_ptr[device] == nullptr) {
-        void* ptr = nullptr;
-        const cudaError_t err = cudaGetSymbolAddress(&ptr, g_scratch);
-        if (err != cudaSuccess) {
-            return cuda_fail(err, "ngx_apsp_noalloc: cudaGetSymbolAddress of the scratch array");
-        }
-        if ((reinterpret_cast<uintptr_t>(ptr) & 255u) != 0u) {
-            return fail(NGX_CUDA_ERROR, "ngx_apsp_noalloc: the scratch array is not 256-byte aligned");
-        }
-        g_scratch_ptr[device] = ptr;
+    if ((reinterpret_cast<uintptr_t>(ptr) & 255u) != 0u) {
+        return fail(NGX_CUDA_ERROR, "ngx_apsp_noalloc: the scratch array is not 256-byte aligned");
     }
-    *out = g_scratch_ptr[device];
+    *out = ptr;
     return NGX_OK;
 }
 
 }  // namespace
-}  // namespace ngx
 
-using namespace ngx;
-
-extern "C" {
-
-int ngx_apsp_noalloc(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result) {
+int run_apsp_noalloc(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result) {
     if (const int rc = check_opts(g, opts); rc != NGX_OK) {
         return rc;
     }
@@ -102,7 +90,7 @@ int ngx_apsp_noalloc(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* r
     }
     NGX_CUDA_TRY(cudaSetDevice(g->device));
     void* scratch = nullptr;
-    if (const int rc = scratch_for_device(g->device, &scratch); rc != NGX_OK) {
+    if (const int rc = scratch_address(&scratch); rc != NGX_OK) {
         return rc;
     }
     *g->h_abort = 0;
@@ -195,6 +183,14 @@ int ngx_apsp_noalloc(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* r
     }
     NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
     return NGX_OK;
+}
+
+}  // namespace ngx
+
+extern "C" {
+
+int ngx_apsp_noalloc(ngx_graph* graph, const ngx_apsp_opts* opts, ngx_apsp_result* result) {
+    return ngx::guard_host("ngx_apsp_noalloc", [&]() -> int { return ngx::run_apsp_noalloc(graph, opts, result); });
 }
 
 }  // extern "C"

@@ -1,7 +1,8 @@
 // C++20 host-side adapter between neurograph's DistributedGraph / metric classes and the neurograph-b200 C ABI.
 //
-// Header-only; a maintainer includes it from the reference's metric headers. It mirrors the
-// reference's own interfaces:
+// Header-only; a maintainer includes it from the reference's metric headers, where the new GPU enum values are
+// dispatched (AllPairsShortestPath::compute_apsp_impl, BetweennessCentrality::compute_average_betweenness_centrality).
+// It mirrors the reference's own interfaces:
 //   compute_apsp_gpu<distance_type>          AllPairsShortestPath::compute_apsp           (AllPairsShortestPath.h:54-57)
 //   compute_apsp_gpu<inverse_distance_type>  AllPairsShortestPath::compute_apsp_inverse   (AllPairsShortestPath.h:76-79)
 //   compute_average_betweenness_gpu          BetweennessCentrality::compute_average_betweenness_centrality

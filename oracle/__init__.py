@@ -28,7 +28,19 @@ RESTATEMENT_SO = os.path.join(HERE, "libngx_oracle.so")
 REFERENCE_SO = os.path.join(HERE, "_ref", "libngx_ref.so")
 REFERENCE_GTESTS = os.path.join(HERE, "_ref", "ref_gtests")
 INTEGRATION_CHECK = os.path.join(HERE, "_ref", "integration_check")
-REFERENCE_SOURCES = os.environ.get("NGX_REFERENCE_DIR", "/root/reference")
+REFERENCE_DIR_RECORD = os.path.join(HERE, "_ref", "reference_dir.txt")
+
+
+def _reference_sources() -> str | None:
+    """The reference source tree: $NGX_REFERENCE_DIR, else the tree the reference build was made from."""
+    path = os.environ.get("NGX_REFERENCE_DIR")
+    if not path and os.path.exists(REFERENCE_DIR_RECORD):
+        with open(REFERENCE_DIR_RECORD) as f:
+            path = f.read().strip()
+    return path if path and os.path.isdir(os.path.join(path, "source")) else None
+
+
+REFERENCE_SOURCES = _reference_sources()
 
 METRIC_REGULAR = 0
 METRIC_INVERSE = 1
@@ -39,16 +51,19 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 
 
-def build(reference: bool | None = None, quiet: bool = True) -> None:
-    """Compile the restatement and, when the reference sources exist here, the reference harness."""
+def build(reference_dir: str | None = None, quiet: bool = True) -> None:
+    """Compile the restatement and, when `reference_dir` (or $NGX_REFERENCE_DIR) holds the reference sources, the
+    reference harness built from them."""
+    global REFERENCE_SOURCES
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", HERE, "restatement"], check=True, stdout=out)
-    if reference is None:
-        reference = os.path.isdir(os.path.join(REFERENCE_SOURCES, "source"))
-    if reference:
-        subprocess.run(["make", "-C", HERE, "-j8", "reference", f"REF={REFERENCE_SOURCES}"], check=True, stdout=out)
+    ref = reference_dir or os.environ.get("NGX_REFERENCE_DIR")
+    if ref and os.path.isdir(os.path.join(ref, "source")):
+        ref = os.path.abspath(ref)
+        subprocess.run(["make", "-C", HERE, "-j8", "reference", f"REF={ref}"], check=True, stdout=out)
         if os.path.exists(os.path.join(os.path.dirname(HERE), "neurograph_b200", "lib", "libngx_b200.so")):
-            subprocess.run(["make", "-C", HERE, "integration", f"REF={REFERENCE_SOURCES}"], check=True, stdout=out)
+            subprocess.run(["make", "-C", HERE, "integration", f"REF={ref}"], check=True, stdout=out)
+        REFERENCE_SOURCES = _reference_sources() or ref
 
 
 class _Graph(C.Structure):
@@ -199,6 +214,55 @@ class Restatement:
         if rc != 0:
             raise ValueError(f"ngxo_apsp_grad failed ({rc})")
         return dcpl[: g.m], deff[: g.m], _totals_dict(totals)
+
+
+def _chunks(sources, threads: int) -> list[np.ndarray]:
+    srcs = np.ascontiguousarray(sources, dtype=np.int64)
+    parts = max(1, min(int(threads) if threads else (os.cpu_count() or 1), srcs.size))
+    return [c for c in np.array_split(srcs, parts) if c.size]
+
+
+def _pool_map(fn, items, threads: int):
+    """fn over items on host threads (the C calls release the interpreter lock), in item order."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max(1, int(threads) if threads else (os.cpu_count() or 1))) as ex:
+        return list(ex.map(fn, items))
+
+
+class ParallelRestatement(Restatement):
+    """The restatement over a source list on host threads, for parity checks on large graphs. Every per-source value
+    is computed exactly as by the sequential calls; only totals that sum over sources (betweenness, gradients) are
+    combined in another order (relative differences of a few units in the last place)."""
+
+    def __init__(self, threads: int = 0, path: str = RESTATEMENT_SO):
+        super().__init__(path)
+        self.threads = threads
+
+    def sssp_rows(self, g: Csr, sources, metric: int = METRIC_REGULAR) -> np.ndarray:
+        return np.stack(_pool_map(lambda s: self.sssp(g, int(s), metric), list(sources), self.threads))
+
+    def apsp_sources(self, g: Csr, sources, metric: int = METRIC_REGULAR, bins: int = 0, hist_max: float = 0.0) -> dict:
+        """Per-source summaries (bit-identical to apsp()'s), histogram, overflow, unreachable and traversed arcs."""
+        parts = _pool_map(lambda c: self.apsp(g, c, metric, bins, hist_max), _chunks(sources, self.threads), self.threads)
+        per = {k: np.concatenate([p["per_source"][k] for p in parts]) for k in parts[0]["per_source"]}
+        out = {"per_source": per, "hist": None if bins <= 0 else np.sum([p["hist"] for p in parts], axis=0).astype(np.uint64)}
+        for key in ("unreachable", "reached_pairs", "traversed_arcs", "hist_overflow"):
+            out[key] = int(sum(int(p[key]) for p in parts))
+        out["diameter"] = max(p["diameter"] for p in parts)
+        return out
+
+    def brandes_sources(self, g: Csr, sources) -> np.ndarray:
+        return np.sum(_pool_map(lambda c: self.brandes(g, c), _chunks(sources, self.threads), self.threads), axis=0)
+
+    def apsp_grad_sources(self, g: Csr, sources=None):
+        """(dcpl, deff, reached_pairs): each chunk's gradient scaled back by its own R and divided by the total R."""
+        srcs = np.arange(g.n) if sources is None else sources
+        parts = _pool_map(lambda c: self.apsp_grad(g, c), _chunks(srcs, self.threads), self.threads)
+        total = sum(int(p[2]["reached_pairs"]) for p in parts)
+        dcpl = np.sum([p[0] * float(p[2]["reached_pairs"]) for p in parts], axis=0) / float(total)
+        deff = np.sum([p[1] * float(p[2]["reached_pairs"]) for p in parts], axis=0) / float(total)
+        return dcpl, deff, total
 
 
 def _scc_summary(component: np.ndarray) -> dict:

@@ -1,7 +1,7 @@
 /*
  * Integration check (test infrastructure): the reference's own one-rank fixture graphs, built by its own fixture
  * code, go through the reference's AllPairsShortestPath / BetweennessCentrality and through the C++20 adapter
- * neurograph_b200/host/ngx_neurograph.h that a maintainer would call from those classes (INTEGRATION.md). The results
+ * neurograph_b200/host/ngx_neurograph.h that a maintainer would call from those classes. The results
  * must agree: CPL, diameter, unreachable pairs and cluster sizes exactly, efficiency within the reference's rounding,
  * average betweenness within 1e-12 relative, strongly connected components exactly. Exit code 0 when every fixture agrees. Needs a B200.
  */

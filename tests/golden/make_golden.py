@@ -30,7 +30,9 @@ sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
 
-SAMPLE_INPUT = os.path.join(oracle.REFERENCE_SOURCES, "input", "rank_1_nodes_5000_arcs_6")
+# the reference project's source tree: $NGX_REFERENCE_DIR, or where this machine keeps it
+REFERENCE_DIR = oracle.REFERENCE_SOURCES or os.environ.get("NGX_REFERENCE_DIR", "/root/reference")
+SAMPLE_INPUT = os.path.join(REFERENCE_DIR, "input", "rank_1_nodes_5000_arcs_6")
 
 # Golden values from the reference's test suite (paths relative to the reference project).
 EXPECTATIONS = {
@@ -135,7 +137,7 @@ def _record(ref: oracle.Reference, prefix: str, graph: oracle.RefGraph, out: dic
 
 
 def main() -> None:
-    oracle.build(reference=True)
+    oracle.build(reference_dir=REFERENCE_DIR)
     ref = oracle.Reference()
     out: dict[str, np.ndarray] = {}
     names = []

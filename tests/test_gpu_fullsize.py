@@ -1,10 +1,10 @@
 """Parity at the benchmark's full size (connectome N=100000, ~9.9M arcs, log-normal FP64 weights).
 
-The oracle is too slow for all 1e5 sources, so this checks a seeded sample of sources against it (per-source exact
-sums, maxima, unreachable and traversed-arc counts bit for bit; betweenness of the sample within 1e-12 relative), and
-size-independent properties of a full wave of 9,472 sources: the exact sums of disjoint chunks merge to the sum of the
-whole wave, per-source sums add up to the wave total exactly (a checksum of checksums), and a repeated run gives the
-same bits.
+The oracle is too slow for all 1e5 sources, so this checks 64 seeded sources against it, on host threads: the full
+distance rows bit for bit, the per-source exact sums, maxima, unreachable and traversed-arc counts and the 1024-bin
+histogram bit for bit, and the betweenness of those sources within 1e-12 relative. A full wave of 9,472 sources is
+checked through size-independent properties: the exact sums of disjoint chunks merge to the sum of the whole wave,
+per-source sums add up to the wave total (a checksum of checksums), and a repeated run gives the same bits.
 """
 
 from __future__ import annotations
@@ -33,19 +33,24 @@ def graph():
     return c
 
 
-def test_sampled_sources_match_the_oracle(graph, restatement):
+def test_sampled_sources_match_the_oracle(graph):
     c = graph
     csr = oracle.Csr.from_arrays(c.n, c.row_ptr, c.col, c.w)
-    sample = np.random.default_rng(7).choice(c.n, size=3, replace=False)
-    want = restatement.apsp(csr, sources=sample, bins=1024, hist_max=2.0)
+    sample = np.random.default_rng(7).choice(c.n, size=64, replace=False)
+    check = oracle.ParallelRestatement()
+    want_rows = check.sssp_rows(csr, sample)
+    want = check.apsp_sources(csr, sample, bins=1024, hist_max=2.0)
+    want_bc = check.brandes_sources(csr, sample)
     with ngx.Graph(c.n, c.row_ptr, c.col, c.w) as g:
+        rows = g.sssp_rows(sample)
         got = g.apsp(sources=sample, per_source=True, hist_bins=1024, hist_max=2.0)
         bc, _ = g.brandes(sources=sample)
+    assert np.array_equal(rows, want_rows)
     for k in ("sum", "sum_inv", "max", "unreachable", "arcs"):
         assert np.array_equal(got.per_source[k], want["per_source"][k]), k
-    assert got.sum_distances == want["sum_distances"] and got.sum_inverse == want["sum_inverse"]
     assert np.array_equal(got.hist, want["hist"]) and got.hist_overflow == want["hist_overflow"]
-    want_bc = restatement.brandes(csr, sources=sample)
+    assert got.unreachable == want["unreachable"] and got.traversed_arcs == want["traversed_arcs"]
+    assert got.diameter == want["diameter"]
     floor = REL * max(1.0, float(np.abs(want_bc).mean()))
     assert np.all(np.abs(bc - want_bc) <= np.maximum(REL * np.abs(want_bc), floor))
 

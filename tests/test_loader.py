@@ -19,7 +19,7 @@ import neurograph_b200 as ngx
 import oracle
 
 FLAGS = list(itertools.product([False, True], repeat=3))
-SAMPLE = os.path.join(oracle.REFERENCE_SOURCES, "input", "rank_1_nodes_5000_arcs_6")
+SAMPLE = os.path.join(oracle.REFERENCE_SOURCES or "", "input", "rank_1_nodes_5000_arcs_6")
 
 
 def triples(n, row_ptr, col, w):

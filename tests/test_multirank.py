@@ -123,5 +123,72 @@ def _bench_helpers(rank, world):
     assert bench.reduce_over_ranks(dist, 1.5 + rank, "sum", "cpu") == sum(1.5 + r for r in range(world))
 
 
+def _fixed_words(values) -> list[int]:
+    """The library's 128-bit fixed point of non-negative doubles (value * 2^64, fraction truncated), as Python ints."""
+    out = []
+    for x in values:
+        x = float(x)
+        if not x > 0.0:
+            out.append(0)
+            continue
+        whole = math.floor(x)
+        out.append((int(whole) << 64) + int(math.ldexp(x - whole, 64)))
+    return out
+
+
+def _pack(ints) -> np.ndarray:
+    mask = (1 << 64) - 1
+    return np.array([[v & mask, (v >> 64) & mask] for v in ints], dtype=np.uint64).reshape(-1, 2)
+
+
+def _random_words(rank, count=3000):
+    rng = np.random.default_rng(200 + rank)
+    words = rng.integers(0, 1 << 63, size=(count, 2), dtype=np.uint64) * np.uint64(2) + np.uint64(1)
+    words[:10] = np.uint64(0xFFFFFFFFFFFFFFFF)  # carries through every limb, and the modulo-2^128 wrap
+    words[10:20, 1] = 0
+    return words
+
+
+def _fixed_merge(rank, world):
+    merged = sharded.merge_fixed(_random_words(rank), dist)
+    want = [0] * merged.shape[0]
+    for r in range(world):
+        for i, (lo, hi) in enumerate(_random_words(r).tolist()):
+            want[i] = (want[i] + lo + (hi << 64)) % (1 << 128)
+    assert np.array_equal(merged, _pack(want))
+
+
+def test_fixed_point_sums_merge_over_ranks():
+    _spawn(_fixed_merge)
+
+
+def _brandes_merge(rank, world):
+    """Each rank's betweenness words, as the library forms them (per-source dependencies truncated to fixed point and
+    summed exactly), from the oracle's per-source dependencies; the merged words equal the all-sources words."""
+    oracle.build()
+    restatement = oracle.Restatement()
+    c, csr = _graph()
+    per_source = [restatement.brandes(csr, sources=[s]) for s in range(c.n)]
+
+    def words_of(sources):
+        total = [0] * c.n
+        for s in sources:
+            for v, x in enumerate(_fixed_words(per_source[s])):
+                total[v] += x
+        return total
+
+    mine = sharded.shard_sources(c.n, rank, world)
+    merged = sharded.merge_fixed(_pack(words_of(mine)), dist)
+    whole = words_of(range(c.n))
+    assert np.array_equal(merged, _pack(whole))
+    bc = ngx.fixed_to_double(merged)
+    want = restatement.brandes(csr)
+    assert np.all(np.abs(bc - want) <= 1e-12 * np.maximum(np.abs(want), 1.0))
+
+
+def test_sharded_betweenness_words_equal_the_single_run():
+    _spawn(_brandes_merge)
+
+
 def test_bench_sharding_and_timing_reductions():
     _spawn(_bench_helpers)

@@ -66,6 +66,19 @@ def test_source_subset_and_no_optional_outputs():
         same(r, bare_want, "all sources, summaries only")
 
 
+def test_largest_graph_with_few_workspace_slots():
+    """At the vertex limit a workspace slot is ~9.2 MB, so only three fit beside the outputs: ten source tiles then
+    reuse each slot several times, as they never do on the smaller graphs above."""
+    c = synth.random_graph(ngx_limit(), 3, weights="lognormal", seed=27)
+    sources = np.random.default_rng(8).choice(c.n, size=300, replace=False)
+    kw = dict(sources=sources, per_source=True, hist_bins=256, hist_max=20.0)
+    with ngx.Graph(c.n, c.row_ptr, c.col, c.w) as g:
+        want = g.apsp(**kw)
+        got = [g.apsp_noalloc(**kw) for _ in range(2)]
+    for r in got:
+        same(r, want, "n = 32768")
+
+
 def test_limits_are_rejected():
     big = synth.random_graph(ngx_limit() + 1, 1, weights="int", seed=25)
     with ngx.Graph(big.n, big.row_ptr, big.col, big.w) as g:
