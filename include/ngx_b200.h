@@ -152,8 +152,30 @@ NGX_API const char* ngx_last_error(void);
 /* Library build identifier (compute capability the kernels were built for, CUDA version). */
 NGX_API const char* ngx_version(void);
 
-/* Validates and uploads the graph to `device`, building the device CSR and reverse CSR. */
+/* Validates and uploads the graph to `device`, building the device CSR and reverse CSR on the GPU: the caller's arcs
+ * are checked, zero weights dropped and both arc lengths written by device kernels, and the reverse CSR comes from a
+ * stable device sort of the stored arcs by target (replaces DistributedGraph::construct_graph's window construction,
+ * source/graph/DistributedGraph.cpp:154-250). */
 NGX_API int ngx_graph_create(const ngx_csr* csr, int device, ngx_graph** out);
+
+#define NGX_BUILD_ON_HOST 1 /* ngx_graph_create_ex: build the arrays on host threads and upload them */
+/* ngx_graph_create with flags (0 or NGX_BUILD_ON_HOST); both builds give bit-identical device arrays. */
+NGX_API int ngx_graph_create_ex(const ngx_csr* csr, int device, int flags, ngx_graph** out);
+
+/* One stored arc as the device holds it (16 bytes): forward CSR {target, caller arc index, length}; reverse CSR
+ * {source, stored forward index, |w|}. */
+typedef struct {
+    int32_t col;
+    int32_t id;
+    double len;
+} ngx_arc;
+
+/* Copies a handle's device arrays to host arrays (any pointer may be NULL): row_ptr and rrow_ptr n + 1 entries per
+ * graph (global stored-arc offsets), arcs (|w| lengths), arcs_inverse (1/|w|), rarcs and arc_src (source vertex of
+ * each stored arc) m_stored entries, mean_lengths[2] = the mean |w| and 1/|w| that default bucket widths derive from.
+ * m_stored = row_ptr[n] of the last graph. No reference counterpart (inspection of DistributedGraph's windows). */
+NGX_API int ngx_graph_layout(const ngx_graph* graph, int64_t* row_ptr, ngx_arc* arcs, ngx_arc* arcs_inverse, int64_t* rrow_ptr,
+                             ngx_arc* rarcs, int32_t* arc_src, double* mean_lengths);
 NGX_API void ngx_graph_destroy(ngx_graph* graph);
 NGX_API int ngx_graph_size(const ngx_graph* graph, int64_t* n, int64_t* m);
 /* Asks an in-flight run on this graph to stop at its next phase boundary; the run returns NGX_ABORTED. */

@@ -34,6 +34,7 @@ METRICS = {"regular": 0, "inverse": 1}
 MODES = {"batched": 0, "plain": 1}
 TASKS = {"apsp": 0, "brandes": 1, "grad": 2}
 SIZE_CLASSES = 32
+BUILD_ON_HOST = 1
 TILE = 32
 ACC_DIGITS = 72
 
@@ -101,6 +102,8 @@ def library() -> C.CDLL:
         lib.ngx_last_error.restype = C.c_char_p
         lib.ngx_version.restype = C.c_char_p
         lib.ngx_graph_create.argtypes = [C.POINTER(_Csr), C.c_int, C.POINTER(C.c_void_p)]
+        lib.ngx_graph_create_ex.argtypes = [C.POINTER(_Csr), C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        lib.ngx_graph_layout.argtypes = [C.c_void_p] + [C.c_void_p] * 7
         lib.ngx_graph_destroy.argtypes = [C.c_void_p]
         lib.ngx_graph_destroy.restype = None
         lib.ngx_graph_size.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
@@ -179,7 +182,9 @@ class ApspResult:
 class Graph:
     """A graph resident on one GPU (device CSR + reverse CSR)."""
 
-    def __init__(self, n: int, row_ptr, col, w, device: int = 0):
+    def __init__(self, n: int, row_ptr, col, w, device: int = 0, build: str = "device"):
+        """build: "device" (the arrays are built by GPU kernels, the default) or "host" (host threads, then uploaded);
+        both give the same arrays bit for bit."""
         lib = library()
         self.n = int(n)
         self.row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
@@ -189,8 +194,29 @@ class Graph:
         csr = _Csr(self.n, self.m, self.row_ptr.ctypes.data, self.col.ctypes.data if self.m else None,
                    self.w.ctypes.data if self.m else None)
         handle = C.c_void_p()
-        _check(lib.ngx_graph_create(C.byref(csr), int(device), C.byref(handle)))
+        if build not in ("device", "host"):
+            raise ValueError(f"unknown build {build!r}")
+        _check(lib.ngx_graph_create_ex(C.byref(csr), int(device), BUILD_ON_HOST if build == "host" else 0, C.byref(handle)))
         self._handle = handle
+
+    def layout(self) -> dict:
+        """The handle's device arrays (ngx_graph_layout): row_ptr, arcs / arcs_inverse / rarcs as (col, id, len)
+        record arrays, rrow_ptr, arc_src and the mean lengths."""
+        m = int(self._stored_arcs())
+        rec = np.dtype([("col", np.int32), ("id", np.int32), ("len", np.float64)])
+        out = {"row_ptr": np.zeros(self.n + 1, np.int64), "rrow_ptr": np.zeros(self.n + 1, np.int64),
+               "arcs": np.zeros(max(m, 1), rec), "arcs_inverse": np.zeros(max(m, 1), rec), "rarcs": np.zeros(max(m, 1), rec),
+               "arc_src": np.zeros(max(m, 1), np.int32), "mean_lengths": np.zeros(2)}
+        _check(library().ngx_graph_layout(self._handle, *(out[k].ctypes.data for k in
+                                                          ("row_ptr", "arcs", "arcs_inverse", "rrow_ptr", "rarcs", "arc_src", "mean_lengths"))))
+        for k in ("arcs", "arcs_inverse", "rarcs", "arc_src"):
+            out[k] = out[k][:m]
+        return out
+
+    def _stored_arcs(self) -> int:
+        rows = np.zeros(self.n + 1, np.int64)
+        _check(library().ngx_graph_layout(self._handle, rows.ctypes.data, None, None, None, None, None, None))
+        return int(rows[-1])
 
     @classmethod
     def from_network(cls, directory: str, number_ranks: int, file_prefix: str = "", remove_self_arcs: bool = False,

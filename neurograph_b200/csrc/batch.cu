@@ -443,6 +443,9 @@ int ngx_graph_update_weights(ngx_graph* g, const double* w) {
             return fail(NGX_INVALID_ARGUMENT, "ngx_graph_update_weights: graph or w is NULL");
         }
         NGX_CUDA_TRY(cudaSetDevice(g->device));
+        if (const int rc = ensure_stored_of_user(g); rc != NGX_OK) {
+            return rc;
+        }
         const size_t m = static_cast<size_t>(g->m_stored);
         std::vector<Arc> regular(m), inverse(m), rarcs(m);
         NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));

@@ -173,6 +173,7 @@ void release(ngx_graph* g) {
     cudaFree(g->d_rrow_ptr);
     cudaFree(g->d_rarcs);
     cudaFree(g->d_arc_src);
+    cudaFree(g->d_stored_of_user);
     cudaFree(g->d_workspace);
     cudaFree(g->d_items);
     cudaFree(g->d_persistent);
@@ -542,7 +543,7 @@ int build_host_graphs(const ngx_csr* csrs, int64_t count, int threads, HostGraph
     return NGX_OK;
 }
 
-int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** out) {
+int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** out, bool on_host) {
     if (out == nullptr) {
         return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: out is NULL");
     }
@@ -550,9 +551,21 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
     if (csrs == nullptr || count <= 0) {
         return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: no graphs");
     }
-    // the input is checked (and laid out) before the device, so that a bad graph is reported as such anywhere
+    // the input is checked (and, on the host path, laid out) before the device, so that a bad graph is reported as
+    // such anywhere
+    // the device build needs a usable device; without one the host path checks the graph and reports what is wrong
+    int devices = 0;
+    const bool have_device = cudaGetDeviceCount(&devices) == cudaSuccess && device >= 0 && device < devices;
+    if (!have_device) {
+        cudaGetLastError();
+    }
+    const bool on_device = !on_host && have_device && count == 1 && csrs[0].n > 0;
     HostGraphs h;
-    if (const int rc = build_host_graphs(csrs, count, 0, &h); rc != NGX_OK) {
+    if (on_device) {
+        if (const int rc = validate_rows(&csrs[0]); rc != NGX_OK) {
+            return rc;
+        }
+    } else if (const int rc = build_host_graphs(csrs, count, 0, &h); rc != NGX_OK) {
         return rc;
     }
     int device_count = 0;
@@ -573,18 +586,20 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
     }
     g->device = device;
     g->sm_count = prop.multiProcessorCount;
-    g->n_total = h.n_total;
-    g->m_user = h.m_user;
-    g->n = h.n_max;
-    g->m_stored = static_cast<int64_t>(h.regular.size());
-    g->parts = std::move(h.parts);
-    g->stored_of_user = std::move(h.stored_of_user);
-    g->source_order = std::move(h.source_order);
-    g->max_out_degree = h.max_out_degree;
-    g->mean_len_regular = h.mean_len_regular;
-    g->mean_len_inverse = h.mean_len_inverse;
-    g->min_len_regular = h.min_len_regular;
-    g->max_len_regular = h.max_len_regular;
+    if (!on_device) {
+        g->n_total = h.n_total;
+        g->m_user = h.m_user;
+        g->n = h.n_max;
+        g->m_stored = static_cast<int64_t>(h.regular.size());
+        g->parts = std::move(h.parts);
+        g->stored_of_user = std::move(h.stored_of_user);
+        g->source_order = std::move(h.source_order);
+        g->max_out_degree = h.max_out_degree;
+        g->mean_len_regular = h.mean_len_regular;
+        g->mean_len_inverse = h.mean_len_inverse;
+        g->min_len_regular = h.min_len_regular;
+        g->max_len_regular = h.max_len_regular;
+    }
 
     const auto finish = [&](int rc) -> int {
         if (rc != NGX_OK) {
@@ -602,6 +617,9 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
     }
     *g->h_abort = 0;
     g->stream = g->own_stream;
+    if (on_device) {
+        return finish(build_graph_on_device(&csrs[0], g));
+    }
 
     const auto upload = [&](auto** dst, const auto& src) -> int {
         using T = std::remove_cv_t<std::remove_reference_t<decltype(src[0])>>;
@@ -627,6 +645,44 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
     return finish(rc);
 }
 
+int ensure_source_order(ngx_graph* g) {
+    if (static_cast<int64_t>(g->source_order.size()) == g->n_total) {
+        return NGX_OK;
+    }
+    if (g->parts.size() != 1) {
+        return fail(NGX_INVALID_ARGUMENT, "a batch handle without its source order");
+    }
+    // the forward CSR back from the device, then the same order the host build computes
+    const int64_t n = g->n;
+    std::vector<int64_t> rows(static_cast<size_t>(n) + 1);
+    HostVector<Arc> arcs(static_cast<size_t>(g->m_stored));
+    NGX_CUDA_TRY(cudaSetDevice(g->device));
+    NGX_CUDA_TRY(cudaMemcpyAsync(rows.data(), g->d_row_ptr, rows.size() * 8, cudaMemcpyDeviceToHost, g->stream));
+    if (!arcs.empty()) {
+        NGX_CUDA_TRY(cudaMemcpyAsync(arcs.data(), g->d_arcs_regular, arcs.size() * sizeof(Arc), cudaMemcpyDeviceToHost, g->stream));
+    }
+    NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    HostVector<int32_t> order;
+    order.reserve(static_cast<size_t>(n));
+    append_source_order(n, rows.data(), arcs.data(), order);
+    g->source_order = std::move(order);
+    return NGX_OK;
+}
+
+int ensure_stored_of_user(ngx_graph* g) {
+    if (static_cast<int64_t>(g->stored_of_user.size()) == g->m_user || g->d_stored_of_user == nullptr) {
+        return NGX_OK;
+    }
+    HostVector<int32_t> map(static_cast<size_t>(g->m_user));
+    NGX_CUDA_TRY(cudaSetDevice(g->device));
+    if (!map.empty()) {
+        NGX_CUDA_TRY(cudaMemcpyAsync(map.data(), g->d_stored_of_user, map.size() * 4, cudaMemcpyDeviceToHost, g->stream));
+        NGX_CUDA_TRY(cudaStreamSynchronize(g->stream));
+    }
+    g->stored_of_user = std::move(map);
+    return NGX_OK;
+}
+
 }  // namespace ngx
 
 using namespace ngx;
@@ -647,13 +703,19 @@ const char* ngx_status_string(int status) {
 }
 
 int ngx_graph_source_order(const ngx_graph* graph, int64_t* order) {
-    if (graph == nullptr || (order == nullptr && graph->n_total > 0)) {
-        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_source_order: graph or order is NULL");
-    }
-    for (size_t i = 0; i < graph->source_order.size(); ++i) {
-        order[i] = graph->source_order[i];
-    }
-    return NGX_OK;
+    return guard_host("ngx_graph_source_order", [&]() -> int {
+        if (graph == nullptr || (order == nullptr && graph->n_total > 0)) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_graph_source_order: graph or order is NULL");
+        }
+        // computed on first use for a device-built handle (a cache, not a change of the graph)
+        if (const int rc = ensure_source_order(const_cast<ngx_graph*>(graph)); rc != NGX_OK) {
+            return rc;
+        }
+        for (size_t i = 0; i < graph->source_order.size(); ++i) {
+            order[i] = graph->source_order[i];
+        }
+        return NGX_OK;
+    });
 }
 
 const char* ngx_last_error(void) { return last_error_message.c_str(); }
@@ -673,6 +735,52 @@ int ngx_graph_create(const ngx_csr* csr, int device, ngx_graph** out) {
             return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create: csr is NULL");
         }
         return create_graphs(csr, 1, device, out);
+    });
+}
+
+int ngx_graph_create_ex(const ngx_csr* csr, int device, int flags, ngx_graph** out) {
+    return guard_host("ngx_graph_create_ex", [&]() -> int {
+        if (csr == nullptr) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create_ex: csr is NULL");
+        }
+        if ((flags & ~NGX_BUILD_ON_HOST) != 0) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_graph_create_ex: unknown flags");
+        }
+        return create_graphs(csr, 1, device, out, (flags & NGX_BUILD_ON_HOST) != 0);
+    });
+}
+
+int ngx_graph_layout(const ngx_graph* graph, int64_t* row_ptr, ngx_arc* arcs, ngx_arc* arcs_inverse, int64_t* rrow_ptr, ngx_arc* rarcs,
+                     int32_t* arc_src, double* mean_lengths) {
+    return guard_host("ngx_graph_layout", [&]() -> int {
+        if (graph == nullptr) {
+            return fail(NGX_INVALID_ARGUMENT, "ngx_graph_layout: graph is NULL");
+        }
+        static_assert(sizeof(ngx_arc) == sizeof(Arc), "ngx_arc mirrors the device arc record");
+        NGX_CUDA_TRY(cudaSetDevice(graph->device));
+        const size_t rows = static_cast<size_t>(graph->n_total + static_cast<int64_t>(graph->parts.size()));
+        const size_t m = static_cast<size_t>(graph->m_stored);
+        const auto get = [&](void* dst, const void* src, size_t bytes) -> int {
+            if (dst != nullptr && bytes > 0) {
+                NGX_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, graph->stream));
+            }
+            return NGX_OK;
+        };
+        int rc = get(row_ptr, graph->d_row_ptr, rows * 8);
+        if (rc == NGX_OK) rc = get(arcs, graph->d_arcs_regular, m * sizeof(Arc));
+        if (rc == NGX_OK) rc = get(arcs_inverse, graph->d_arcs_inverse, m * sizeof(Arc));
+        if (rc == NGX_OK) rc = get(rrow_ptr, graph->d_rrow_ptr, rows * 8);
+        if (rc == NGX_OK) rc = get(rarcs, graph->d_rarcs, m * sizeof(Arc));
+        if (rc == NGX_OK) rc = get(arc_src, graph->d_arc_src, m * 4);
+        if (rc != NGX_OK) {
+            return rc;
+        }
+        NGX_CUDA_TRY(cudaStreamSynchronize(graph->stream));
+        if (mean_lengths != nullptr) {
+            mean_lengths[0] = graph->mean_len_regular;
+            mean_lengths[1] = graph->mean_len_inverse;
+        }
+        return NGX_OK;
     });
 }
 

@@ -69,6 +69,7 @@ struct ngx_graph {
     int64_t* d_rrow_ptr = nullptr;
     ngx::Arc* d_rarcs = nullptr;
     int32_t* d_arc_src = nullptr;  // source vertex (graph-local) of each stored forward arc
+    int32_t* d_stored_of_user = nullptr;  // device build: stored index of each caller arc (-1 for zero weights)
 
     double mean_len_regular = 1.0;
     double mean_len_inverse = 1.0;
@@ -102,7 +103,8 @@ struct ngx_graph {
 
     // bucket width per size class (floor(log2 n)), as a multiple of each graph's mean arc length (ngx_batch_autotune)
     double class_scale[64] = {};
-    // stored forward index of each caller arc (-1 for zero weights), for ngx_graph_update_weights
+    // stored forward index of each caller arc (-1 for zero weights), for ngx_graph_update_weights (a device-built
+    // handle copies it from d_stored_of_user on first use)
     ngx::HostVector<int32_t> stored_of_user;
     // all-sources processing order of each graph (graph-local ids, graph after graph): clusters of nearby vertices,
     // so that the 32 sources of a tile reach most vertices in the same phases and share arc passes
@@ -141,8 +143,18 @@ struct HostGraphs {
 // CUDA calls. The result does not depend on the number of threads.
 int build_host_graphs(const ngx_csr* csrs, int64_t count, int threads, HostGraphs* out);
 
-// Validates and uploads `count` CSRs into one handle (concatenated device CSR + reverse CSR).
-int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** out);
+// Validates and uploads `count` CSRs into one handle (concatenated device CSR + reverse CSR). A single graph is built
+// on the device (build_graph_on_device) unless `on_host`; batches are built on host threads.
+int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** out, bool on_host = false);
+
+// Device build of one graph whose rows passed the host checks, into g (device, stream and sm_count already set).
+int build_graph_on_device(const ngx_csr* csr, ngx_graph* g);
+
+// The all-sources order of a single-graph handle, computed from its device arrays when a run first needs it.
+int ensure_source_order(ngx_graph* g);
+
+// Copies a device-built handle's stored index of every caller arc to the host (ngx_graph_update_weights needs it).
+int ensure_stored_of_user(ngx_graph* g);
 
 // Grows the graph's cached workspace to at least `bytes`.
 int ensure_workspace(ngx_graph* g, size_t bytes);

@@ -555,6 +555,11 @@ int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, d
     // all sources: in the graph's locality order (tiles of nearby sources), results scattered back by vertex;
     // distance rows keep vertex order
     const int32_t* scatter = nullptr;
+    if (opts->sources == nullptr && rows == nullptr) {
+        if (const int rc = ensure_source_order(g); rc != NGX_OK) {
+            return rc;
+        }
+    }
     if (opts->sources == nullptr && rows == nullptr && g->source_order.size() == sources.size()) {
         sources.assign(g->source_order.begin(), g->source_order.end());
         scatter = g->source_order.data();
