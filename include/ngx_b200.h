@@ -96,6 +96,8 @@ typedef struct {
     int64_t hist_bins;       /* bins of the shortest-path distance histogram; 0 = no histogram */
     double hist_max;         /* exclusive upper bound of the histogram; <= 0 = sampled eccentricity x 1.5 */
     uint64_t max_iterations; /* cap on delta-stepping phases per source tile; 0 = 4 * n + 64 */
+    int tile_ctas;           /* CTAs that work on one source tile together (batched form; 1 to 512); 0 picks 1, or more
+                                when the device memory affords fewer workspace slots than there are resident CTAs */
 } ngx_apsp_opts;
 
 /* Totals over all requested sources; per-source arrays are optional caller-allocated host arrays (NULL to skip). */
@@ -273,6 +275,7 @@ typedef struct {
     double hist_max;        /* histogram bound, the same for all graphs; must be > 0 when hist_bins > 0 */
     int use_cuda_graph;     /* capture the run (output reset + launch) and replay it while these options are unchanged */
     uint64_t max_iterations;/* cap on phases per source tile; 0 = 4 * n + 64 of the largest graph */
+    int tile_ctas;          /* CTAs per source tile, as in ngx_apsp_opts */
 } ngx_batch_opts;
 
 /* Validates and uploads `count` CSRs into one handle. Vertex and arc numbering stays per graph in every output. */

@@ -55,7 +55,7 @@ class _Opts(C.Structure):
     _fields_ = [
         ("metric", C.c_int), ("mode", C.c_int), ("sources", C.c_void_p), ("num_sources", C.c_int64),
         ("delta", C.c_double), ("block_threads", C.c_int), ("ctas_per_sm", C.c_int), ("hist_bins", C.c_int64),
-        ("hist_max", C.c_double), ("max_iterations", C.c_uint64),
+        ("hist_max", C.c_double), ("max_iterations", C.c_uint64), ("tile_ctas", C.c_int),
     ]
 
 
@@ -63,6 +63,7 @@ class _BatchOpts(C.Structure):
     _fields_ = [
         ("task", C.c_int), ("metric", C.c_int), ("delta_scale", C.c_double), ("block_threads", C.c_int),
         ("hist_bins", C.c_int64), ("hist_max", C.c_double), ("use_cuda_graph", C.c_int), ("max_iterations", C.c_uint64),
+        ("tile_ctas", C.c_int),
     ]
 
 
@@ -299,14 +300,14 @@ class Graph:
         _check(library().ngx_graph_update_weights(self._handle, w.ctypes.data if self.m else None))
         self.w = w
 
-    def _opts(self, sources, metric, mode, delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations):
+    def _opts(self, sources, metric, mode, delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations, tile_ctas=0):
         srcs = None if sources is None else np.ascontiguousarray(sources, dtype=np.int64)
         opts = _Opts(
             METRICS[metric] if isinstance(metric, str) else int(metric),
             MODES[mode] if isinstance(mode, str) else int(mode),
             None if srcs is None else srcs.ctypes.data,
             0 if srcs is None else srcs.size,
-            float(delta), int(block_threads), int(ctas_per_sm), int(hist_bins), float(hist_max), int(max_iterations),
+            float(delta), int(block_threads), int(ctas_per_sm), int(hist_bins), float(hist_max), int(max_iterations), int(tile_ctas),
         )
         k = self.n if srcs is None else srcs.size
         return opts, srcs, k
@@ -345,9 +346,10 @@ class Graph:
         return r, hist, per
 
     def apsp(self, sources=None, metric="regular", mode="batched", delta=0.0, hist_bins=0, hist_max=0.0,
-             per_source=False, block_threads=0, ctas_per_sm=0, max_iterations=0, exact=False) -> ApspResult:
-        """exact=True also returns the unrounded exact sums (acc_digits), for merging the runs of several ranks."""
-        opts, srcs, k = self._opts(sources, metric, mode, delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations)
+             per_source=False, block_threads=0, ctas_per_sm=0, max_iterations=0, exact=False, tile_ctas=0) -> ApspResult:
+        """exact=True also returns the unrounded exact sums (acc_digits), for merging the runs of several ranks.
+        tile_ctas: CTAs that work on one source tile together (0 = the library's choice)."""
+        opts, srcs, k = self._opts(sources, metric, mode, delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations, tile_ctas)
         r, hist, per = self._result_struct(hist_bins, per_source, k, exact)
         _check(library().ngx_apsp(self._handle, C.byref(opts), C.byref(r)))
         out = self._result(r, hist, per, k)
@@ -364,17 +366,18 @@ class Graph:
         _check(library().ngx_apsp_noalloc(self._handle, C.byref(opts), C.byref(r)))
         return self._result(r, hist, per, k)
 
-    def sssp_rows(self, sources, metric="regular", mode="batched", delta=0.0) -> np.ndarray:
-        opts, srcs, k = self._opts(sources, metric, mode, delta, 0, 0.0, 0, 0, 0)
+    def sssp_rows(self, sources, metric="regular", mode="batched", delta=0.0, tile_ctas=0) -> np.ndarray:
+        opts, srcs, k = self._opts(sources, metric, mode, delta, 0, 0.0, 0, 0, 0, tile_ctas)
         rows = np.zeros((k, self.n), np.float64)
         _check(library().ngx_sssp_rows(self._handle, C.byref(opts), rows.ctypes.data))
         return rows
 
     def brandes(self, sources=None, delta=0.0, hist_bins=0, hist_max=0.0, per_source=False, block_threads=0,
-                ctas_per_sm=0, max_iterations=0, fixed=False, exact=False):
+                ctas_per_sm=0, max_iterations=0, fixed=False, exact=False, tile_ctas=0):
         """Betweenness (sum of pair dependencies over the sources) and the run's APSP result. fixed=True returns the
         unconverted sums instead (ngx_brandes_fixed): an (n, 2) uint64 array of 128-bit fixed-point words."""
-        opts, srcs, k = self._opts(sources, "regular", "batched", delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations)
+        opts, srcs, k = self._opts(sources, "regular", "batched", delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations,
+                                   tile_ctas)
         r, hist, per = self._result_struct(hist_bins, per_source, k, exact)
         if fixed:
             words = np.zeros((max(self.n, 1), 2), np.uint64)
@@ -389,10 +392,10 @@ class Graph:
             out.acc_digits = r._digits
         return bc, out
 
-    def apsp_grad(self, sources=None, delta=0.0, block_threads=0, ctas_per_sm=0, max_iterations=0, fixed=False):
+    def apsp_grad(self, sources=None, delta=0.0, block_threads=0, ctas_per_sm=0, max_iterations=0, fixed=False, tile_ctas=0):
         """Gradients of CPL and efficiency w.r.t. every arc length, and the run's APSP result. fixed=True returns the
         unconverted sums instead (ngx_apsp_grad_fixed): two (m, 2) uint64 arrays, before the division by R."""
-        opts, srcs, k = self._opts(sources, "regular", "batched", delta, 0, 0.0, block_threads, ctas_per_sm, max_iterations)
+        opts, srcs, k = self._opts(sources, "regular", "batched", delta, 0, 0.0, block_threads, ctas_per_sm, max_iterations, tile_ctas)
         r, hist, per = self._result_struct(0, False, k)
         if fixed:
             dcpl = np.zeros((max(self.m, 1), 2), np.uint64)
@@ -445,12 +448,13 @@ class Batch:
         _check(library().ngx_graph_set_stream(self._handle, stream_handle))
 
     def run(self, task="apsp", metric="regular", delta_scale=0.0, hist_bins=0, hist_max=0.0, per_source=False,
-            use_cuda_graph=False, block_threads=0, max_iterations=0):
+            use_cuda_graph=False, block_threads=0, max_iterations=0, tile_ctas=0):
         """Runs `task` for every graph. Returns (results, extra): a list of ApspResult and, per graph, the betweenness
         vector (task "brandes"), the (dcpl, deff) pair (task "grad") or None."""
         t = TASKS[task] if isinstance(task, str) else int(task)
         opts = _BatchOpts(t, METRICS[metric] if isinstance(metric, str) else int(metric), float(delta_scale),
-                          int(block_threads), int(hist_bins), float(hist_max), int(bool(use_cuda_graph)), int(max_iterations))
+                          int(block_threads), int(hist_bins), float(hist_max), int(bool(use_cuda_graph)), int(max_iterations),
+                          int(tile_ctas))
         count = len(self.graphs)
         structs = (_Result * max(1, count))()
         keep = []

@@ -90,6 +90,7 @@ uint64_t options_key(const ngx_batch_opts* o, const ngx_graph* g) {
     std::memcpy(&bits, &o->delta_scale, 8);
     h = mix(h, bits);
     h = mix(h, static_cast<uint64_t>(o->block_threads));
+    h = mix(h, static_cast<uint64_t>(o->tile_ctas));
     h = mix(h, static_cast<uint64_t>(o->hist_bins));
     std::memcpy(&bits, &o->hist_max, 8);
     h = mix(h, bits);
@@ -159,6 +160,7 @@ int ngx_batch_run(ngx_graph* g, const ngx_batch_opts* opts, ngx_apsp_result* res
         aopts.metric = opts->metric;
         aopts.mode = NGX_MODE_BATCHED;
         aopts.block_threads = opts->block_threads;
+        aopts.tile_ctas = opts->tile_ctas;
         aopts.max_iterations = opts->max_iterations;
         if (const int rc = check_opts(g, &aopts); rc != NGX_OK) {
             return rc;

@@ -139,7 +139,7 @@ __device__ __forceinline__ void brandes_sigma_vertex(const DeviceCsr& g, const D
                 const unsigned long long dvs = __shfl_sync(0xFFFFFFFFu, rank_dv, w.r);
                 double contrib = 0.0;
                 if (w.a < deg) {
-                    const Arc arc = arcs[w.a];
+                    const Arc arc = ldg_arc(&arcs[w.a]);
                     const int64_t urow = static_cast<int64_t>(arc.col) * kTile + s;
                     const unsigned long long du = __ldcg(&dist[urow]);
                     if (du != kInfBits && on_dag(du, arc.len, dvs)) {
@@ -179,7 +179,7 @@ __device__ __forceinline__ void brandes_sigma_vertex(const DeviceCsr& g, const D
             len[u] = 0.0;
             dx[u] = kInfBits;
             if (w.a < deg) {
-                const Arc arc = arcs[w.a];
+                const Arc arc = ldg_arc(&arcs[w.a]);
                 x[u] = arc.col;
                 len[u] = arc.len;
                 dx[u] = __ldcg(&dist[static_cast<int64_t>(x[u]) * kTile + s[u]]);
@@ -257,7 +257,7 @@ __device__ __forceinline__ void brandes_delta_vertex(const DeviceCsr& g, int v, 
             len[u] = 0.0;
             dx[u] = kInfBits;
             if (w.a < deg) {
-                const Arc arc = arcs[w.a];
+                const Arc arc = ldg_arc(&arcs[w.a]);
                 x[u] = arc.col;
                 id[u] = arc.id;
                 len[u] = arc.len;
@@ -313,7 +313,7 @@ __device__ __forceinline__ void dag_count_scan(const DeviceCsr& rg, int64_t v, u
         const int cntr = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
         Arc a{ 0, 0, 0.0 };
         if (lane < cntr) {
-            a = rg.arcs[e0 + lane];
+            a = ldg_arc(&rg.arcs[e0 + lane]);
         }
         for (int j = 0; j < cntr; j += 4) {
             unsigned long long du[4];
@@ -384,7 +384,7 @@ __device__ __forceinline__ void dag_count(const DeviceCsr& g, const DeviceCsr& r
             a[i] = Arc{ -1, 0, 0.0 };
             u[i] = 0;
             if (fast[i]) {
-                a[i] = g.arcs[e[i]];
+                a[i] = ldg_arc(&g.arcs[e[i]]);
                 u[i] = __ldg(&arc_src[e[i]]);
             }
         }
@@ -421,43 +421,6 @@ __device__ __forceinline__ void dag_count(const DeviceCsr& g, const DeviceCsr& r
     if (lane == 0 && active_count != 0ull) {
         atomicAdd(active_pairs, active_count);
     }
-}
-
-// Exclusive prefix sum of in[0..len) into out[0..len] (out[len] = total) by one CTA; returns the total to every thread.
-__device__ __forceinline__ unsigned long long block_exclusive_scan(const uint32_t* in, uint32_t* out, int64_t len, unsigned long long* s_part) {
-    const int tid = threadIdx.x;
-    const int nthreads = blockDim.x;
-    const int64_t chunk = (len + nthreads - 1) / nthreads;
-    const int64_t beg = tid * chunk < len ? tid * chunk : len;
-    const int64_t end = beg + chunk < len ? beg + chunk : len;
-    unsigned long long sum = 0;
-    for (int64_t i = beg; i < end; ++i) {
-        sum += __ldcg(&in[i]);
-    }
-    s_part[tid] = sum;
-    __syncthreads();
-    if (tid == 0) {
-        unsigned long long run = 0;
-        for (int t = 0; t < nthreads; ++t) {
-            const unsigned long long x = s_part[t];
-            s_part[t] = run;
-            run += x;
-        }
-        s_part[nthreads] = run;
-    }
-    __syncthreads();
-    unsigned long long run = s_part[tid];
-    for (int64_t i = beg; i < end; ++i) {
-        const uint32_t x = __ldcg(&in[i]);
-        out[i] = static_cast<uint32_t>(run);
-        run += x;
-    }
-    const unsigned long long total = s_part[nthreads];
-    if (tid == 0) {
-        out[len] = static_cast<uint32_t>(total);
-    }
-    __syncthreads();
-    return total;
 }
 
 template <bool kTarget>
@@ -519,7 +482,7 @@ __device__ __forceinline__ void dag_fill_scan(const DeviceCsr& rg, int64_t v, bo
             const int cntr = static_cast<int>(end - e0 < 32 ? end - e0 : 32);
             Arc a{ 0, 0, 0.0 };
             if (lane < cntr) {
-                a = rg.arcs[e0 + lane];
+                a = ldg_arc(&rg.arcs[e0 + lane]);
             }
             for (int j = 0; j < cntr; j += 4) {
                 unsigned long long du[4];
@@ -546,16 +509,17 @@ __device__ __forceinline__ void dag_fill_scan(const DeviceCsr& rg, int64_t v, bo
     }
 }
 
-// Sorts each successor list by its entries (the fill order depends on timing; the sums must not).
-__device__ __forceinline__ void dag_sort(const uint32_t* soff, uint32_t* succ, int64_t nt) {
-    for (int64_t i = threadIdx.x; i < nt; i += blockDim.x) {
+// Sorts each successor list by its entries (the fill order depends on timing; the sums must not). Lists are spread
+// over the threads of the group: thread `first` of `stride` takes lists first, first + stride, ...
+__device__ __forceinline__ void dag_sort(const uint32_t* soff, uint32_t* succ, int64_t nt, int64_t first, int64_t stride) {
+    for (int64_t i = first; i < nt; i += stride) {
         const uint32_t beg = __ldcg(&soff[i]);
         const uint32_t end = __ldcg(&soff[i + 1]);
         for (uint32_t a = beg + 1; a < end; ++a) {
-            const uint32_t key = succ[a];
+            const uint32_t key = __ldcg(&succ[a]);
             uint32_t b = a;
-            while (b > beg && succ[b - 1] > key) {
-                succ[b] = succ[b - 1];
+            while (b > beg && __ldcg(&succ[b - 1]) > key) {
+                succ[b] = __ldcg(&succ[b - 1]);
                 --b;
             }
             succ[b] = key;
@@ -640,7 +604,7 @@ __device__ __forceinline__ void dag_sigma_level(const DeviceCsr& g, const int32_
                 x[u] = 0;
                 if (ok[u]) {
                     const uint32_t e = __ldcg(&succ[j]);
-                    x[u] = kTarget ? e : static_cast<uint32_t>(g.arcs[e].col);
+                    x[u] = kTarget ? e : static_cast<uint32_t>(ldg_arc(&g.arcs[e]).col);
                 }
             }
 #pragma unroll
@@ -705,7 +669,7 @@ __device__ __forceinline__ void dag_tree_level(const DeviceCsr& g, const int32_t
                 x[u] = 0;
                 if (ok[u]) {
                     const uint32_t e = __ldcg(&succ[j]);
-                    x[u] = kTarget ? e : static_cast<uint32_t>(g.arcs[e].col);
+                    x[u] = kTarget ? e : static_cast<uint32_t>(ldg_arc(&g.arcs[e]).col);
                 }
             }
 #pragma unroll
@@ -726,10 +690,10 @@ __device__ __forceinline__ void dag_tree_level(const DeviceCsr& g, const int32_t
 template <int kMode, bool kTree>
 __device__ __forceinline__ void dag_delta_level(const DeviceCsr& g, const int32_t* entries, int len, const unsigned long long* dist, const double* sigma,
                                                 double* delta, double* delta_g, const uint32_t* soff, const uint32_t* succ, unsigned long long* grad_cpl,
-                                                unsigned long long* grad_eff, double* buf, int lane, int warp, int nwarps) {
+                                                unsigned long long* grad_eff, double* buf, int lane, int buf_warp, int warp, int nwarps) {
     constexpr bool kTarget = kMode == kModeBrandes;
     constexpr int kU = delta_level_unroll(kMode);
-    double* const wbuf = buf + static_cast<size_t>(warp) * 32 * kU * (kMode == kModeGrad ? 2 : 1);
+    double* const wbuf = buf + static_cast<size_t>(buf_warp) * 32 * kU * (kMode == kModeGrad ? 2 : 1);
     for (int base = warp * 32; base < len; base += nwarps * 32) {
         const int i = base + lane;
         uint32_t entry = 0, beg = 0, count = 0;
@@ -766,7 +730,7 @@ __device__ __forceinline__ void dag_delta_level(const DeviceCsr& g, const int32_
                     const uint32_t e = __ldcg(&succ[j]);
                     uint32_t x = e;
                     if constexpr (!kTarget) {
-                        const Arc arc = g.arcs[e];
+                        const Arc arc = ldg_arc(&g.arcs[e]);
                         x = static_cast<uint32_t>(arc.col);
                         id[u] = arc.id;
                     }

@@ -25,6 +25,16 @@ struct __align__(16) Arc {
 };
 static_assert(sizeof(Arc) == 16, "Arc must be 16 bytes");
 
+// Arc records are read-only while a kernel runs: loaded through the read-only data path (L1 kept), one 128-bit load.
+__device__ __forceinline__ Arc ldg_arc(const Arc* p) {
+    const int4 v = __ldg(reinterpret_cast<const int4*>(p));
+    Arc a;
+    a.col = v.x;
+    a.id = v.y;
+    a.len = __hiloint2double(v.w, v.z);
+    return a;
+}
+
 struct DeviceCsr {
     int64_t n;
     int64_t m;               // stored (non-zero-weight) arcs

@@ -23,6 +23,7 @@ namespace {
 constexpr int kBatchedUnroll = 4;
 constexpr int kPlainWarpsMax = 16;
 constexpr int kBatchedDefaultBlock = 512;
+constexpr int kMaxGroupSize = 512;  // CTAs sharing one tile at most (above any SM count x resident CTAs per SM used here)
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 }  // namespace
@@ -69,6 +70,9 @@ int check_opts(const ngx_graph* g, const ngx_apsp_opts* opts) {
     }
     if (opts->hist_bins < 0 || opts->hist_bins > kMaxHistBins) {
         return fail(NGX_INVALID_ARGUMENT, "hist_bins must be in [0, " + std::to_string(kMaxHistBins) + "]");
+    }
+    if (opts->tile_ctas < 0 || opts->tile_ctas > kMaxGroupSize) {
+        return fail(NGX_INVALID_ARGUMENT, "tile_ctas must be in [0, " + std::to_string(kMaxGroupSize) + "]");
     }
     if (opts->block_threads != 0 && (opts->block_threads < 64 || opts->block_threads > 512 || opts->block_threads % 32 != 0)) {
         return fail(NGX_INVALID_ARGUMENT, "block_threads must be a multiple of 32 in [64, 512]");
@@ -161,6 +165,35 @@ const void* tile_kernel_for_block(int block, int ctas_per_sm = 0) {
     }
 }
 
+// CTAs per tile group: the caller's choice, else 1 unless the device memory affords fewer workspace slots than there
+// are resident CTAs (and tiles to fill them), in which case each slot gets enough CTAs to use every SM.
+int choose_group_size(int requested, int64_t resident, int64_t num_tiles, int64_t affordable_slots) {
+    if (requested > 0) {
+        return static_cast<int>(std::min<int64_t>({ static_cast<int64_t>(requested), resident, static_cast<int64_t>(kMaxGroupSize) }));
+    }
+    const int64_t busy = std::min(resident, num_tiles);  // CTAs a run of single-CTA tiles would keep busy
+    if (affordable_slots >= busy) {
+        return 1;
+    }
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(resident / std::max<int64_t>(1, affordable_slots), kMaxGroupSize)));
+}
+
+// Launches the tile kernel: cooperative when several CTAs share a tile (they wait for one another at group barriers,
+// so all of them must be resident at once).
+cudaError_t launch_tile_kernel(const void* kernel, int64_t grid, int block, size_t smem, cudaStream_t stream, int group_size, void** args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(static_cast<unsigned>(block));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = group_size > 1 ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, kernel, args);
+}
+
 int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const TileJob& job, int64_t hist_bins, double hist_max, RunOutputs& o,
                  DagOutputs* extra, float* kernel_ms, bool synchronous) {
     const bool batched = opts->mode == NGX_MODE_BATCHED || tile_mode != kModeApsp;
@@ -195,9 +228,15 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
         per_sm = std::min(per_sm, opts->ctas_per_sm);
     }
     const int64_t n = job.n_max;
-    const size_t slot_bytes = sssp_slot_bytes(n, width) + (tile_mode != kModeApsp ? brandes_slot_bytes(n, tile_mode == kModeGrad) : 0);
+    const int64_t resident = static_cast<int64_t>(g->sm_count) * per_sm;
+    const size_t data_bytes = sssp_slot_bytes(n, width) + (tile_mode != kModeApsp ? brandes_slot_bytes(n, tile_mode == kModeGrad) : 0);
     const size_t budget = workspace_budget(g);
-    int64_t slots = std::min<int64_t>(num_tiles, static_cast<int64_t>(g->sm_count) * per_sm);
+    // the group size decides the group storage per slot, which the slot count must leave room for
+    const int64_t affordable = static_cast<int64_t>(budget / (data_bytes + static_cast<size_t>(group_stride_words(kMaxGroupSize)) * 8));
+    const int group = batched ? choose_group_size(opts->tile_ctas, resident, num_tiles, affordable) : 1;
+    const size_t group_bytes = static_cast<size_t>(group_stride_words(group)) * 8;
+    const size_t slot_bytes = data_bytes + group_bytes;
+    int64_t slots = std::min<int64_t>(num_tiles, resident / group);
     slots = std::min<int64_t>(slots, static_cast<int64_t>(budget / slot_bytes));
     if (slots <= 0) {
         return fail(NGX_OUT_OF_MEMORY, "not enough device memory for one workspace slot (" + std::to_string(slot_bytes) + " bytes)");
@@ -206,6 +245,9 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
         return rc;
     }
     char* ws = static_cast<char*>(g->d_workspace);
+    // group storage first (256-byte aligned slots), then the slot arrays
+    unsigned long long* group_ws = reinterpret_cast<unsigned long long*>(ws);
+    ws += static_cast<size_t>(slots) * group_bytes;
     SsspParams p{};
     p.g = g->csr(opts->metric);
     p.g.n = n;
@@ -229,6 +271,9 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
     ws += static_cast<size_t>(slots) * 2 * n * 4;
     p.ws_stamp = reinterpret_cast<uint32_t*>(ws);
     ws += static_cast<size_t>(slots) * n * 4;
+    p.group_size = group;
+    p.group_stride = group_stride_words(group);
+    p.group_ws = group_ws;
     BrandesParams bp{};
     if (tile_mode != kModeApsp) {
         const size_t nt = static_cast<size_t>(n) * kTile;
@@ -293,7 +338,10 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
     cudaError_t err = cudaSuccess;
     if (batched) {
         void* args[] = { &p, &bp };
-        err = cudaLaunchKernel(kernel, dim3(static_cast<unsigned>(slots)), dim3(block), args, smem, g->stream);
+        err = cudaMemsetAsync(group_ws, 0, static_cast<size_t>(slots) * group_bytes, g->stream);
+        if (err == cudaSuccess) {
+            err = launch_tile_kernel(kernel, slots * group, block, smem, g->stream, group, args);
+        }
     } else {
         sssp_plain_kernel<<<static_cast<unsigned>(slots), block, smem, g->stream>>>(p);
         err = cudaGetLastError();
@@ -346,13 +394,16 @@ int launch_apsp_in_workspace(ngx_graph* g, const ngx_apsp_opts* opts, const Tile
         per_sm = std::min(per_sm, opts->ctas_per_sm);
     }
     const int64_t n = job.n_max;
-    const size_t slot_bytes = sssp_slot_bytes(n, kTile);
+    const size_t group_bytes = static_cast<size_t>(group_stride_words(1)) * 8;  // one CTA per tile
+    const size_t slot_bytes = sssp_slot_bytes(n, kTile) + group_bytes;
     int64_t slots = std::min<int64_t>(job.num_items, static_cast<int64_t>(g->sm_count) * per_sm);
     slots = std::min<int64_t>(slots, static_cast<int64_t>(ws_bytes / slot_bytes));
     if (slots <= 0) {
         return fail(NGX_OUT_OF_MEMORY, "the workspace holds no slot of " + std::to_string(slot_bytes) + " bytes");
     }
     char* w = static_cast<char*>(ws);
+    unsigned long long* group_ws = reinterpret_cast<unsigned long long*>(w);
+    w += static_cast<size_t>(slots) * group_bytes;
     SsspParams p{};
     p.g = g->csr(opts->metric);
     p.g.n = n;
@@ -375,6 +426,9 @@ int launch_apsp_in_workspace(ngx_graph* g, const ngx_apsp_opts* opts, const Tile
     p.ws_queue = reinterpret_cast<int32_t*>(w);
     w += static_cast<size_t>(slots) * 2 * n * 4;
     p.ws_stamp = reinterpret_cast<uint32_t*>(w);
+    p.group_size = 1;
+    p.group_stride = group_stride_words(1);
+    p.group_ws = group_ws;
     BrandesParams bp{};
     p.out.acc_sum = o.acc;
     p.out.acc_inv = o.acc + kAccDigits;
@@ -393,7 +447,10 @@ int launch_apsp_in_workspace(ngx_graph* g, const ngx_apsp_opts* opts, const Tile
         p.out.src_arcs = o.src_u64 + job.num_sources;
     }
     void* args[] = { &p, &bp };
-    const cudaError_t err = cudaLaunchKernel(kernel, dim3(static_cast<unsigned>(slots)), dim3(block), args, smem, g->stream);
+    cudaError_t err = cudaMemsetAsync(group_ws, 0, static_cast<size_t>(slots) * group_bytes, g->stream);
+    if (err == cudaSuccess) {
+        err = cudaLaunchKernel(kernel, dim3(static_cast<unsigned>(slots)), dim3(block), args, smem, g->stream);
+    }
     return err == cudaSuccess ? NGX_OK : cuda_fail(err, "tile kernel launch");
 }
 

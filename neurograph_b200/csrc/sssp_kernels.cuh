@@ -32,6 +32,7 @@
 
 #include "brandes_kernels.cuh"
 #include "ngx_common.cuh"
+#include "ngx_group.cuh"
 
 namespace ngx {
 
@@ -72,6 +73,10 @@ struct SsspParams {
     uint32_t* ws_far;              // slots * n
     int32_t* ws_queue;             // slots * 2n
     uint32_t* ws_stamp;            // slots * n
+    // groups: the CTAs blockIdx.x / group_size share slot (blockIdx.x / group_size) and its tiles
+    int group_size;
+    int64_t group_stride;          // words of group storage per slot (group_stride_words)
+    unsigned long long* group_ws;  // slots * group_stride words, zero at launch
     TileOutputs out;
 };
 
@@ -86,24 +91,65 @@ __device__ __forceinline__ double next_theta(double d_min, double delta) {
     return theta > d_min ? theta : INFINITY;
 }
 
-// Shared state of a CTA working on one tile.
+// Control block of the CTAs working on one tile: one per workspace slot in global memory, and a copy in each CTA's
+// shared memory that every group barrier refreshes (ngx_group.cuh). Only atomics and barrier updates change it.
 struct TileShared {
     long long tile;
     int qlen[2];
     int cur;
     int stop;
     unsigned stamp;                 // id of the iteration about to run (queue dedup)
+    int done;                       // bucket step: no pending far pair is left
     double theta;
+    double theta_next;              // bucket step: the bound below which pass 2 moves pairs to the near queue
     unsigned long long min_bits;
     unsigned long long iterations;
-    unsigned long long overflow;
+    unsigned long long overflow;    // histogram overflow of the tile (plain form)
     // Brandes / adjoint levels
     unsigned level;
     int lvl_start;
     int lvl_len;
     int next_len;
     unsigned long long active_pairs;  // reached (vertex, source) pairs other than the sources, counted by the DAG pass
+    int grab;                       // next queue entry handed to a warp in the current near iteration
+    int pad;
+    // the state of a CTA that left its group (ngx_group.cuh): no tile, nothing queued, pending or levelled
+    __device__ void halt() {
+        stop = 1;
+        tile = 0x7FFFFFFFFFFFFFFFll;
+        qlen[0] = 0;
+        qlen[1] = 0;
+        done = 1;
+        level = 0u;
+        lvl_start = 0;
+        lvl_len = 0;
+    }
 };
+static_assert(sizeof(TileShared) % 8 == 0, "TileShared is copied in 8-byte words");
+
+// Per-slot group storage, in 8-byte words: the control block, the barrier, one scan partial per CTA, and (groups of
+// several CTAs) the per-source epilogue sums: exact accumulators of d and 1/d, unreachable, arcs and maximum per source.
+constexpr int kCtlWords = static_cast<int>(sizeof(TileShared) / 8);
+constexpr int kGroupAccWords = 2 * kTile * kAccDigits + 3 * kTile;
+inline int64_t group_stride_words(int group_size) {
+    const int64_t words = kCtlWords + 1 + group_size + (group_size > 1 ? kGroupAccWords : 0);
+    return (words + 31) / 32 * 32;  // 256-byte aligned slots
+}
+
+// This CTA's view of its tile group (see SsspParams::group_*).
+template <typename Params>
+__device__ __forceinline__ Group<TileShared> tile_group(const Params& p) {
+    unsigned long long* const gws = p.group_ws + (blockIdx.x / p.group_size) * p.group_stride;
+    return Group<TileShared>{ reinterpret_cast<TileShared*>(gws), reinterpret_cast<GroupBarrier*>(gws + kCtlWords), gws + kCtlWords + 1,
+                              p.group_size, static_cast<int>(blockIdx.x % p.group_size), p.error };
+}
+
+// Queue entries a warp takes at a time: all 32 when the near queue is long, fewer towards the end of a frontier so
+// that the group's warps share it evenly.
+__device__ __forceinline__ int expand_chunk(int qlen, int group_warps) {
+    const int c = qlen / (2 * group_warps);
+    return c < 1 ? 1 : (c > 32 ? 32 : c);
+}
 
 // ------------------------------------------------------------------------------------------ batched form
 // Expands vertex v for the k sources pending on it. The deg(v) x k (arc, source) pairs are spread over the 32 lanes:
@@ -177,7 +223,7 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
             nd[u] = 0.0;
             cur[u] = 0ull;
             if (valid[u]) {
-                const Arc arc = arcs[a];
+                const Arc arc = ldg_arc(&arcs[a]);
                 x[u] = arc.col;
                 nd[u] = __dadd_rn(dvs, arc.len);
                 cur[u] = __ldcg(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]]);
@@ -232,22 +278,31 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
     }
 }
 
-// One near iteration of a tile: the warps take the queue 32 entries at a time; lane j fetches entry j's vertex, its
-// pending mask, far marks and row offsets (one round of parallel loads for 32 vertices), clears the mask and the
-// superseded far marks, and the warp then expands the 32 vertices one after another.
+// One near iteration of a tile: the warps of the group take the queue `chunk` entries at a time from a shared counter;
+// lane j fetches entry j's vertex, its pending mask, far marks and row offsets (one round of parallel loads), clears the
+// mask and the superseded far marks, and the warp then expands the vertices one after another.
 template <int kUnroll, bool kTrack>
-__device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* q_cur, int qlen, int lane, int warp, int nwarps,
+__device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* q_cur, int qlen, int lane, int* grab, int chunk,
                                              unsigned long long* __restrict__ dist, uint32_t* pend_cur, uint32_t* pend_nxt, uint32_t* far,
                                              int32_t* q_nxt, int* qlen_nxt, uint32_t* stamp, unsigned next_stamp, double theta,
                                              unsigned long long& expansions, unsigned long long& lane_expansions, unsigned long long* pred_key,
                                              uint32_t* tie, unsigned long long* last) {
-    for (int base = warp * 32; base < qlen; base += nwarps * 32) {
+    for (;;) {
+        int base = 0;
+        if (lane == 0) {
+            base = atomicAdd(grab, chunk);
+        }
+        base = __shfl_sync(kFullMask, base, 0);
+        if (base >= qlen) {
+            break;
+        }
         const int i = base + lane;
+        const int count = qlen - base < chunk ? qlen - base : chunk;
         int vj = 0;
         uint32_t mj = 0;
         int64_t bj = 0;
         int dj = 0;
-        if (i < qlen) {
+        if (lane < count) {
             vj = __ldcg(&q_cur[i]);
             mj = __ldcg(&pend_cur[vj]);
             const uint32_t fm = __ldcg(&far[vj]);
@@ -260,7 +315,6 @@ __device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* 
                 }
             }
         }
-        const int count = qlen - base < 32 ? qlen - base : 32;
         for (int j = 0; j < count; ++j) {
             const uint32_t amask = __shfl_sync(kFullMask, mj, j);
             if (amask == 0u) {
@@ -282,17 +336,27 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     unsigned long long* s_acc_inv = smem + kTile * kAccDigits;          // kTile * kAccDigits
     unsigned int* s_hist = reinterpret_cast<unsigned int*>(smem + 2 * kTile * kAccDigits);
     __shared__ TileShared s;
+    __shared__ unsigned s_bar;
     __shared__ int s_src[kTile];
     __shared__ unsigned long long s_unreach[kTile];
     __shared__ unsigned long long s_arcs[kTile];
     __shared__ unsigned long long s_max[kTile];
+    __shared__ unsigned long long s_part[kBlock + 3];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    const int nwarps = blockDim.x >> 5;
     const int64_t n_slot = p.g.n;  // every slot holds the largest graph of the batch
-    const int64_t slot = blockIdx.x;
+    // The CTAs blockIdx.x / group_size share workspace slot `slot` and work on its tiles together. The group's
+    // pointers and indices are recomputed from the launch parameters where they are used (fewer live registers).
+    const int64_t slot = blockIdx.x / p.group_size;
+    const auto grp = [&]() { return tile_group(p); };
+    const auto ctl = [&]() { return reinterpret_cast<TileShared*>(p.group_ws + (blockIdx.x / p.group_size) * p.group_stride); };
+    // this thread's (warp's) index among the group's threads (warps), and their counts
+#define NGX_GT (static_cast<int64_t>(blockIdx.x % p.group_size) * blockDim.x + threadIdx.x)
+#define NGX_GTHREADS (static_cast<int64_t>(p.group_size) * blockDim.x)
+#define NGX_GW (static_cast<int>(blockIdx.x % p.group_size) * static_cast<int>(blockDim.x >> 5) + static_cast<int>(threadIdx.x >> 5))
+#define NGX_GWARPS (p.group_size * static_cast<int>(blockDim.x >> 5))
     unsigned long long expansions = 0, lane_expansions = 0;
 
     unsigned long long* dist = p.ws_dist + slot * n_slot * kTile;
@@ -314,14 +378,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     uint32_t* soff = nullptr;
     uint32_t* succ = nullptr;
     uint32_t* tie = nullptr;
-    __shared__ unsigned long long s_part[kBlock + 1];
     if constexpr (kMode != kModeApsp) {
         scnt = b.ws_scnt + slot * nt_slot;
         soff = b.ws_soff + slot * (nt_slot + 1);
         succ = b.ws_succ + slot * b.succ_capacity;
-        for (int64_t i = tid; i < nt_slot; i += blockDim.x) {
-            scnt[i] = 0u;
-        }
         sigma = b.ws_sigma + slot * nt_slot;
         delta = b.ws_delta + slot * nt_slot;
         delta_g = kMode == kModeGrad ? b.ws_delta_g + slot * nt_slot : nullptr;
@@ -330,10 +390,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         list = b.ws_list + slot * nt_slot;
         loff = b.ws_loff + slot * (n_slot + 2);
         tie = b.ws_tie + slot * n_slot;
-        for (int64_t i = tid; i < n_slot; i += blockDim.x) {
+        for (int64_t i = NGX_GT; i < n_slot; i += NGX_GTHREADS) {
             tie[i] = 0u;
         }
-        for (int64_t i = tid; i < nt_slot; i += blockDim.x) {
+        for (int64_t i = NGX_GT; i < nt_slot; i += NGX_GTHREADS) {
+            scnt[i] = 0u;
             sigma[i] = __longlong_as_double(-1ll);  // all-ones: the empty predecessor key (sigma is zeroed by the count pass)
             delta[i] = __longlong_as_double(-1ll);  // all-ones: no expansion yet (delta holds last[][] in the SSSP phase)
             if constexpr (kMode == kModeGrad) {
@@ -344,10 +405,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         }
     }
 
-    for (int64_t i = tid; i < nt_slot; i += blockDim.x) {
+    for (int64_t i = NGX_GT; i < nt_slot; i += NGX_GTHREADS) {
         dist[i] = kInfBits;
     }
-    for (int64_t i = tid; i < n_slot; i += blockDim.x) {
+    for (int64_t i = NGX_GT; i < n_slot; i += NGX_GTHREADS) {
         pend0[i] = 0u;
         pend1[i] = 0u;
         far[i] = 0u;
@@ -360,21 +421,32 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         s_hist[i] = 0u;
     }
     if (tid == 0) {
-        s.stamp = 1u;
+        s_bar = 0u;
     }
-    __syncthreads();
+    bool first_tile = true;
 
     for (;;) {
-        if (tid == 0) {
-            s.tile = static_cast<long long>(atomicAdd(p.tile_counter, 1ull));
-            s.stop = (*reinterpret_cast<volatile int*>(p.error) != 0) ? 1 : 0;
-            s.qlen[0] = 0;
-            s.qlen[1] = 0;
-            s.cur = 0;
-            s.iterations = 0;
-            s.overflow = 0;
-        }
-        __syncthreads();
+        // ---- the next work item, taken for the whole group; the slot's queue stamp counts on across tiles
+        grp().sync(s, s_bar, [&](volatile TileShared& c) {
+            if (first_tile) {
+                c.stamp = 1u;
+            }
+            c.tile = static_cast<long long>(atomicAdd(p.tile_counter, 1ull));
+            c.stop = *reinterpret_cast<volatile int*>(p.error) != 0 ? 1 : 0;
+            c.qlen[0] = 0;
+            c.qlen[1] = 0;
+            c.cur = 0;
+            c.done = 0;
+            c.iterations = 0;
+            c.min_bits = kInfBits;
+            c.active_pairs = 0;
+            c.grab = 0;
+            if (c.tile < p.num_tiles) {
+                const WorkItem it = p.items != nullptr ? p.items[c.tile] : WorkItem{ 0, static_cast<int32_t>(c.tile) };
+                c.theta = p.graphs[it.graph].delta;
+            }
+        });
+        first_tile = false;
         if (s.stop != 0 || s.tile >= p.num_tiles) {
             break;
         }
@@ -393,9 +465,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         const int64_t tile_first = static_cast<int64_t>(item.tile) * kTile;
         const int64_t base = gd.src_off + tile_first;
         const int nsrc = static_cast<int>(gd.num_sources - tile_first < kTile ? gd.num_sources - tile_first : kTile);
-        if (tid == 0) {
-            s.theta = gd.delta;
-        }
         if (tid < kTile) {
             s_src[tid] = tid < nsrc ? p.sources[base + tid] : -1;
             s_unreach[tid] = 0ull;
@@ -403,17 +472,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             s_max[tid] = 0ull;
         }
         __syncthreads();
-        if (warp == 0) {
+        if (grp().rank == 0 && warp == 0) {
             const int v = s_src[lane];
             if (v >= 0) {
                 dist[static_cast<int64_t>(v) * kTile + lane] = 0ull;
                 atomicOr(&pend0[v], 1u << lane);
                 if (atomicExch(&stamp[v], s.stamp) != s.stamp) {
-                    q0[atomicAdd(&s.qlen[0], 1)] = v;
+                    q0[atomicAdd(&ctl()->qlen[0], 1)] = v;
                 }
             }
         }
-        __syncthreads();
+        grp().sync(s, s_bar);
 
         // ------------------------------------------------------------ delta-stepping over the tile
         long long t_phase = clock64();
@@ -430,25 +499,24 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 int32_t* q_nxt = cur ? q0 : q1;
                 const unsigned next_stamp = s.stamp + 1u;
                 const double theta = s.theta;
-                expand_queue<kUnroll, kMode != kModeApsp>(g, q_cur, qlen, lane, warp, nwarps, dist, pend_cur, pend_nxt, far, q_nxt,
-                                                          &s.qlen[cur ^ 1], stamp, next_stamp, theta, expansions, lane_expansions,
+                expand_queue<kUnroll, kMode != kModeApsp>(g, q_cur, qlen, lane, &ctl()->grab, expand_chunk(qlen, NGX_GWARPS), dist, pend_cur, pend_nxt,
+                                                          far, q_nxt, &ctl()->qlen[cur ^ 1], stamp, next_stamp, theta, expansions, lane_expansions,
                                                           reinterpret_cast<unsigned long long*>(sigma), tie,
                                                           reinterpret_cast<unsigned long long*>(delta));
-                __syncthreads();
-                if (tid == 0) {
-                    s.qlen[cur] = 0;
-                    s.cur = cur ^ 1;
-                    s.stamp = next_stamp;
-                    s.iterations += 1;
-                    if (s.iterations > p.max_iterations) {
+                grp().sync(s, s_bar, [&](volatile TileShared& c) {
+                    c.qlen[cur] = 0;
+                    c.cur = cur ^ 1;
+                    c.stamp = next_stamp;
+                    c.grab = 0;
+                    c.iterations = c.iterations + 1;
+                    if (c.iterations > p.max_iterations) {
                         atomicCAS(p.error, kDevOk, kDevTimeout);
-                        s.stop = 1;
+                        c.stop = 1;
                     } else if (*p.abort_flag != 0) {
                         atomicCAS(p.error, kDevOk, kDevAborted);
-                        s.stop = 1;
+                        c.stop = 1;
                     }
-                }
-                __syncthreads();
+                });
                 if (s.stop != 0) {
                     break;
                 }
@@ -456,13 +524,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             if (s.stop != 0) {
                 break;
             }
-            // bucket step, pass 1: smallest pending far distance
-            if (tid == 0) {
-                s.min_bits = kInfBits;
-            }
-            __syncthreads();
+            // bucket step, pass 1: smallest pending far distance (min_bits is +inf here: reset at the tile's start and
+            // after every bucket step)
             unsigned long long local_min = kInfBits;
-            for (int64_t vb = static_cast<int64_t>(warp) * 32; vb < n; vb += static_cast<int64_t>(nwarps) * 32) {
+            for (int64_t vb = static_cast<int64_t>(NGX_GW) * 32; vb < n; vb += static_cast<int64_t>(NGX_GWARPS) * 32) {
                 const int64_t v = vb + lane;
                 const uint32_t fm = v < n ? __ldcg(&far[v]) : 0u;
                 unsigned any = __ballot_sync(kFullMask, fm != 0u);
@@ -482,18 +547,24 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 local_min = o < local_min ? o : local_min;
             }
             if (lane == 0 && local_min != kInfBits) {
-                atomicMin(&s.min_bits, local_min);
+                atomicMin(&ctl()->min_bits, local_min);
             }
-            __syncthreads();
-            if (s.min_bits == kInfBits) {
-                break;  // nothing pending: the tile's distances are final
+            grp().sync(s, s_bar, [&](volatile TileShared& c) {
+                if (c.min_bits == kInfBits) {
+                    c.done = 1;  // nothing pending: the tile's distances are final
+                } else {
+                    c.theta_next = next_theta(__longlong_as_double(static_cast<long long>(c.min_bits)), gd.delta);
+                }
+            });
+            if (s.done != 0) {
+                break;
             }
-            const double theta = next_theta(__longlong_as_double(static_cast<long long>(s.min_bits)), gd.delta);
+            const double theta = s.theta_next;
             // pass 2: move the pairs below the new bound into the near queue of the next iteration
             const int cur = s.cur;
             uint32_t* pend_cur = cur ? pend1 : pend0;
             int32_t* q_cur = cur ? q1 : q0;
-            for (int64_t vb = static_cast<int64_t>(warp) * 32; vb < n; vb += static_cast<int64_t>(nwarps) * 32) {
+            for (int64_t vb = static_cast<int64_t>(NGX_GW) * 32; vb < n; vb += static_cast<int64_t>(NGX_GWARPS) * 32) {
                 const int64_t v = vb + lane;
                 const uint32_t fm = v < n ? __ldcg(&far[v]) : 0u;
                 unsigned any = __ballot_sync(kFullMask, fm != 0u);
@@ -510,15 +581,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                         const int64_t vv = vb + l;
                         far[vv] = f & ~nmask;
                         pend_cur[vv] = nmask;
-                        q_cur[atomicAdd(&s.qlen[cur], 1)] = static_cast<int32_t>(vv);
+                        q_cur[atomicAdd(&ctl()->qlen[cur], 1)] = static_cast<int32_t>(vv);
                     }
                 }
             }
-            __syncthreads();
-            if (tid == 0) {
-                s.theta = theta;
-            }
-            __syncthreads();
+            grp().sync(s, s_bar, [&](volatile TileShared& c) {
+                c.theta = c.theta_next;
+                c.min_bits = kInfBits;
+            });
         }
         if (s.stop != 0) {
             break;
@@ -533,56 +603,58 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             // ------------------------------------------------------------ shortest-path DAG: counts, sigma, delta
             // the level lists are built only after the successor lists: their storage holds pred[][] until then
             uint32_t* const pred = reinterpret_cast<uint32_t*>(list);
-            if (tid == 0) {
-                s.active_pairs = 0ull;
-            }
-            __syncthreads();
-            dag_count(g, rg, b.arc_src, b.m_total, n, nsrc, s_src, dist, tie, reinterpret_cast<unsigned long long*>(sigma), cnt, scnt, pred, lane, warp,
-                      nwarps, &s.active_pairs);
-            __syncthreads();
-            const unsigned long long dag_arcs = block_exclusive_scan(scnt, soff, nt, s_part);
+            dag_count(g, rg, b.arc_src, b.m_total, n, nsrc, s_src, dist, tie, reinterpret_cast<unsigned long long*>(sigma), cnt, scnt, pred, lane,
+                      NGX_GW, NGX_GWARPS, &ctl()->active_pairs);
+            grp().sync(s, s_bar);
+            const unsigned long long dag_arcs = group_exclusive_scan(grp(), s, s_bar, scnt, soff, nt, s_part);
             const bool use_lists = dag_arcs <= static_cast<unsigned long long>(b.succ_capacity);
-            for (int64_t i = tid; i < nt; i += blockDim.x) {
+            for (int64_t i = NGX_GT; i < nt; i += NGX_GTHREADS) {
                 scnt[i] = 0u;
             }
-            __syncthreads();
+            grp().sync(s, s_bar);
             if (use_lists) {
-                dag_fill<kMode == kModeBrandes>(rg, b.arc_src, n, dist, cnt, pred, soff, scnt, succ, lane, warp, nwarps);
-                __syncthreads();
-                dag_sort(soff, succ, nt);
-                __syncthreads();
+                dag_fill<kMode == kModeBrandes>(rg, b.arc_src, n, dist, cnt, pred, soff, scnt, succ, lane, NGX_GW, NGX_GWARPS);
+                grp().sync(s, s_bar);
+                dag_sort(soff, succ, nt, NGX_GT, NGX_GTHREADS);
             }
+            grp().sync(s, s_bar, [&](volatile TileShared& c) {
+                if (!use_lists) {
+                    c.stamp = c.stamp + 1u;
+                }
+                c.level = 0u;
+                c.lvl_start = 0;
+                c.lvl_len = 0;
+                c.next_len = 0;
+                loff[0] = 0;
+            });
             if (tid == 0) {
                 const long long now = clock64();
                 atomicAdd(&cnts[kCyclesCount], static_cast<unsigned long long>(now - t_phase));
                 t_phase = now;
-                if (!use_lists) {
+                if (!use_lists && grp().rank == 0) {
                     atomicAdd(&cnts[kDagScanTiles], 1ull);
                 }
             }
-          if (use_lists) {
-            // --- sigma and delta over the successor lists. When every reached pair has exactly one DAG predecessor
-            // (as many DAG arcs as reached non-source pairs) the DAGs are trees: every sigma is 1 and every child is
-            // released by its only parent, so the sigma levels need neither sums nor counts.
-            const bool tree = dag_arcs == s.active_pairs;
-            if (tid == 0) {
-                s.level = 0u;
-                s.lvl_start = 0;
-                s.lvl_len = 0;
-                s.next_len = 0;
-                loff[0] = 0;
-            }
-            __syncthreads();
-            if (warp == 0) {
+            // the sources form level 0
+            if (grp().rank == 0 && warp == 0) {
                 const int v = s_src[lane];
                 if (v >= 0) {
                     const int64_t row = static_cast<int64_t>(v) * kTile + lane;
                     lvl[row] = 0u;
                     sigma[row] = 1.0;
-                    list[atomicAdd(&s.lvl_len, 1)] = static_cast<int32_t>((static_cast<uint32_t>(v) << 5) | static_cast<uint32_t>(lane));
+                    if (use_lists) {
+                        list[atomicAdd(&ctl()->lvl_len, 1)] = static_cast<int32_t>((static_cast<uint32_t>(v) << 5) | static_cast<uint32_t>(lane));
+                    } else if (atomicExch(&stamp[v], s.stamp) != s.stamp) {
+                        list[atomicAdd(&ctl()->lvl_len, 1)] = v;
+                    }
                 }
             }
-            __syncthreads();
+            grp().sync(s, s_bar);
+          if (use_lists) {
+            // --- sigma and delta over the successor lists. When every reached pair has exactly one DAG predecessor
+            // (as many DAG arcs as reached non-source pairs) the DAGs are trees: every sigma is 1 and every child is
+            // released by its only parent, so the sigma levels need neither sums nor counts.
+            const bool tree = dag_arcs == s.active_pairs;
             for (;;) {
                 const int start = s.lvl_start;
                 const int len = s.lvl_len;
@@ -591,20 +663,19 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 }
                 const unsigned level = s.level;
                 if (tree) {
-                    dag_tree_level<kMode == kModeBrandes>(g, list + start, len, sigma, soff, succ, list + start + len, &s.next_len, lane, warp, nwarps);
+                    dag_tree_level<kMode == kModeBrandes>(g, list + start, len, sigma, soff, succ, list + start + len, &ctl()->next_len, lane, NGX_GW,
+                                                          NGX_GWARPS);
                 } else {
-                    dag_sigma_level<kMode == kModeBrandes>(g, list + start, len, level, sigma, cnt, lvl, soff, succ, list + start + len, &s.next_len,
-                                                           b.sigma_inexact, lane, warp, nwarps);
+                    dag_sigma_level<kMode == kModeBrandes>(g, list + start, len, level, sigma, cnt, lvl, soff, succ, list + start + len,
+                                                           &ctl()->next_len, b.sigma_inexact, lane, NGX_GW, NGX_GWARPS);
                 }
-                __syncthreads();
-                if (tid == 0) {
-                    s.lvl_start = start + len;
-                    s.lvl_len = s.next_len;
-                    s.next_len = 0;
-                    s.level = level + 1u;
+                grp().sync(s, s_bar, [&](volatile TileShared& c) {
+                    c.lvl_start = start + len;
+                    c.lvl_len = c.next_len;
+                    c.next_len = 0;
+                    c.level = level + 1u;
                     loff[level + 1u] = start + len;
-                }
-                __syncthreads();
+                });
             }
             if (tid == 0) {
                 const long long now = clock64();
@@ -618,48 +689,29 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 const int end = __ldcg(&loff[level + 1]);
                 if (tree) {
                     dag_delta_level<kMode, true>(g, list + start, end - start, dist, sigma, delta, delta_g, soff, succ, b.grad_cpl, b.grad_eff,
-                                                 reinterpret_cast<double*>(s_acc_sum), lane, warp, nwarps);
+                                                 reinterpret_cast<double*>(s_acc_sum), lane, warp, NGX_GW, NGX_GWARPS);
                 } else {
                     dag_delta_level<kMode, false>(g, list + start, end - start, dist, sigma, delta, delta_g, soff, succ, b.grad_cpl, b.grad_eff,
-                                                  reinterpret_cast<double*>(s_acc_sum), lane, warp, nwarps);
+                                                  reinterpret_cast<double*>(s_acc_sum), lane, warp, NGX_GW, NGX_GWARPS);
                 }
-                __syncthreads();
+                grp().sync(s, s_bar);
             }
             // the pair buffers borrowed the epilogue's accumulators, which must start the epilogue at zero
-            for (int k = tid; k < nwarps * 32 * delta_level_unroll(kMode) * (kMode == kModeGrad ? 2 : 1); k += blockDim.x) {
+            for (int k = tid; k < (kBlock / 32) * 32 * delta_level_unroll(kMode) * (kMode == kModeGrad ? 2 : 1); k += blockDim.x) {
                 s_acc_sum[k] = 0ull;
             }
             __syncthreads();
             if (tid == 0) {
-                atomicAdd(&cnts[kDagLevels], static_cast<unsigned long long>(levels));
-                atomicAdd(&cnts[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
+                if (grp().rank == 0) {
+                    atomicAdd(&cnts[kDagLevels], static_cast<unsigned long long>(levels));
+                    atomicAdd(&cnts[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
+                }
                 const long long now = clock64();
                 atomicAdd(&cnts[kCyclesDelta], static_cast<unsigned long long>(now - t_phase));
                 t_phase = now;
             }
           } else {
             // --- too many DAG arcs for the lists (many ties): the arc-scanning passes, one vertex per warp
-            if (tid == 0) {
-                s.stamp += 1u;
-                s.level = 0u;
-                s.lvl_start = 0;
-                s.lvl_len = 0;
-                s.next_len = 0;
-                loff[0] = 0;
-            }
-            __syncthreads();
-            if (warp == 0) {
-                const int v = s_src[lane];
-                if (v >= 0) {
-                    const int64_t row = static_cast<int64_t>(v) * kTile + lane;
-                    lvl[row] = 0u;
-                    sigma[row] = 1.0;
-                    if (atomicExch(&stamp[v], s.stamp) != s.stamp) {
-                        list[atomicAdd(&s.lvl_len, 1)] = v;
-                    }
-                }
-            }
-            __syncthreads();
             for (;;) {
                 const int start = s.lvl_start;
                 const int len = s.lvl_len;
@@ -669,26 +721,24 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 const unsigned level = s.level;
                 const unsigned level_stamp = s.stamp + 1u;
                 if (b.sigma_pull != 0) {
-                    for (int i = warp; i < len; i += nwarps) {
+                    for (int i = NGX_GW; i < len; i += NGX_GWARPS) {
                         brandes_sigma_vertex<true, 2>(g, rg, __ldcg(&list[start + i]), level, nsrc, lane, dist, sigma, cnt, lvl, stamp, level_stamp,
-                                                      list + start + len, &s.next_len, b.sigma_inexact);
+                                                      list + start + len, &ctl()->next_len, b.sigma_inexact);
                     }
                 } else {
-                    for (int i = warp; i < len; i += nwarps) {
+                    for (int i = NGX_GW; i < len; i += NGX_GWARPS) {
                         brandes_sigma_vertex<false, 2>(g, rg, __ldcg(&list[start + i]), level, nsrc, lane, dist, sigma, cnt, lvl, stamp, level_stamp,
-                                                       list + start + len, &s.next_len, b.sigma_inexact);
+                                                       list + start + len, &ctl()->next_len, b.sigma_inexact);
                     }
                 }
-                __syncthreads();
-                if (tid == 0) {
-                    s.lvl_start = start + len;
-                    s.lvl_len = s.next_len;
-                    s.next_len = 0;
-                    s.stamp = level_stamp;
-                    s.level = level + 1u;
+                grp().sync(s, s_bar, [&](volatile TileShared& c) {
+                    c.lvl_start = start + len;
+                    c.lvl_len = c.next_len;
+                    c.next_len = 0;
+                    c.stamp = level_stamp;
+                    c.level = level + 1u;
                     loff[level + 1u] = start + len;
-                }
-                __syncthreads();
+                });
             }
             if (tid == 0) {
                 const long long now = clock64();
@@ -701,17 +751,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             for (int level = levels - 1; level >= lowest; --level) {
                 const int start = __ldcg(&loff[level]);
                 const int end = __ldcg(&loff[level + 1]);
-                for (int i = start + warp; i < end; i += nwarps) {
+                for (int i = start + NGX_GW; i < end; i += NGX_GWARPS) {
                     brandes_delta_vertex<kMode, 2>(g, __ldcg(&list[i]), static_cast<unsigned>(level), nsrc, lane, dist, sigma, delta, delta_g, lvl,
                                                    b.grad_cpl, b.grad_eff);
                 }
-                __syncthreads();
+                grp().sync(s, s_bar);
             }
             if (tid == 0) {
-                atomicAdd(&cnts[kDagLevels], static_cast<unsigned long long>(levels));
-                atomicAdd(&cnts[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
-            }
-            if (tid == 0) {
+                if (grp().rank == 0) {
+                    atomicAdd(&cnts[kDagLevels], static_cast<unsigned long long>(levels));
+                    atomicAdd(&cnts[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
+                }
                 const long long now = clock64();
                 atomicAdd(&cnts[kCyclesDelta], static_cast<unsigned long long>(now - t_phase));
                 t_phase = now;
@@ -723,7 +773,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         const int my_src = s_src[lane];
         const bool valid = lane < nsrc;
         unsigned long long unreach = 0, arcs = 0, mx = 0, overflow = 0;
-        for (int64_t v = warp; v < n; v += nwarps) {
+        for (int64_t v = NGX_GW; v < n; v += NGX_GWARPS) {
             unsigned long long* slot_ptr = &dist[v * kTile + lane];
             const unsigned long long bits = __ldcg(slot_ptr);
             *slot_ptr = kInfBits;
@@ -788,45 +838,78 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             atomicMax(&s_max[lane], mx);
         }
         if (overflow != 0) {
-            atomicAdd(&s.overflow, overflow);
+            atomicAdd(&cnts[kHistOverflow], overflow);
         }
         __syncthreads();
-        if (tid < nsrc) {
-            unsigned long long* a_sum = &s_acc_sum[tid * kAccDigits];
-            unsigned long long* a_inv = &s_acc_inv[tid * kAccDigits];
-            acc_normalize(a_sum);
-            acc_normalize(a_inv);
-            const int64_t pos = base + tid;
-            if (p.out.src_sum != nullptr) p.out.src_sum[pos] = acc_round_normalized(a_sum);
-            if (p.out.src_inv != nullptr) p.out.src_inv[pos] = acc_round_normalized(a_inv);
-            if (p.out.src_max != nullptr) p.out.src_max[pos] = __longlong_as_double(static_cast<long long>(s_max[tid]));
-            if (p.out.src_unreach != nullptr) p.out.src_unreach[pos] = s_unreach[tid];
-            if (p.out.src_arcs != nullptr) p.out.src_arcs[pos] = s_arcs[tid];
-            const unsigned long long reached = static_cast<unsigned long long>(n) - s_unreach[tid];
-            atomicAdd(&cnts[kUnreachable], s_unreach[tid]);
-            atomicAdd(&cnts[kReachedPairs], reached - 1ull);
-            atomicAdd(&cnts[kTraversedArcs], s_arcs[tid]);
-            atomicMax(&cnts[kDiameterBits], s_max[tid]);
-        }
-        __syncthreads();
-        for (int i = tid; i < kAccDigits; i += blockDim.x) {
-            unsigned long long t_sum = 0, t_inv = 0;
-            for (int k = 0; k < nsrc; ++k) {
-                t_sum += s_acc_sum[k * kAccDigits + i];
-                t_inv += s_acc_inv[k * kAccDigits + i];
+        if (p.group_size > 1) {
+            // the group's CTAs add their per-source sums into the group's (exact integer adds), and the first CTA
+            // finishes the tile's per-source outputs from them
+            unsigned long long* const g_acc = p.group_ws + slot * p.group_stride + kCtlWords + 1 + p.group_size;  // kGroupAccWords
+            for (int i = tid; i < 2 * kTile * kAccDigits; i += blockDim.x) {
+                if (smem[i] != 0ull) {
+                    atomicAdd(&g_acc[i], smem[i]);
+                }
             }
-            if (t_sum != 0) atomicAdd(&acc_sum_g[i], t_sum);
-            if (t_inv != 0) atomicAdd(&acc_inv_g[i], t_inv);
+            if (tid < kTile) {
+                atomicAdd(&g_acc[2 * kTile * kAccDigits + tid], s_unreach[tid]);
+                atomicAdd(&g_acc[2 * kTile * kAccDigits + kTile + tid], s_arcs[tid]);
+                atomicMax(&g_acc[2 * kTile * kAccDigits + 2 * kTile + tid], s_max[tid]);
+            }
+            grp().sync(s, s_bar);
+            if (grp().rank == 0) {
+                for (int i = tid; i < 2 * kTile * kAccDigits; i += blockDim.x) {
+                    smem[i] = __ldcg(&g_acc[i]);
+                    g_acc[i] = 0ull;
+                }
+                if (tid < kTile) {
+                    unsigned long long* const per = g_acc + 2 * kTile * kAccDigits;
+                    s_unreach[tid] = __ldcg(&per[tid]);
+                    s_arcs[tid] = __ldcg(&per[kTile + tid]);
+                    s_max[tid] = __ldcg(&per[2 * kTile + tid]);
+                    per[tid] = 0ull;
+                    per[kTile + tid] = 0ull;
+                    per[2 * kTile + tid] = 0ull;
+                }
+            }
+            __syncthreads();
+        }
+        if (grp().rank == 0) {
+            if (tid < nsrc) {
+                unsigned long long* a_sum = &s_acc_sum[tid * kAccDigits];
+                unsigned long long* a_inv = &s_acc_inv[tid * kAccDigits];
+                acc_normalize(a_sum);
+                acc_normalize(a_inv);
+                const int64_t pos = base + tid;
+                if (p.out.src_sum != nullptr) p.out.src_sum[pos] = acc_round_normalized(a_sum);
+                if (p.out.src_inv != nullptr) p.out.src_inv[pos] = acc_round_normalized(a_inv);
+                if (p.out.src_max != nullptr) p.out.src_max[pos] = __longlong_as_double(static_cast<long long>(s_max[tid]));
+                if (p.out.src_unreach != nullptr) p.out.src_unreach[pos] = s_unreach[tid];
+                if (p.out.src_arcs != nullptr) p.out.src_arcs[pos] = s_arcs[tid];
+                const unsigned long long reached = static_cast<unsigned long long>(n) - s_unreach[tid];
+                atomicAdd(&cnts[kUnreachable], s_unreach[tid]);
+                atomicAdd(&cnts[kReachedPairs], reached - 1ull);
+                atomicAdd(&cnts[kTraversedArcs], s_arcs[tid]);
+                atomicMax(&cnts[kDiameterBits], s_max[tid]);
+            }
+            __syncthreads();
+            for (int i = tid; i < kAccDigits; i += blockDim.x) {
+                unsigned long long t_sum = 0, t_inv = 0;
+                for (int k = 0; k < nsrc; ++k) {
+                    t_sum += s_acc_sum[k * kAccDigits + i];
+                    t_inv += s_acc_inv[k * kAccDigits + i];
+                }
+                if (t_sum != 0) atomicAdd(&acc_sum_g[i], t_sum);
+                if (t_inv != 0) atomicAdd(&acc_inv_g[i], t_inv);
+            }
+            if (tid == 0) {
+                atomicAdd(&cnts[kIterations], s.iterations);
+            }
         }
         for (int i = tid; i < p.out.hist_bins; i += blockDim.x) {
             if (s_hist[i] != 0u) {
                 atomicAdd(&hist_g[i], static_cast<unsigned long long>(s_hist[i]));
                 s_hist[i] = 0u;
             }
-        }
-        if (tid == 0) {
-            if (s.overflow != 0) atomicAdd(&cnts[kHistOverflow], s.overflow);
-            atomicAdd(&cnts[kIterations], s.iterations);
         }
         __syncthreads();
         for (int i = tid; i < 2 * kTile * kAccDigits; i += blockDim.x) {
@@ -842,6 +925,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         atomicAdd(&p.out.counters[kExpansions], expansions);
         atomicAdd(&p.out.counters[kLaneExpansions], lane_expansions);
     }
+#undef NGX_GT
+#undef NGX_GTHREADS
+#undef NGX_GW
+#undef NGX_GWARPS
 }
 
 // ------------------------------------------------------------------------------------------ plain form
@@ -963,7 +1050,7 @@ __global__ void __launch_bounds__(512, 2) sssp_plain_kernel(const SsspParams p) 
                         bool push = false;
                         int x = 0;
                         if (e < end) {
-                            const Arc a = p.g.arcs[e];
+                            const Arc a = ldg_arc(&p.g.arcs[e]);
                             x = a.col;
                             const double nd = __dadd_rn(dv, a.len);
                             const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd));
