@@ -201,6 +201,28 @@ NGX_API int ngx_graph_set_memory_budget(ngx_graph* graph, uint64_t bytes);
  */
 NGX_API int ngx_graph_source_order(const ngx_graph* graph, int64_t* order);
 
+/*
+ * Autotuning of a single-graph handle. ngx_graph_autotune times the task (NGX_TASK_APSP, _BRANDES or _GRAD, below) on
+ * the first `sample_sources` sources of the graph's all-sources order (0 = one wave: 32 x resident CTAs) for bucket
+ * widths (multiples of the mean arc length), block shapes and CTAs per source tile, one parameter at a time, and keeps
+ * the fastest (traversed arcs per second) in the handle: later runs of that task use it for every option they leave
+ * at 0 (delta, block_threads with ctas_per_sm, tile_ctas). Results never depend on these choices. best (optional)
+ * receives the choice. No reference counterpart (the reference has no launch parameters; its delta-stepping takes
+ * delta from --apsp-delta, neurograph.cpp:507-515).
+ */
+typedef enum { NGX_TASK_APSP = 0, NGX_TASK_BRANDES = 1, NGX_TASK_GRAD = 2 } ngx_task;
+
+typedef struct {
+    double delta_scale; /* bucket width = delta_scale x the mean arc length */
+    int block_threads;  /* threads per CTA */
+    int ctas_per_sm;    /* resident CTAs per SM */
+    int tile_ctas;      /* CTAs per source tile */
+    int trials;         /* configurations timed */
+    double gteps;       /* traversed arcs per second of the choice on the sample, in 1e9 */
+} ngx_tuning;
+
+NGX_API int ngx_graph_autotune(ngx_graph* graph, int task, int64_t sample_sources, ngx_tuning* best);
+
 /* APSP summaries (and optional histogram / per-source outputs) over the requested sources. */
 NGX_API int ngx_apsp(ngx_graph* graph, const ngx_apsp_opts* opts, ngx_apsp_result* result);
 
@@ -261,7 +283,6 @@ NGX_API int ngx_apsp_noalloc(ngx_graph* graph, const ngx_apsp_opts* opts, ngx_ap
  * (graph, source tile) work items in longest-first order. No reference counterpart: the reference processes one
  * graph per run (neurograph.cpp:139-416); the batch runs that loop's APSP / betweenness for every graph at once.
  */
-typedef enum { NGX_TASK_APSP = 0, NGX_TASK_BRANDES = 1, NGX_TASK_GRAD = 2 } ngx_task;
 
 #define NGX_SIZE_CLASSES 32 /* graphs are grouped by floor(log2(n)) for the tuned bucket widths */
 
@@ -291,9 +312,17 @@ NGX_API int ngx_batch_run(ngx_graph* batch, const ngx_batch_opts* opts, ngx_apsp
 /*
  * Picks the bucket width scale of every size class present in the batch: for each class, the median-size graph's first
  * wave of source tiles runs with scales 1/8 .. 4 and the fastest (traversed arcs per second) is kept in the handle.
- * class_scales (optional, NGX_SIZE_CLASSES entries) receives the result (0 for classes without graphs).
+ * Then, since one launch runs every graph, one launch shape for the whole batch: block shapes (512 x 2, 384 x 2,
+ * 256 x 3, 256 x 4 threads x CTAs per SM) and then 1, 2 or 4 CTAs per source tile, timed on the size class holding
+ * most of the batch's work; ngx_batch_run uses it when its options leave block_threads and tile_ctas at 0, and
+ * ngx_graph_tuning reads it. class_scales (optional, NGX_SIZE_CLASSES entries) receives the scales (0 for classes
+ * without graphs).
  */
 NGX_API int ngx_batch_autotune(ngx_graph* batch, int task, double* class_scales);
+
+/* The launch shape and bucket width a handle keeps for `task` (from ngx_graph_autotune or ngx_batch_autotune; all
+ * zero if the task was not tuned). */
+NGX_API int ngx_graph_tuning(const ngx_graph* graph, int task, ngx_tuning* out);
 
 /*
  * Replaces the weights of a graph or batch handle in place (same arcs, caller order, sum of m entries). A weight may

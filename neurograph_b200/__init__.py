@@ -67,6 +67,11 @@ class _BatchOpts(C.Structure):
     ]
 
 
+class _Tuning(C.Structure):
+    _fields_ = [("delta_scale", C.c_double), ("block_threads", C.c_int), ("ctas_per_sm", C.c_int), ("tile_ctas", C.c_int),
+                ("trials", C.c_int), ("gteps", C.c_double)]
+
+
 class _Result(C.Structure):
     _fields_ = [
         ("sum_distances", C.c_double), ("sum_inverse", C.c_double), ("diameter", C.c_double),
@@ -105,6 +110,8 @@ def library() -> C.CDLL:
         lib.ngx_graph_create.argtypes = [C.POINTER(_Csr), C.c_int, C.POINTER(C.c_void_p)]
         lib.ngx_graph_create_ex.argtypes = [C.POINTER(_Csr), C.c_int, C.c_int, C.POINTER(C.c_void_p)]
         lib.ngx_graph_layout.argtypes = [C.c_void_p] + [C.c_void_p] * 7
+        lib.ngx_graph_autotune.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.POINTER(_Tuning)]
+        lib.ngx_graph_tuning.argtypes = [C.c_void_p, C.c_int, C.POINTER(_Tuning)]
         lib.ngx_graph_destroy.argtypes = [C.c_void_p]
         lib.ngx_graph_destroy.restype = None
         lib.ngx_graph_size.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
@@ -272,6 +279,14 @@ class Graph:
 
     def set_memory_budget(self, nbytes: int) -> None:
         _check(library().ngx_graph_set_memory_budget(self._handle, int(nbytes)))
+
+    def autotune(self, task="apsp", sample_sources: int = 0) -> dict:
+        """ngx_graph_autotune: times the task on a sample of the all-sources order for bucket widths, block shapes and
+        CTAs per tile, keeps the fastest for later runs that leave those options at 0, and returns it."""
+        t = _Tuning()
+        _check(library().ngx_graph_autotune(self._handle, TASKS[task] if isinstance(task, str) else int(task), int(sample_sources),
+                                            C.byref(t)))
+        return {name: getattr(t, name) for name, _ in _Tuning._fields_}
 
     def source_order(self) -> np.ndarray:
         """The order in which all-sources runs take the sources (tiles of nearby vertices); contiguous chunks of it
@@ -488,8 +503,15 @@ class Batch:
             a_off += m
         return results, extras
 
+    def tuning(self, task="apsp") -> dict:
+        """The launch shape ngx_batch_autotune picked for the task (ngx_graph_tuning)."""
+        t = _Tuning()
+        _check(library().ngx_graph_tuning(self._handle, TASKS[task] if isinstance(task, str) else int(task), C.byref(t)))
+        return {name: getattr(t, name) for name, _ in _Tuning._fields_}
+
     def autotune(self, task="apsp") -> np.ndarray:
-        """Tunes the bucket width per size class (floor(log2 n)); returns the chosen scales (0 = class empty)."""
+        """Tunes the bucket width per size class (floor(log2 n)) and the batch's launch shape; returns the chosen scales
+        (0 = class empty)."""
         scales = np.zeros(SIZE_CLASSES)
         _check(library().ngx_batch_autotune(self._handle, TASKS[task] if isinstance(task, str) else int(task), scales.ctypes.data))
         return scales

@@ -99,7 +99,72 @@ uint64_t options_key(const ngx_batch_opts* o, const ngx_graph* g) {
         std::memcpy(&bits, &g->class_scale[c], 8);
         h = mix(h, bits);
     }
+    for (const ngx_tuning& t : g->tuned) {
+        h = mix(h, static_cast<uint64_t>(t.block_threads) << 32 | static_cast<uint64_t>(t.ctas_per_sm) << 16 | static_cast<uint64_t>(t.tile_ctas));
+    }
     return h == 0 ? 1 : h;
+}
+
+// Times the first wave of graph gi's source tiles (at most 2 x SMs tiles, in the order a run takes them) with bucket
+// width `scale` x its mean arc length and the launch options of `aopts`; *rate = traversed arcs per millisecond.
+int time_wave(ngx_graph* g, int mode, int32_t gi, double scale, const ngx_apsp_opts& aopts, double* rate) {
+    *rate = 0.0;
+    const GraphPart& part = g->parts[static_cast<size_t>(gi)];
+    const int64_t tiles = std::min<int64_t>((part.n + kTile - 1) / kTile, 2 * g->sm_count);
+    std::vector<WorkItem> items(static_cast<size_t>(tiles));
+    for (int64_t t = 0; t < tiles; ++t) {
+        items[static_cast<size_t>(t)] = WorkItem{ 0, static_cast<int32_t>(t) };
+    }
+    const std::vector<int32_t> sources(g->source_order.begin() + part.vertex_off, g->source_order.begin() + part.vertex_off + part.n);
+    WorkItem* d_items = nullptr;
+    NGX_CUDA_TRY(cudaMalloc(&d_items, std::max<size_t>(1, items.size()) * sizeof(WorkItem)));
+    struct Free {
+        WorkItem* p;
+        ~Free() { cudaFree(p); }
+    } free_items{ d_items };
+    NGX_CUDA_TRY(cudaMemcpy(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
+    RunOutputs o;
+    int rc = alloc_outputs(g, 1, part.n, 0, false, o, false);
+    DagOutputs extra;
+    const size_t dag_words = 1 + (mode == kModeBrandes ? 2 * static_cast<size_t>(g->n_total) : 0) +
+                             (mode == kModeGrad ? 4 * static_cast<size_t>(g->m_user) : 0);
+    if (rc == NGX_OK && mode != kModeApsp) {
+        rc = grow_buffer(g, &g->d_call_dag, &g->call_dag_bytes, dag_words * 8);
+        if (rc == NGX_OK) {
+            auto* dag = static_cast<unsigned long long*>(g->d_call_dag);
+            cudaMemsetAsync(dag, 0, dag_words * 8, g->stream);
+            extra.sigma_inexact = reinterpret_cast<int*>(dag);
+            if (mode == kModeBrandes) extra.bc = dag + 1;
+            if (mode == kModeGrad) {
+                extra.grad_cpl = dag + 1;
+                extra.grad_eff = dag + 1 + 2 * static_cast<size_t>(g->m_user);
+            }
+        }
+    }
+    if (rc == NGX_OK) {
+        const GraphDesc desc{ part.n, part.m_stored, part.row_off, 0, part.n, part.vertex_off, pick_delta(part.mean_len_regular, 0.0, scale) };
+        cudaMemsetAsync(o.block, 0, o.zeroed_bytes, g->stream);
+        cudaMemcpyAsync(o.graphs, &desc, sizeof(desc), cudaMemcpyHostToDevice, g->stream);
+        cudaMemcpyAsync(o.sources, sources.data(), sources.size() * 4, cudaMemcpyHostToDevice, g->stream);
+        TileJob job;
+        job.num_graphs = 1;
+        job.num_items = tiles;
+        job.d_items = d_items;
+        job.num_sources = part.n;
+        job.n_max = g->n;
+        float ms = 0.0f;
+        rc = launch_tiles(g, &aopts, mode, job, 0, 0.0, o, mode != kModeApsp ? &extra : nullptr, &ms, true);
+        if (rc == NGX_OK) {
+            std::vector<unsigned long long> acc, counters;
+            rc = read_totals(g, o, acc, counters);
+            if (rc == NGX_OK && ms > 0.0f) {
+                *rate = static_cast<double>(counters[kTraversedArcs]) / ms;
+            }
+        }
+    }
+    free_outputs(g, o);
+    cudaStreamSynchronize(g->stream);
+    return rc;
 }
 
 // Resets the zero-initialised part of the outputs (and the betweenness / gradient sums), then launches.
@@ -161,6 +226,14 @@ int ngx_batch_run(ngx_graph* g, const ngx_batch_opts* opts, ngx_apsp_result* res
         aopts.mode = NGX_MODE_BATCHED;
         aopts.block_threads = opts->block_threads;
         aopts.tile_ctas = opts->tile_ctas;
+        const ngx_tuning& tuned = g->tuned[mode];
+        if (tuned.block_threads > 0 && aopts.block_threads == 0) {
+            aopts.block_threads = tuned.block_threads;  // the launch shape ngx_batch_autotune picked
+            aopts.ctas_per_sm = tuned.ctas_per_sm;
+        }
+        if (tuned.tile_ctas > 0 && aopts.tile_ctas == 0) {
+            aopts.tile_ctas = tuned.tile_ctas;
+        }
         aopts.max_iterations = opts->max_iterations;
         if (const int rc = check_opts(g, &aopts); rc != NGX_OK) {
             return rc;
@@ -346,14 +419,18 @@ int ngx_batch_autotune(ngx_graph* g, int task, double* class_scales) {
         NGX_CUDA_TRY(cudaSetDevice(g->device));
         *g->h_abort = 0;
         static const double kScales[] = { 0.125, 0.25, 0.5, 1.0, 2.0, 4.0 };
-        ngx_apsp_opts aopts{};
-        aopts.metric = NGX_METRIC_REGULAR;
-        aopts.mode = NGX_MODE_BATCHED;
+        g->tuned[mode] = ngx_tuning{};
+        // the graph of each size class whose first wave is timed: its median-size member
+        int32_t heaviest = -1;
+        double heaviest_work = -1.0;
+        std::vector<int32_t> probe(NGX_SIZE_CLASSES, -1);
         for (int c = 0; c < NGX_SIZE_CLASSES; ++c) {
             std::vector<int32_t> members;
+            double work = 0.0;
             for (size_t i = 0; i < g->parts.size(); ++i) {
                 if (size_class(g->parts[i].n) == c && g->parts[i].n > 0) {
                     members.push_back(static_cast<int32_t>(i));
+                    work += static_cast<double>(g->parts[i].n) * static_cast<double>(g->parts[i].m_stored);
                 }
             }
             if (class_scales != nullptr) {
@@ -363,80 +440,99 @@ int ngx_batch_autotune(ngx_graph* g, int task, double* class_scales) {
                 continue;
             }
             std::sort(members.begin(), members.end(), [&](int32_t a, int32_t b) { return g->parts[static_cast<size_t>(a)].n < g->parts[static_cast<size_t>(b)].n; });
-            const int32_t gi = members[members.size() / 2];
-            const GraphPart& part = g->parts[static_cast<size_t>(gi)];
-            // one wave of the graph's source tiles (at most 2 x SMs tiles)
-            const int64_t tiles = std::min<int64_t>((part.n + kTile - 1) / kTile, 2 * g->sm_count);
-            std::vector<WorkItem> items(static_cast<size_t>(tiles));
-            for (int64_t t = 0; t < tiles; ++t) {
-                items[static_cast<size_t>(t)] = WorkItem{ 0, static_cast<int32_t>(t) };
+            probe[static_cast<size_t>(c)] = members[members.size() / 2];
+            if (work > heaviest_work) {
+                heaviest_work = work;
+                heaviest = c;
             }
-            // the graph's sources in the order a run takes them
-            const std::vector<int32_t> sources(g->source_order.begin() + part.vertex_off, g->source_order.begin() + part.vertex_off + part.n);
-            WorkItem* d_items = nullptr;
-            NGX_CUDA_TRY(cudaMalloc(&d_items, items.size() * sizeof(WorkItem)));
-            NGX_CUDA_TRY(cudaMemcpy(d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice));
+        }
+        // bucket width per size class, with the default launch shape
+        ngx_apsp_opts aopts{};
+        aopts.metric = NGX_METRIC_REGULAR;
+        aopts.mode = NGX_MODE_BATCHED;
+        for (int c = 0; c < NGX_SIZE_CLASSES; ++c) {
+            if (probe[static_cast<size_t>(c)] < 0) {
+                continue;
+            }
             double best_rate = -1.0, best_scale = 1.0;
             for (const double scale : kScales) {
-                RunOutputs o;
-                int rc = alloc_outputs(g, 1, part.n, 0, false, o, false);
-                DagOutputs extra;
-                unsigned long long* dag = nullptr;
-                const size_t dag_words = 1 + (mode == kModeBrandes ? 2 * static_cast<size_t>(g->n_total) : 0) +
-                                         (mode == kModeGrad ? 4 * static_cast<size_t>(g->m_user) : 0);
-                if (rc == NGX_OK && mode != kModeApsp) {
-                    rc = grow_buffer(g, &g->d_call_dag, &g->call_dag_bytes, dag_words * 8);
-                    if (rc == NGX_OK) {
-                        dag = static_cast<unsigned long long*>(g->d_call_dag);
-                        cudaMemsetAsync(dag, 0, dag_words * 8, g->stream);
-                        extra.sigma_inexact = reinterpret_cast<int*>(dag);
-                        if (mode == kModeBrandes) extra.bc = dag + 1;
-                        if (mode == kModeGrad) {
-                            extra.grad_cpl = dag + 1;
-                            extra.grad_eff = dag + 1 + 2 * static_cast<size_t>(g->m_user);
-                        }
-                    }
-                }
-                if (rc == NGX_OK) {
-                    const GraphDesc desc{ part.n, part.m_stored, part.row_off, 0, part.n, part.vertex_off, pick_delta(part.mean_len_regular, 0.0, scale) };
-                    cudaMemsetAsync(o.block, 0, o.zeroed_bytes, g->stream);
-                    cudaMemcpyAsync(o.graphs, &desc, sizeof(desc), cudaMemcpyHostToDevice, g->stream);
-                    cudaMemcpyAsync(o.sources, sources.data(), sources.size() * 4, cudaMemcpyHostToDevice, g->stream);
-                    TileJob job;
-                    job.num_graphs = 1;
-                    job.num_items = tiles;
-                    job.d_items = d_items;
-                    job.num_sources = part.n;
-                    job.n_max = g->n;
-                    float ms = 0.0f;
-                    rc = launch_tiles(g, &aopts, mode, job, 0, 0.0, o, mode != kModeApsp ? &extra : nullptr, &ms, true);
-                    if (rc == NGX_OK) {
-                        std::vector<unsigned long long> acc, counters;
-                        rc = read_totals(g, o, acc, counters);
-                        if (rc == NGX_OK && ms > 0.0f) {
-                            const double rate = static_cast<double>(counters[kTraversedArcs]) / ms;
-                            if (rate > best_rate) {
-                                best_rate = rate;
-                                best_scale = scale;
-                            }
-                        }
-                    }
-                }
-                free_outputs(g, o);
-                cudaStreamSynchronize(g->stream);
-                if (rc != NGX_OK) {
-                    cudaFree(d_items);
+                double rate = 0.0;
+                if (const int rc = time_wave(g, mode, probe[static_cast<size_t>(c)], scale, aopts, &rate); rc != NGX_OK) {
                     return rc;
                 }
+                if (rate > best_rate) {
+                    best_rate = rate;
+                    best_scale = scale;
+                }
             }
-            cudaFree(d_items);
             g->class_scale[c] = best_scale;
             if (class_scales != nullptr) {
                 class_scales[c] = best_scale;
             }
         }
+        // one launch shape for the whole batch (one launch runs every graph): block shape, then CTAs per tile, timed on
+        // the size class that holds most of the batch's work
+        if (heaviest >= 0) {
+            const int32_t gi = probe[static_cast<size_t>(heaviest)];
+            const double scale = g->class_scale[heaviest];
+            struct Shape {
+                int block, per_sm;
+            };
+            static const Shape kShapes[] = { { 512, 2 }, { 384, 2 }, { 256, 3 }, { 256, 4 } };
+            double best_rate = -1.0;
+            Shape best_shape = kShapes[0];
+            int trials = 0;
+            for (const Shape& sh : kShapes) {
+                aopts.block_threads = sh.block;
+                aopts.ctas_per_sm = sh.per_sm;
+                aopts.tile_ctas = 1;
+                double rate = 0.0;
+                if (const int rc = time_wave(g, mode, gi, scale, aopts, &rate); rc != NGX_OK) {
+                    return rc;
+                }
+                ++trials;
+                if (rate > best_rate) {
+                    best_rate = rate;
+                    best_shape = sh;
+                }
+            }
+            int best_group = 1;
+            for (const int gs : { 2, 4 }) {
+                aopts.block_threads = best_shape.block;
+                aopts.ctas_per_sm = best_shape.per_sm;
+                aopts.tile_ctas = gs;
+                double rate = 0.0;
+                if (const int rc = time_wave(g, mode, gi, scale, aopts, &rate); rc != NGX_OK) {
+                    return rc;
+                }
+                ++trials;
+                if (rate > best_rate) {
+                    best_rate = rate;
+                    best_group = gs;
+                }
+            }
+            ngx_tuning& t = g->tuned[mode];
+            t.delta_scale = scale;
+            t.block_threads = best_shape.block;
+            t.ctas_per_sm = best_shape.per_sm;
+            t.tile_ctas = best_group;
+            t.trials = trials;
+            t.gteps = best_rate / 1e6;
+        }
         return NGX_OK;
     });
+}
+
+int ngx_graph_tuning(const ngx_graph* g, int task, ngx_tuning* out) {
+    if (g == nullptr || out == nullptr) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_tuning: graph or out is NULL");
+    }
+    const int mode = task_mode(task);
+    if (mode < 0) {
+        return fail(NGX_INVALID_ARGUMENT, "ngx_graph_tuning: unknown task");
+    }
+    *out = g->tuned[mode];
+    return NGX_OK;
 }
 
 int ngx_graph_update_weights(ngx_graph* g, const double* w) {

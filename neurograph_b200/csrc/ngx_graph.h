@@ -103,6 +103,9 @@ struct ngx_graph {
 
     // bucket width per size class (floor(log2 n)), as a multiple of each graph's mean arc length (ngx_batch_autotune)
     double class_scale[64] = {};
+    // launch shape and bucket width picked by ngx_graph_autotune, per task (APSP, Brandes, gradient); runs use them
+    // for the options they leave at 0
+    ngx_tuning tuned[3] = {};
     // stored forward index of each caller arc (-1 for zero weights), for ngx_graph_update_weights (a device-built
     // handle copies it from d_stored_of_user on first use)
     ngx::HostVector<int32_t> stored_of_user;

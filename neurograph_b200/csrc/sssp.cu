@@ -596,10 +596,27 @@ int auto_hist_max(ngx_graph* g, const ngx_apsp_opts* opts, const std::vector<int
     return rc;
 }
 
-int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, double* rows, int tile_mode, DagOutputs* extra) {
-    if (const int rc = check_opts(g, opts); rc != NGX_OK) {
+int run_apsp(ngx_graph* g, const ngx_apsp_opts* caller_opts, ngx_apsp_result* result, double* rows, int tile_mode, DagOutputs* extra) {
+    if (const int rc = check_opts(g, caller_opts); rc != NGX_OK) {
         return rc;
     }
+    // options left at 0 take the handle's tuned values for this task (ngx_graph_autotune), if any
+    ngx_apsp_opts tuned_opts = *caller_opts;
+    const ngx_tuning& t = g->tuned[tile_mode];
+    if (t.block_threads > 0 && tuned_opts.mode == NGX_MODE_BATCHED) {
+        if (tuned_opts.block_threads == 0 && tuned_opts.ctas_per_sm == 0) {
+            tuned_opts.block_threads = t.block_threads;
+            tuned_opts.ctas_per_sm = t.ctas_per_sm;
+        }
+        if (tuned_opts.tile_ctas == 0) {
+            tuned_opts.tile_ctas = t.tile_ctas;
+        }
+        if (!(tuned_opts.delta > 0.0) && g->parts.size() == 1) {
+            const GraphPart& part = g->parts[0];
+            tuned_opts.delta = pick_delta(tuned_opts.metric == NGX_METRIC_INVERSE ? part.mean_len_inverse : part.mean_len_regular, 0.0, t.delta_scale);
+        }
+    }
+    const ngx_apsp_opts* opts = &tuned_opts;
     if (g->parts.size() != 1) {
         return fail(NGX_INVALID_ARGUMENT, "this handle holds a batch of graphs: use ngx_batch_run");
     }

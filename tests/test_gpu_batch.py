@@ -170,7 +170,11 @@ def test_autotune_keeps_results():
     with ngx.Batch(graphs) as b:
         before, _ = b.run("apsp")
         scales = b.autotune("apsp")
+        shape = b.tuning("apsp")
         after, _ = b.run("apsp")
+    # one launch shape for the whole batch
+    assert (shape["block_threads"], shape["ctas_per_sm"]) in ((512, 2), (384, 2), (256, 3), (256, 4)), shape
+    assert shape["tile_ctas"] in (1, 2, 4) and shape["trials"] == 6 and shape["gteps"] > 0, shape
     classes = {int(np.floor(np.log2(n))) for n, *_ in graphs if n > 0}
     for c in range(ngx.SIZE_CLASSES):
         if c in classes:
