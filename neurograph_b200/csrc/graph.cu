@@ -645,7 +645,50 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
     return finish(rc);
 }
 
+// SCC passes (kernel launches with a host flag read, ~10-20 us each) the APSP pre-pass may spend.
+constexpr int64_t kSccPrePassCap = 2048;
+
+int ensure_components(ngx_graph* g) {
+    if (g->scc_components != 0 || g->parts.size() != 1 || g->n == 0) {
+        return NGX_OK;
+    }
+    // a pre-pass for the runs, so bounded: graphs whose components need more passes (long chains) run without it
+    uint64_t count = 0, largest = 0;
+    g->scc_pass_cap = kSccPrePassCap;
+    g->scc_passes = 0;
+    const int rc = ngx_scc(g, nullptr, &count, &largest, nullptr);
+    g->scc_pass_cap = 0;
+    if (rc == NGX_TIMEOUT) {
+        g->scc_components = -1;
+        set_last_error("");
+        return NGX_OK;
+    }
+    if (rc != NGX_OK) {
+        return rc;
+    }
+    g->scc_components = static_cast<int64_t>(count);
+    return NGX_OK;
+}
+
 int ensure_source_order(ngx_graph* g) {
+    if (g->parts.size() == 1 && !g->order_grouped && static_cast<int64_t>(g->source_order.size()) == g->n_total) {
+        // a graph of several strongly connected components: the sources of each component together (in their
+        // locality order), so that a tile's sources reach the same vertices (StronglyConnectedComponents.h:34-35)
+        if (const int rc = ensure_components(g); rc != NGX_OK) {
+            return rc;
+        }
+        if (g->scc_components > 1) {
+            std::vector<int32_t> comp(static_cast<size_t>(g->n));
+            uint64_t count = 0, largest = 0;
+            if (const int rc = ngx_scc(g, comp.data(), &count, &largest, nullptr); rc != NGX_OK) {
+                return rc;
+            }
+            std::stable_sort(g->source_order.begin(), g->source_order.end(),
+                             [&](int32_t a, int32_t b) { return comp[static_cast<size_t>(a)] < comp[static_cast<size_t>(b)]; });
+        }
+        g->order_grouped = true;
+        return NGX_OK;
+    }
     if (static_cast<int64_t>(g->source_order.size()) == g->n_total) {
         return NGX_OK;
     }
@@ -666,7 +709,7 @@ int ensure_source_order(ngx_graph* g) {
     order.reserve(static_cast<size_t>(n));
     append_source_order(n, rows.data(), arcs.data(), order);
     g->source_order = std::move(order);
-    return NGX_OK;
+    return ensure_source_order(g);  // then grouped by component
 }
 
 int ensure_stored_of_user(ngx_graph* g) {

@@ -112,6 +112,12 @@ struct ngx_graph {
     // all-sources processing order of each graph (graph-local ids, graph after graph): clusters of nearby vertices,
     // so that the 32 sources of a tile reach most vertices in the same phases and share arc passes
     ngx::HostVector<int32_t> source_order;
+    // strongly connected components of a single graph (ensure_components; 0 = not computed yet). When there are
+    // several, the all-sources order keeps each component's sources together and tiles list the vertices they reach.
+    int64_t scc_components = 0;   // -1: not known (the pre-pass gave up)
+    bool order_grouped = false;
+    int64_t scc_pass_cap = 0;     // SCC passes allowed (0 = no cap; the APSP pre-pass sets one)
+    int64_t scc_passes = 0;
 
     ngx::DeviceCsr csr(int metric) const {
         return ngx::DeviceCsr{ n, m_stored, d_row_ptr, metric == NGX_METRIC_INVERSE ? d_arcs_inverse : d_arcs_regular };
@@ -155,6 +161,9 @@ int build_graph_on_device(const ngx_csr* csr, ngx_graph* g);
 
 // The all-sources order of a single-graph handle, computed from its device arrays when a run first needs it.
 int ensure_source_order(ngx_graph* g);
+
+// The strongly connected components of a single-graph handle (ngx_scc on its device), counted once per handle.
+int ensure_components(ngx_graph* g);
 
 // Copies a device-built handle's stored index of every caller arc to the host (ngx_graph_update_weights needs it).
 int ensure_stored_of_user(ngx_graph* g);

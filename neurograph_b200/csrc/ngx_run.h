@@ -41,6 +41,7 @@ struct TileJob {
     int64_t num_sources = 0;
     int64_t n_max = 0;                 // largest graph (workspace slot size)
     double plain_delta = 1.0;          // bucket width of the plain form (single graph)
+    bool track_reach = false;          // keep per-tile reach lists (a graph of several strongly connected components)
 };
 
 // Device buffers of the DAG passes: per-vertex betweenness and per-arc gradients in 128-bit fixed point.

@@ -143,6 +143,9 @@ __global__ void scc_count_kernel(int64_t n, const int32_t* comp, unsigned long l
 template <typename Launch>
 int until_stable(ngx_graph* g, int* d_flag, int* h_flag, int64_t max_passes, Launch launch) {
     for (int64_t pass = 0; pass <= max_passes; ++pass) {
+        if (g->scc_pass_cap > 0 && ++g->scc_passes > g->scc_pass_cap) {
+            return fail(NGX_TIMEOUT, "ngx_scc: more passes than the pre-pass allows");
+        }
         NGX_CUDA_TRY(cudaMemsetAsync(d_flag, 0, sizeof(int), g->stream));
         launch();
         NGX_CUDA_TRY(cudaGetLastError());

@@ -229,7 +229,10 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
     }
     const int64_t n = job.n_max;
     const int64_t resident = static_cast<int64_t>(g->sm_count) * per_sm;
-    const size_t data_bytes = sssp_slot_bytes(n, width) + (tile_mode != kModeApsp ? brandes_slot_bytes(n, tile_mode == kModeGrad) : 0);
+    const bool track = batched && job.track_reach;
+    const size_t reach_bytes = track ? static_cast<size_t>(n) * 8 + 512 : 0;  // reach mask + reached list
+    const size_t data_bytes =
+        sssp_slot_bytes(n, width) + (tile_mode != kModeApsp ? brandes_slot_bytes(n, tile_mode == kModeGrad) : 0) + reach_bytes;
     const size_t budget = workspace_budget(g);
     // the group size decides the group storage per slot, which the slot count must leave room for
     const int64_t affordable = static_cast<int64_t>(budget / (data_bytes + static_cast<size_t>(group_stride_words(kMaxGroupSize)) * 8));
@@ -274,6 +277,13 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
     p.group_size = group;
     p.group_stride = group_stride_words(group);
     p.group_ws = group_ws;
+    if (track) {
+        ws = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(ws) + 255) & ~uintptr_t(255));
+        p.ws_reach = reinterpret_cast<uint32_t*>(ws);
+        ws += static_cast<size_t>(slots) * n * 4;
+        p.ws_touched = reinterpret_cast<int32_t*>(ws);
+        ws += static_cast<size_t>(slots) * n * 4;
+    }
     BrandesParams bp{};
     if (tile_mode != kModeApsp) {
         const size_t nt = static_cast<size_t>(n) * kTile;
@@ -566,6 +576,7 @@ int run_sources(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const st
     job.num_sources = num_sources;
     job.n_max = part.n;
     job.plain_delta = delta;
+    job.track_reach = g->scc_components > 1;
     return launch_tiles(g, opts, tile_mode, job, hist_bins, hist_max, o, extra, ms, true);
 }
 
@@ -622,6 +633,10 @@ int run_apsp(ngx_graph* g, const ngx_apsp_opts* caller_opts, ngx_apsp_result* re
     }
     NGX_CUDA_TRY(cudaSetDevice(g->device));
     *g->h_abort = 0;
+    // the strongly connected components decide whether tiles keep reach lists (several components)
+    if (const int rc = ensure_components(g); rc != NGX_OK) {
+        return rc;
+    }
     std::vector<int32_t> sources;
     if (const int rc = prepare_sources(g, opts, sources); rc != NGX_OK) {
         return rc;

@@ -73,6 +73,10 @@ struct SsspParams {
     uint32_t* ws_far;              // slots * n
     int32_t* ws_queue;             // slots * 2n
     uint32_t* ws_stamp;            // slots * n
+    // reach lists (graphs of several strongly connected components; nullptr otherwise): per vertex the tile's
+    // sources that reached it, and the list of the vertices reached, so that per-tile passes visit only those
+    uint32_t* ws_reach;            // slots * n
+    int32_t* ws_touched;           // slots * n
     // groups: the CTAs blockIdx.x / group_size share slot (blockIdx.x / group_size) and its tiles
     int group_size;
     int64_t group_stride;          // words of group storage per slot (group_stride_words)
@@ -112,7 +116,7 @@ struct TileShared {
     int next_len;
     unsigned long long active_pairs;  // reached (vertex, source) pairs other than the sources, counted by the DAG pass
     int grab;                       // next queue entry handed to a warp in the current near iteration
-    int pad;
+    int touched_len;                // vertices the tile has reached so far (reach lists; see SsspParams::ws_touched)
     // the state of a CTA that left its group (ngx_group.cuh): no tile, nothing queued, pending or levelled
     __device__ void halt() {
         stop = 1;
@@ -151,6 +155,19 @@ __device__ __forceinline__ int expand_chunk(int qlen, int group_warps) {
     return c < 1 ? 1 : (c > 32 ? 32 : c);
 }
 
+// The reach list of a tile: mask[v] has bit s set once source s reached v; a vertex is appended to list[] (length
+// *len) by the relaxation that gives it its first finite distance of the tile. Disabled when mask is nullptr.
+struct Reach {
+    uint32_t* mask;
+    int32_t* list;
+    int* len;
+    __device__ __forceinline__ void add(int v, uint32_t bit) const {
+        if (atomicOr(&mask[v], bit) == 0u) {
+            list[atomicAdd(len, 1)] = v;
+        }
+    }
+};
+
 // ------------------------------------------------------------------------------------------ batched form
 // Expands vertex v for the k sources pending on it. The deg(v) x k (arc, source) pairs are spread over the 32 lanes:
 // pair p = 32 i + lane takes arc p / k and the (p % k)-th pending source, so no lane idles when few sources are
@@ -169,7 +186,7 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
                                                unsigned long long* __restrict__ dist, uint32_t* pend_nxt, uint32_t* far, int32_t* q_nxt,
                                                int* qlen_nxt, uint32_t* stamp, unsigned next_stamp, double theta, unsigned long long& expansions,
                                                unsigned long long& lane_expansions, unsigned long long* pred_key, uint32_t* tie,
-                                               unsigned long long* last) {
+                                               unsigned long long* last, const Reach& reach) {
     const uint32_t amask0 = amask;
     int k = __popc(amask);
     // lane r < k holds the r-th pending source and its distance to v
@@ -251,6 +268,9 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
                     }
                     if (nb < old) {
                         const uint32_t bit = 1u << src[u];
+                        if (reach.mask != nullptr && old == kInfBits) {
+                            reach.add(x[u], bit);  // the first distance of (x, s): x joins the tile's reached vertices
+                        }
                         if (nd[u] < theta) {
                             atomicOr(&pend_nxt[x[u]], bit);
                             push = atomicExch(&stamp[x[u]], next_stamp) != next_stamp;
@@ -286,7 +306,7 @@ __device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* 
                                              unsigned long long* __restrict__ dist, uint32_t* pend_cur, uint32_t* pend_nxt, uint32_t* far,
                                              int32_t* q_nxt, int* qlen_nxt, uint32_t* stamp, unsigned next_stamp, double theta,
                                              unsigned long long& expansions, unsigned long long& lane_expansions, unsigned long long* pred_key,
-                                             uint32_t* tie, unsigned long long* last) {
+                                             uint32_t* tie, unsigned long long* last, const Reach& reach) {
     for (;;) {
         int base = 0;
         if (lane == 0) {
@@ -324,7 +344,7 @@ __device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* 
             const int64_t beg = __shfl_sync(kFullMask, bj, j);
             const int deg = __shfl_sync(kFullMask, dj, j);
             batched_expand<kUnroll, kTrack>(g, v, amask, beg, deg, lane, dist, pend_nxt, far, q_nxt, qlen_nxt, stamp, next_stamp, theta,
-                                            expansions, lane_expansions, pred_key, tie, last);
+                                            expansions, lane_expansions, pred_key, tie, last, reach);
         }
     }
 }
@@ -366,6 +386,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     int32_t* q0 = p.ws_queue + slot * 2 * n_slot;
     int32_t* q1 = q0 + n_slot;
     uint32_t* stamp = p.ws_stamp + slot * n_slot;
+    const Reach reach{ p.ws_reach != nullptr ? p.ws_reach + slot * n_slot : nullptr, p.ws_touched != nullptr ? p.ws_touched + slot * n_slot : nullptr,
+                       &ctl()->touched_len };
     const int64_t nt_slot = n_slot * kTile;
     double* sigma = nullptr;
     double* delta = nullptr;
@@ -413,6 +435,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         pend1[i] = 0u;
         far[i] = 0u;
         stamp[i] = 0u;
+        if (reach.mask != nullptr) {
+            reach.mask[i] = 0u;
+        }
     }
     for (int i = tid; i < 2 * kTile * kAccDigits; i += blockDim.x) {
         smem[i] = 0ull;
@@ -441,6 +466,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             c.min_bits = kInfBits;
             c.active_pairs = 0;
             c.grab = 0;
+            c.touched_len = 0;
             if (c.tile < p.num_tiles) {
                 const WorkItem it = p.items != nullptr ? p.items[c.tile] : WorkItem{ 0, static_cast<int32_t>(c.tile) };
                 c.theta = p.graphs[it.graph].delta;
@@ -480,6 +506,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 if (atomicExch(&stamp[v], s.stamp) != s.stamp) {
                     q0[atomicAdd(&ctl()->qlen[0], 1)] = v;
                 }
+                if (reach.mask != nullptr) {
+                    reach.add(v, 1u << lane);
+                }
             }
         }
         grp().sync(s, s_bar);
@@ -502,7 +531,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 expand_queue<kUnroll, kMode != kModeApsp>(g, q_cur, qlen, lane, &ctl()->grab, expand_chunk(qlen, NGX_GWARPS), dist, pend_cur, pend_nxt,
                                                           far, q_nxt, &ctl()->qlen[cur ^ 1], stamp, next_stamp, theta, expansions, lane_expansions,
                                                           reinterpret_cast<unsigned long long*>(sigma), tie,
-                                                          reinterpret_cast<unsigned long long*>(delta));
+                                                          reinterpret_cast<unsigned long long*>(delta), reach);
                 grp().sync(s, s_bar, [&](volatile TileShared& c) {
                     c.qlen[cur] = 0;
                     c.cur = cur ^ 1;
@@ -526,17 +555,21 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             }
             // bucket step, pass 1: smallest pending far distance (min_bits is +inf here: reset at the tile's start and
             // after every bucket step)
+            // (over the tile's reached vertices when it keeps a reach list: no other vertex has far marks)
+            const int64_t span = reach.mask != nullptr ? static_cast<int64_t>(s.touched_len) : n;
             unsigned long long local_min = kInfBits;
-            for (int64_t vb = static_cast<int64_t>(NGX_GW) * 32; vb < n; vb += static_cast<int64_t>(NGX_GWARPS) * 32) {
-                const int64_t v = vb + lane;
-                const uint32_t fm = v < n ? __ldcg(&far[v]) : 0u;
+            for (int64_t vb = static_cast<int64_t>(NGX_GW) * 32; vb < span; vb += static_cast<int64_t>(NGX_GWARPS) * 32) {
+                const int64_t i = vb + lane;
+                const int64_t v = i < span ? (reach.mask != nullptr ? static_cast<int64_t>(__ldcg(&reach.list[i])) : i) : 0;
+                const uint32_t fm = i < span ? __ldcg(&far[v]) : 0u;
                 unsigned any = __ballot_sync(kFullMask, fm != 0u);
                 while (any != 0u) {
                     const int l = __ffs(any) - 1;
                     any &= any - 1u;
                     const uint32_t f = __shfl_sync(kFullMask, fm, l);
+                    const int64_t vl = __shfl_sync(kFullMask, v, l);
                     if ((f >> lane) & 1u) {
-                        const unsigned long long d = __ldcg(&dist[(vb + l) * kTile + lane]);
+                        const unsigned long long d = __ldcg(&dist[vl * kTile + lane]);
                         local_min = d < local_min ? d : local_min;
                     }
                 }
@@ -564,21 +597,22 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             const int cur = s.cur;
             uint32_t* pend_cur = cur ? pend1 : pend0;
             int32_t* q_cur = cur ? q1 : q0;
-            for (int64_t vb = static_cast<int64_t>(NGX_GW) * 32; vb < n; vb += static_cast<int64_t>(NGX_GWARPS) * 32) {
-                const int64_t v = vb + lane;
-                const uint32_t fm = v < n ? __ldcg(&far[v]) : 0u;
+            for (int64_t vb = static_cast<int64_t>(NGX_GW) * 32; vb < span; vb += static_cast<int64_t>(NGX_GWARPS) * 32) {
+                const int64_t i = vb + lane;
+                const int64_t v = i < span ? (reach.mask != nullptr ? static_cast<int64_t>(__ldcg(&reach.list[i])) : i) : 0;
+                const uint32_t fm = i < span ? __ldcg(&far[v]) : 0u;
                 unsigned any = __ballot_sync(kFullMask, fm != 0u);
                 while (any != 0u) {
                     const int l = __ffs(any) - 1;
                     any &= any - 1u;
                     const uint32_t f = __shfl_sync(kFullMask, fm, l);
+                    const int64_t vv = __shfl_sync(kFullMask, v, l);
                     bool near = false;
                     if ((f >> lane) & 1u) {
-                        near = __longlong_as_double(static_cast<long long>(__ldcg(&dist[(vb + l) * kTile + lane]))) < theta;
+                        near = __longlong_as_double(static_cast<long long>(__ldcg(&dist[vv * kTile + lane]))) < theta;
                     }
                     const unsigned nmask = __ballot_sync(kFullMask, near);
                     if (nmask != 0u && lane == 0) {
-                        const int64_t vv = vb + l;
                         far[vv] = f & ~nmask;
                         pend_cur[vv] = nmask;
                         q_cur[atomicAdd(&ctl()->qlen[cur], 1)] = static_cast<int32_t>(vv);
@@ -773,7 +807,19 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         const int my_src = s_src[lane];
         const bool valid = lane < nsrc;
         unsigned long long unreach = 0, arcs = 0, mx = 0, overflow = 0;
-        for (int64_t v = NGX_GW; v < n; v += NGX_GWARPS) {
+        // APSP with a reach list visits the reached vertices only: every other vertex is unreached by every source and
+        // its state was never touched; the DAG passes have written every vertex's rows, and distance rows need every
+        // vertex, so those visit all of them
+        const bool by_list = reach.mask != nullptr && kMode == kModeApsp && p.out.rows == nullptr;
+        const int64_t span = by_list ? static_cast<int64_t>(s.touched_len) : n;
+        if (by_list && valid && grp().rank == 0 && warp == 0) {
+            unreach = static_cast<unsigned long long>(n - span);
+        }
+        for (int64_t i = NGX_GW; i < span; i += NGX_GWARPS) {
+            const int64_t v = by_list ? static_cast<int64_t>(__ldcg(&reach.list[i])) : i;
+            if (reach.mask != nullptr && lane == 0) {
+                reach.mask[v] = 0u;
+            }
             unsigned long long* slot_ptr = &dist[v * kTile + lane];
             const unsigned long long bits = __ldcg(slot_ptr);
             *slot_ptr = kInfBits;
