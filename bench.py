@@ -115,7 +115,7 @@ def make_graph(n, degree, length_scale=WORKLOAD["length_scale"], sigma=1.0, work
 def workload_overrides(args):
     """Config keys that differ from the default connectome (other generator parameters on the same code path)."""
     if args.workload == "c1":
-        return dict(WORKLOAD_C1)
+        return {k: v for k, v in WORKLOAD_C1.items() if k != "n"}  # n comes from the generated graph
     if (args.n, args.degree, args.length_scale, args.sigma) == (WORKLOAD["n"], WORKLOAD["mean_degree"], WORKLOAD["length_scale"], 1.0):
         return {}
     return {"workload": f"single graph: synthetic connectome N={args.n}, out-degree Poisson({args.degree:g}), kernel "
