@@ -26,7 +26,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libngx_b200.so")
+LIB_PATH = os.environ.get("NGX_B200_LIBRARY") or os.path.join(HERE, "lib", "libngx_b200.so")
 
 NGX_OK = 0
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARGUMENT", 2: "OUT_OF_MEMORY", 3: "CUDA_ERROR", 4: "TIMEOUT", 5: "ABORTED", 6: "UNSUPPORTED"}

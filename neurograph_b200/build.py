@@ -22,9 +22,7 @@ LIB = os.path.join(LIB_DIR, "libngx_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
-# -dlcm=cg: plain global loads are cached in L2 only, never in an SM's L1, which is not coherent across SMs: the CTAs of
-# a tile group read what other CTAs wrote before their last group barrier. Read-only arrays go through __ldg.
-NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xptxas", "-dlcm=cg", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
               "--expt-relaxed-constexpr"]
 
 

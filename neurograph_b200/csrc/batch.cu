@@ -498,8 +498,9 @@ int ngx_batch_autotune(ngx_graph* g, int task, double* class_scales) {
             }
             int best_group = 1;
             for (const int gs : { 2, 4 }) {
-                aopts.block_threads = best_shape.block;
-                aopts.ctas_per_sm = best_shape.per_sm;
+                // groups of several CTAs per tile run with the default block shape
+                aopts.block_threads = kShapes[0].block;
+                aopts.ctas_per_sm = kShapes[0].per_sm;
                 aopts.tile_ctas = gs;
                 double rate = 0.0;
                 if (const int rc = time_wave(g, mode, gi, scale, aopts, &rate); rc != NGX_OK) {
@@ -509,6 +510,7 @@ int ngx_batch_autotune(ngx_graph* g, int task, double* class_scales) {
                 if (rate > best_rate) {
                     best_rate = rate;
                     best_group = gs;
+                    best_shape = kShapes[0];
                 }
             }
             ngx_tuning& t = g->tuned[mode];

@@ -586,6 +586,7 @@ int create_graphs(const ngx_csr* csrs, int64_t count, int device, ngx_graph** ou
     }
     g->device = device;
     g->sm_count = prop.multiProcessorCount;
+    g->l2_bytes = static_cast<size_t>(prop.l2CacheSize);
     if (!on_device) {
         g->n_total = h.n_total;
         g->m_user = h.m_user;

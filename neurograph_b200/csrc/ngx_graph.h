@@ -49,6 +49,7 @@ struct GraphPart {
 struct ngx_graph {
     int device = 0;
     int sm_count = 0;
+    size_t l2_bytes = 0;  // the device's L2 cache
     cudaStream_t stream = nullptr;        // the stream all work of the graph is issued on
     cudaStream_t own_stream = nullptr;    // created with the graph; `stream` points here unless the caller set one
 

@@ -4,8 +4,8 @@
 // control block: queue lengths, bucket bound, level bounds, counters) lives in global memory and is changed only
 // (a) by atomics on counters and (b) by the last CTA to arrive at a group barrier, which applies the barrier's update
 // before it releases the others. After every barrier each CTA copies the control block into its shared memory, so
-// between barriers all CTAs of a group read the same values. With size 1 the barrier is __syncthreads() and the update
-// runs on thread 0; with size > 1 the launch is cooperative (all CTAs resident) and every wait is bounded in time: a CTA
+// between barriers all CTAs of a group read the same values. With size 1 the control block may be the CTA's own shared
+// copy (ctl == &local), the barrier is __syncthreads() and the update runs on thread 0; with size > 1 the launch is cooperative (all CTAs resident) and every wait is bounded in time: a CTA
 // that waits longer than kGroupWaitNs records NGX_TIMEOUT in the run's error flag and stops, and so, bounded the same
 // way, do the others.
 #pragma once
@@ -102,7 +102,9 @@ struct Group {
                 }
             }
             static_assert(sizeof(Ctl) % 8 == 0, "control block must be whole 8-byte words");
-            copy_from_l2(&local, ctl, static_cast<int>(sizeof(Ctl) / 8));
+            if (ctl != &local) {
+                copy_from_l2(&local, ctl, static_cast<int>(sizeof(Ctl) / 8));
+            }
             if (timed_out) {
                 bar_target = kGroupLeft;
                 local.halt();

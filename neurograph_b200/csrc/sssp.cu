@@ -152,9 +152,19 @@ int device_error_status(int code) {
     }
 }
 
-// The instantiation for a block size; 256 threads with ctas_per_sm >= 4 selects the 4-CTA (64-register) build.
+// The instantiation for a block size; 256 threads with ctas_per_sm >= 4 selects the 4-CTA (64-register) build. Tile
+// groups of several CTAs (multi) and reach lists (reach) are built for the default shape only (512 threads x 2 CTAs per
+// SM); nullptr for other combinations.
 template <int kMode>
-const void* tile_kernel_for_block(int block, int ctas_per_sm = 0) {
+const void* tile_kernel_for_block(int block, int ctas_per_sm, bool reach, bool multi) {
+    if (reach || multi) {
+        if (block != kBatchedDefaultBlock) {
+            return nullptr;
+        }
+        if (multi && reach) return reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 512, 2, true, true>);
+        if (multi) return reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 512, 2, true, false>);
+        return reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 512, 2, false, true>);
+    }
     switch (block) {
     case 256:
         return ctas_per_sm >= 4 ? reinterpret_cast<const void*>(&tile_kernel<kMode, kBatchedUnroll, 256, 4>)
@@ -165,17 +175,29 @@ const void* tile_kernel_for_block(int block, int ctas_per_sm = 0) {
     }
 }
 
-// CTAs per tile group: the caller's choice, else 1 unless the device memory affords fewer workspace slots than there
-// are resident CTAs (and tiles to fill them), in which case each slot gets enough CTAs to use every SM.
-int choose_group_size(int requested, int64_t resident, int64_t num_tiles, int64_t affordable_slots) {
+// CTAs per tile group: the caller's choice, else the largest of three needs.
+//  * L2 residency: the distance phase of a tile touches about 280 bytes per vertex (its 256-byte distance rows, pending
+//    marks, queues); when a tile fits in L2, as many tiles are kept in flight as fit in 90 % of it, each worked by
+//    resident / that many CTAs (measured: 4 tiles of 74 CTAs on the 100,000-vertex connectome, +20 % for APSP and
+//    +18 % for Brandes over one CTA per tile).
+//  * Few tiles: a run with fewer tiles than resident CTAs gives each tile the CTAs the others would leave idle.
+//  * Memory: when the device affords fewer workspace slots than that, each slot gets enough CTAs to use every SM.
+int choose_group_size(int requested, int64_t resident, int64_t num_tiles, int64_t affordable_slots, int64_t n, size_t l2_bytes) {
     if (requested > 0) {
         return static_cast<int>(std::min<int64_t>({ static_cast<int64_t>(requested), resident, static_cast<int64_t>(kMaxGroupSize) }));
     }
-    const int64_t busy = std::min(resident, num_tiles);  // CTAs a run of single-CTA tiles would keep busy
-    if (affordable_slots >= busy) {
-        return 1;
+    int64_t group = 1;
+    const double tile_bytes = 280.0 * static_cast<double>(std::max<int64_t>(n, 1));
+    const double room = 0.9 * static_cast<double>(l2_bytes);
+    if (tile_bytes <= 0.5 * room) {
+        const int64_t in_flight = std::max<int64_t>(1, static_cast<int64_t>(room / tile_bytes));
+        group = std::max<int64_t>(group, resident / in_flight);
     }
-    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(resident / std::max<int64_t>(1, affordable_slots), kMaxGroupSize)));
+    group = std::max<int64_t>(group, resident / std::max<int64_t>(1, num_tiles));
+    if (affordable_slots < std::min(resident, num_tiles)) {
+        group = std::max<int64_t>(group, resident / std::max<int64_t>(1, affordable_slots));
+    }
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({ group, resident, static_cast<int64_t>(kMaxGroupSize) })));
 }
 
 // Launches the tile kernel: cooperative when several CTAs share a tile (they wait for one another at group barriers,
@@ -210,10 +232,19 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
     }
 
     const void* kernel = reinterpret_cast<const void*>(&sssp_plain_kernel);
+    // reach lists (several strongly connected components) and tile groups run with the default block shape only
+    const bool default_shape = block == kBatchedDefaultBlock && (opts->ctas_per_sm == 0 || opts->ctas_per_sm >= 2);
+    if (batched && opts->tile_ctas > 1 && !default_shape) {
+        return fail(NGX_INVALID_ARGUMENT, "tile groups (tile_ctas > 1) run with the default block shape (512 threads, 2 CTAs per SM)");
+    }
+    const bool track = batched && job.track_reach && default_shape;
+    const auto pick = [&](bool reach, bool multi) -> const void* {
+        return tile_mode == kModeBrandes ? tile_kernel_for_block<kModeBrandes>(block, opts->ctas_per_sm, reach, multi)
+               : tile_mode == kModeGrad  ? tile_kernel_for_block<kModeGrad>(block, opts->ctas_per_sm, reach, multi)
+                                         : tile_kernel_for_block<kModeApsp>(block, opts->ctas_per_sm, reach, multi);
+    };
     if (batched) {
-        kernel = tile_mode == kModeBrandes ? tile_kernel_for_block<kModeBrandes>(block, opts->ctas_per_sm)
-                 : tile_mode == kModeGrad  ? tile_kernel_for_block<kModeGrad>(block, opts->ctas_per_sm)
-                                           : tile_kernel_for_block<kModeApsp>(block, opts->ctas_per_sm);
+        kernel = pick(track, false);
         if (kernel == nullptr) {
             return fail(NGX_INVALID_ARGUMENT, "batched mode supports block_threads 256, 384 or 512");
         }
@@ -229,14 +260,17 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
     }
     const int64_t n = job.n_max;
     const int64_t resident = static_cast<int64_t>(g->sm_count) * per_sm;
-    const bool track = batched && job.track_reach;
     const size_t reach_bytes = track ? static_cast<size_t>(n) * 8 + 512 : 0;  // reach mask + reached list
     const size_t data_bytes =
         sssp_slot_bytes(n, width) + (tile_mode != kModeApsp ? brandes_slot_bytes(n, tile_mode == kModeGrad) : 0) + reach_bytes;
     const size_t budget = workspace_budget(g);
     // the group size decides the group storage per slot, which the slot count must leave room for
     const int64_t affordable = static_cast<int64_t>(budget / (data_bytes + static_cast<size_t>(group_stride_words(kMaxGroupSize)) * 8));
-    const int group = batched ? choose_group_size(opts->tile_ctas, resident, num_tiles, affordable) : 1;
+    const int group = batched && default_shape ? choose_group_size(opts->tile_ctas, resident, num_tiles, affordable, n, g->l2_bytes) : 1;
+    if (group > 1) {
+        kernel = pick(track, true);  // the same shape and occupancy, built for groups
+        NGX_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    }
     const size_t group_bytes = static_cast<size_t>(group_stride_words(group)) * 8;
     const size_t slot_bytes = data_bytes + group_bytes;
     int64_t slots = std::min<int64_t>(num_tiles, resident / group);
@@ -386,7 +420,7 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
 int launch_apsp_in_workspace(ngx_graph* g, const ngx_apsp_opts* opts, const TileJob& job, int64_t hist_bins, double hist_max, RunOutputs& o, void* ws,
                              size_t ws_bytes) {
     const int block = opts->block_threads > 0 ? opts->block_threads : kBatchedDefaultBlock;
-    const void* kernel = tile_kernel_for_block<kModeApsp>(block, opts->ctas_per_sm);
+    const void* kernel = tile_kernel_for_block<kModeApsp>(block, opts->ctas_per_sm, false, false);
     if (kernel == nullptr) {
         return fail(NGX_INVALID_ARGUMENT, "batched mode supports block_threads 256, 384 or 512");
     }

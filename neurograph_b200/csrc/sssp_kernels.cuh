@@ -140,12 +140,14 @@ inline int64_t group_stride_words(int group_size) {
     return (words + 31) / 32 * 32;  // 256-byte aligned slots
 }
 
-// This CTA's view of its tile group (see SsspParams::group_*).
+// This CTA's view of its tile group (see SsspParams::group_*). A group of one CTA keeps the control block in the CTA's
+// shared memory (`local`), where its counters are shared-memory atomics; larger groups keep it in global memory.
 template <typename Params>
-__device__ __forceinline__ Group<TileShared> tile_group(const Params& p) {
+__device__ __forceinline__ Group<TileShared> tile_group(const Params& p, TileShared* local) {
     unsigned long long* const gws = p.group_ws + (blockIdx.x / p.group_size) * p.group_stride;
-    return Group<TileShared>{ reinterpret_cast<TileShared*>(gws), reinterpret_cast<GroupBarrier*>(gws + kCtlWords), gws + kCtlWords + 1,
-                              p.group_size, static_cast<int>(blockIdx.x % p.group_size), p.error };
+    TileShared* const ctl = p.group_size == 1 ? local : reinterpret_cast<TileShared*>(gws);
+    return Group<TileShared>{ ctl, reinterpret_cast<GroupBarrier*>(gws + kCtlWords), gws + kCtlWords + 1, p.group_size,
+                              static_cast<int>(blockIdx.x % p.group_size), p.error };
 }
 
 // Queue entries a warp takes at a time: all 32 when the near queue is long, fewer towards the end of a frontier so
@@ -181,7 +183,7 @@ struct Reach {
 // distance of the latest expansion, and sources whose distance has not changed since are dropped from the next.
 // The caller has taken v's pending mask (amask, non-zero), cleared it and v's superseded far marks, and read its row
 // offsets (beg, deg): see expand_queue.
-template <int kUnroll, bool kTrack>
+template <int kUnroll, bool kTrack, bool kReach>
 __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32_t amask, int64_t beg, int deg, int lane,
                                                unsigned long long* __restrict__ dist, uint32_t* pend_nxt, uint32_t* far, int32_t* q_nxt,
                                                int* qlen_nxt, uint32_t* stamp, unsigned next_stamp, double theta, unsigned long long& expansions,
@@ -268,7 +270,7 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
                     }
                     if (nb < old) {
                         const uint32_t bit = 1u << src[u];
-                        if (reach.mask != nullptr && old == kInfBits) {
+                        if (kReach && old == kInfBits) {
                             reach.add(x[u], bit);  // the first distance of (x, s): x joins the tile's reached vertices
                         }
                         if (nd[u] < theta) {
@@ -301,7 +303,7 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
 // One near iteration of a tile: the warps of the group take the queue `chunk` entries at a time from a shared counter;
 // lane j fetches entry j's vertex, its pending mask, far marks and row offsets (one round of parallel loads), clears the
 // mask and the superseded far marks, and the warp then expands the vertices one after another.
-template <int kUnroll, bool kTrack>
+template <int kUnroll, bool kTrack, bool kReach>
 __device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* q_cur, int qlen, int lane, int* grab, int chunk,
                                              unsigned long long* __restrict__ dist, uint32_t* pend_cur, uint32_t* pend_nxt, uint32_t* far,
                                              int32_t* q_nxt, int* qlen_nxt, uint32_t* stamp, unsigned next_stamp, double theta,
@@ -343,13 +345,15 @@ __device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* 
             const int v = __shfl_sync(kFullMask, vj, j);
             const int64_t beg = __shfl_sync(kFullMask, bj, j);
             const int deg = __shfl_sync(kFullMask, dj, j);
-            batched_expand<kUnroll, kTrack>(g, v, amask, beg, deg, lane, dist, pend_nxt, far, q_nxt, qlen_nxt, stamp, next_stamp, theta,
+            batched_expand<kUnroll, kTrack, kReach>(g, v, amask, beg, deg, lane, dist, pend_nxt, far, q_nxt, qlen_nxt, stamp, next_stamp, theta,
                                             expansions, lane_expansions, pred_key, tie, last, reach);
         }
     }
 }
 
-template <int kMode, int kUnroll, int kBlock, int kMinBlocks>
+// kMulti: the launch may put several CTAs on a tile (p.group_size > 1, cooperative launch); without it the group is
+// the CTA itself, whose control block lives in shared memory. kReach: the tiles keep reach lists.
+template <int kMode, int kUnroll, int kBlock, int kMinBlocks, bool kMulti = false, bool kReach = false>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspParams p, const BrandesParams b) {
     extern __shared__ __align__(16) unsigned long long smem[];
     unsigned long long* s_acc_sum = smem;                                // kTile * kAccDigits
@@ -370,13 +374,29 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     // The CTAs blockIdx.x / group_size share workspace slot `slot` and work on its tiles together. The group's
     // pointers and indices are recomputed from the launch parameters where they are used (fewer live registers).
     const int64_t slot = blockIdx.x / p.group_size;
-    const auto grp = [&]() { return tile_group(p); };
-    const auto ctl = [&]() { return reinterpret_cast<TileShared*>(p.group_ws + (blockIdx.x / p.group_size) * p.group_stride); };
+    const auto grp = [&]() { return tile_group(p, &s); };
+    const auto ctl = [&]() {
+        return kMulti ? reinterpret_cast<TileShared*>(p.group_ws + (blockIdx.x / p.group_size) * p.group_stride) : &s;
+    };
+    // a group barrier whose last arrival applies `update` to the control block (a block barrier without kMulti)
+    const auto sync = [&](auto&& update) {
+        if constexpr (kMulti) {
+            grp().sync(s, s_bar, update);
+        } else {
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                update(s);
+            }
+            __syncthreads();
+        }
+    };
+    const auto sync0 = [&]() { sync([](volatile TileShared&) {}); };
     // this thread's (warp's) index among the group's threads (warps), and their counts
-#define NGX_GT (static_cast<int64_t>(blockIdx.x % p.group_size) * blockDim.x + threadIdx.x)
-#define NGX_GTHREADS (static_cast<int64_t>(p.group_size) * blockDim.x)
-#define NGX_GW (static_cast<int>(blockIdx.x % p.group_size) * static_cast<int>(blockDim.x >> 5) + static_cast<int>(threadIdx.x >> 5))
-#define NGX_GWARPS (p.group_size * static_cast<int>(blockDim.x >> 5))
+#define NGX_GT (kMulti ? static_cast<int64_t>(blockIdx.x % p.group_size) * blockDim.x + threadIdx.x : static_cast<int64_t>(threadIdx.x))
+#define NGX_GTHREADS (kMulti ? static_cast<int64_t>(p.group_size) * blockDim.x : static_cast<int64_t>(blockDim.x))
+#define NGX_GW (kMulti ? static_cast<int>(blockIdx.x % p.group_size) * static_cast<int>(blockDim.x >> 5) + static_cast<int>(threadIdx.x >> 5) \
+                       : static_cast<int>(threadIdx.x >> 5))
+#define NGX_GWARPS (kMulti ? p.group_size * static_cast<int>(blockDim.x >> 5) : static_cast<int>(blockDim.x >> 5))
     unsigned long long expansions = 0, lane_expansions = 0;
 
     unsigned long long* dist = p.ws_dist + slot * n_slot * kTile;
@@ -386,8 +406,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     int32_t* q0 = p.ws_queue + slot * 2 * n_slot;
     int32_t* q1 = q0 + n_slot;
     uint32_t* stamp = p.ws_stamp + slot * n_slot;
-    const Reach reach{ p.ws_reach != nullptr ? p.ws_reach + slot * n_slot : nullptr, p.ws_touched != nullptr ? p.ws_touched + slot * n_slot : nullptr,
-                       &ctl()->touched_len };
+    // reach lists: compiled in only for the kernels that keep them (kReach), so the others carry no extra registers
+    const Reach reach{ kReach ? p.ws_reach + slot * n_slot : nullptr, kReach ? p.ws_touched + slot * n_slot : nullptr,
+                       kReach ? &ctl()->touched_len : nullptr };
     const int64_t nt_slot = n_slot * kTile;
     double* sigma = nullptr;
     double* delta = nullptr;
@@ -435,7 +456,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         pend1[i] = 0u;
         far[i] = 0u;
         stamp[i] = 0u;
-        if (reach.mask != nullptr) {
+        if (kReach) {
             reach.mask[i] = 0u;
         }
     }
@@ -452,7 +473,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
 
     for (;;) {
         // ---- the next work item, taken for the whole group; the slot's queue stamp counts on across tiles
-        grp().sync(s, s_bar, [&](volatile TileShared& c) {
+        sync([&](volatile TileShared& c) {
             if (first_tile) {
                 c.stamp = 1u;
             }
@@ -498,7 +519,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             s_max[tid] = 0ull;
         }
         __syncthreads();
-        if (grp().rank == 0 && warp == 0) {
+        if ((!kMulti || grp().rank == 0) && warp == 0) {
             const int v = s_src[lane];
             if (v >= 0) {
                 dist[static_cast<int64_t>(v) * kTile + lane] = 0ull;
@@ -506,12 +527,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 if (atomicExch(&stamp[v], s.stamp) != s.stamp) {
                     q0[atomicAdd(&ctl()->qlen[0], 1)] = v;
                 }
-                if (reach.mask != nullptr) {
+                if (kReach) {
                     reach.add(v, 1u << lane);
                 }
             }
         }
-        grp().sync(s, s_bar);
+        sync0();
 
         // ------------------------------------------------------------ delta-stepping over the tile
         long long t_phase = clock64();
@@ -528,11 +549,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 int32_t* q_nxt = cur ? q0 : q1;
                 const unsigned next_stamp = s.stamp + 1u;
                 const double theta = s.theta;
-                expand_queue<kUnroll, kMode != kModeApsp>(g, q_cur, qlen, lane, &ctl()->grab, expand_chunk(qlen, NGX_GWARPS), dist, pend_cur, pend_nxt,
+                expand_queue<kUnroll, kMode != kModeApsp, kReach>(g, q_cur, qlen, lane, &ctl()->grab, expand_chunk(qlen, NGX_GWARPS), dist, pend_cur, pend_nxt,
                                                           far, q_nxt, &ctl()->qlen[cur ^ 1], stamp, next_stamp, theta, expansions, lane_expansions,
                                                           reinterpret_cast<unsigned long long*>(sigma), tie,
                                                           reinterpret_cast<unsigned long long*>(delta), reach);
-                grp().sync(s, s_bar, [&](volatile TileShared& c) {
+                sync([&](volatile TileShared& c) {
                     c.qlen[cur] = 0;
                     c.cur = cur ^ 1;
                     c.stamp = next_stamp;
@@ -556,11 +577,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             // bucket step, pass 1: smallest pending far distance (min_bits is +inf here: reset at the tile's start and
             // after every bucket step)
             // (over the tile's reached vertices when it keeps a reach list: no other vertex has far marks)
-            const int64_t span = reach.mask != nullptr ? static_cast<int64_t>(s.touched_len) : n;
+            const int64_t span = kReach ? static_cast<int64_t>(s.touched_len) : n;
             unsigned long long local_min = kInfBits;
             for (int64_t vb = static_cast<int64_t>(NGX_GW) * 32; vb < span; vb += static_cast<int64_t>(NGX_GWARPS) * 32) {
                 const int64_t i = vb + lane;
-                const int64_t v = i < span ? (reach.mask != nullptr ? static_cast<int64_t>(__ldcg(&reach.list[i])) : i) : 0;
+                const int64_t v = i < span ? (kReach ? static_cast<int64_t>(__ldcg(&reach.list[i])) : i) : 0;
                 const uint32_t fm = i < span ? __ldcg(&far[v]) : 0u;
                 unsigned any = __ballot_sync(kFullMask, fm != 0u);
                 while (any != 0u) {
@@ -582,7 +603,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             if (lane == 0 && local_min != kInfBits) {
                 atomicMin(&ctl()->min_bits, local_min);
             }
-            grp().sync(s, s_bar, [&](volatile TileShared& c) {
+            sync([&](volatile TileShared& c) {
                 if (c.min_bits == kInfBits) {
                     c.done = 1;  // nothing pending: the tile's distances are final
                 } else {
@@ -599,7 +620,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             int32_t* q_cur = cur ? q1 : q0;
             for (int64_t vb = static_cast<int64_t>(NGX_GW) * 32; vb < span; vb += static_cast<int64_t>(NGX_GWARPS) * 32) {
                 const int64_t i = vb + lane;
-                const int64_t v = i < span ? (reach.mask != nullptr ? static_cast<int64_t>(__ldcg(&reach.list[i])) : i) : 0;
+                const int64_t v = i < span ? (kReach ? static_cast<int64_t>(__ldcg(&reach.list[i])) : i) : 0;
                 const uint32_t fm = i < span ? __ldcg(&far[v]) : 0u;
                 unsigned any = __ballot_sync(kFullMask, fm != 0u);
                 while (any != 0u) {
@@ -619,7 +640,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                     }
                 }
             }
-            grp().sync(s, s_bar, [&](volatile TileShared& c) {
+            sync([&](volatile TileShared& c) {
                 c.theta = c.theta_next;
                 c.min_bits = kInfBits;
             });
@@ -639,19 +660,19 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             uint32_t* const pred = reinterpret_cast<uint32_t*>(list);
             dag_count(g, rg, b.arc_src, b.m_total, n, nsrc, s_src, dist, tie, reinterpret_cast<unsigned long long*>(sigma), cnt, scnt, pred, lane,
                       NGX_GW, NGX_GWARPS, &ctl()->active_pairs);
-            grp().sync(s, s_bar);
+            sync0();
             const unsigned long long dag_arcs = group_exclusive_scan(grp(), s, s_bar, scnt, soff, nt, s_part);
             const bool use_lists = dag_arcs <= static_cast<unsigned long long>(b.succ_capacity);
             for (int64_t i = NGX_GT; i < nt; i += NGX_GTHREADS) {
                 scnt[i] = 0u;
             }
-            grp().sync(s, s_bar);
+            sync0();
             if (use_lists) {
                 dag_fill<kMode == kModeBrandes>(rg, b.arc_src, n, dist, cnt, pred, soff, scnt, succ, lane, NGX_GW, NGX_GWARPS);
-                grp().sync(s, s_bar);
+                sync0();
                 dag_sort(soff, succ, nt, NGX_GT, NGX_GTHREADS);
             }
-            grp().sync(s, s_bar, [&](volatile TileShared& c) {
+            sync([&](volatile TileShared& c) {
                 if (!use_lists) {
                     c.stamp = c.stamp + 1u;
                 }
@@ -665,12 +686,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 const long long now = clock64();
                 atomicAdd(&cnts[kCyclesCount], static_cast<unsigned long long>(now - t_phase));
                 t_phase = now;
-                if (!use_lists && grp().rank == 0) {
+                if (!use_lists && (!kMulti || grp().rank == 0)) {
                     atomicAdd(&cnts[kDagScanTiles], 1ull);
                 }
             }
             // the sources form level 0
-            if (grp().rank == 0 && warp == 0) {
+            if ((!kMulti || grp().rank == 0) && warp == 0) {
                 const int v = s_src[lane];
                 if (v >= 0) {
                     const int64_t row = static_cast<int64_t>(v) * kTile + lane;
@@ -683,7 +704,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                     }
                 }
             }
-            grp().sync(s, s_bar);
+            sync0();
           if (use_lists) {
             // --- sigma and delta over the successor lists. When every reached pair has exactly one DAG predecessor
             // (as many DAG arcs as reached non-source pairs) the DAGs are trees: every sigma is 1 and every child is
@@ -703,7 +724,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                     dag_sigma_level<kMode == kModeBrandes>(g, list + start, len, level, sigma, cnt, lvl, soff, succ, list + start + len,
                                                            &ctl()->next_len, b.sigma_inexact, lane, NGX_GW, NGX_GWARPS);
                 }
-                grp().sync(s, s_bar, [&](volatile TileShared& c) {
+                sync([&](volatile TileShared& c) {
                     c.lvl_start = start + len;
                     c.lvl_len = c.next_len;
                     c.next_len = 0;
@@ -728,7 +749,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                     dag_delta_level<kMode, false>(g, list + start, end - start, dist, sigma, delta, delta_g, soff, succ, b.grad_cpl, b.grad_eff,
                                                   reinterpret_cast<double*>(s_acc_sum), lane, warp, NGX_GW, NGX_GWARPS);
                 }
-                grp().sync(s, s_bar);
+                sync0();
             }
             // the pair buffers borrowed the epilogue's accumulators, which must start the epilogue at zero
             for (int k = tid; k < (kBlock / 32) * 32 * delta_level_unroll(kMode) * (kMode == kModeGrad ? 2 : 1); k += blockDim.x) {
@@ -736,7 +757,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             }
             __syncthreads();
             if (tid == 0) {
-                if (grp().rank == 0) {
+                if ((!kMulti || grp().rank == 0)) {
                     atomicAdd(&cnts[kDagLevels], static_cast<unsigned long long>(levels));
                     atomicAdd(&cnts[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
                 }
@@ -765,7 +786,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                                                        list + start + len, &ctl()->next_len, b.sigma_inexact);
                     }
                 }
-                grp().sync(s, s_bar, [&](volatile TileShared& c) {
+                sync([&](volatile TileShared& c) {
                     c.lvl_start = start + len;
                     c.lvl_len = c.next_len;
                     c.next_len = 0;
@@ -789,10 +810,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                     brandes_delta_vertex<kMode, 2>(g, __ldcg(&list[i]), static_cast<unsigned>(level), nsrc, lane, dist, sigma, delta, delta_g, lvl,
                                                    b.grad_cpl, b.grad_eff);
                 }
-                grp().sync(s, s_bar);
+                sync0();
             }
             if (tid == 0) {
-                if (grp().rank == 0) {
+                if ((!kMulti || grp().rank == 0)) {
                     atomicAdd(&cnts[kDagLevels], static_cast<unsigned long long>(levels));
                     atomicAdd(&cnts[kDagEntries], static_cast<unsigned long long>(__ldcg(&loff[levels])));
                 }
@@ -810,14 +831,14 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
         // APSP with a reach list visits the reached vertices only: every other vertex is unreached by every source and
         // its state was never touched; the DAG passes have written every vertex's rows, and distance rows need every
         // vertex, so those visit all of them
-        const bool by_list = reach.mask != nullptr && kMode == kModeApsp && p.out.rows == nullptr;
+        const bool by_list = kReach && kMode == kModeApsp && p.out.rows == nullptr;
         const int64_t span = by_list ? static_cast<int64_t>(s.touched_len) : n;
-        if (by_list && valid && grp().rank == 0 && warp == 0) {
+        if (by_list && valid && (!kMulti || grp().rank == 0) && warp == 0) {
             unreach = static_cast<unsigned long long>(n - span);
         }
         for (int64_t i = NGX_GW; i < span; i += NGX_GWARPS) {
             const int64_t v = by_list ? static_cast<int64_t>(__ldcg(&reach.list[i])) : i;
-            if (reach.mask != nullptr && lane == 0) {
+            if (kReach && lane == 0) {
                 reach.mask[v] = 0u;
             }
             unsigned long long* slot_ptr = &dist[v * kTile + lane];
@@ -887,7 +908,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             atomicAdd(&cnts[kHistOverflow], overflow);
         }
         __syncthreads();
-        if (p.group_size > 1) {
+        if (kMulti && p.group_size > 1) {
             // the group's CTAs add their per-source sums into the group's (exact integer adds), and the first CTA
             // finishes the tile's per-source outputs from them
             unsigned long long* const g_acc = p.group_ws + slot * p.group_stride + kCtlWords + 1 + p.group_size;  // kGroupAccWords
@@ -901,8 +922,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 atomicAdd(&g_acc[2 * kTile * kAccDigits + kTile + tid], s_arcs[tid]);
                 atomicMax(&g_acc[2 * kTile * kAccDigits + 2 * kTile + tid], s_max[tid]);
             }
-            grp().sync(s, s_bar);
-            if (grp().rank == 0) {
+            sync0();
+            if ((!kMulti || grp().rank == 0)) {
                 for (int i = tid; i < 2 * kTile * kAccDigits; i += blockDim.x) {
                     smem[i] = __ldcg(&g_acc[i]);
                     g_acc[i] = 0ull;
@@ -919,7 +940,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             }
             __syncthreads();
         }
-        if (grp().rank == 0) {
+        if ((!kMulti || grp().rank == 0)) {
             if (tid < nsrc) {
                 unsigned long long* a_sum = &s_acc_sum[tid * kAccDigits];
                 unsigned long long* a_inv = &s_acc_inv[tid * kAccDigits];

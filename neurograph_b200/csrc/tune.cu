@@ -93,15 +93,16 @@ int ngx_graph_autotune(ngx_graph* g, int task, int64_t sample_sources, ngx_tunin
         static const double kScales[] = { 0.125, 0.25, 0.5, 1.0, 2.0 };
         static const Shape kShapes[] = { { 512, 2 }, { 384, 2 }, { 256, 3 }, { 256, 4 } };
         const int tiles = static_cast<int>((k + kTile - 1) / kTile);
-        // CTAs per tile: 1, and the sizes at which the sample's tiles fill the resident CTAs or groups fill one or
-        // two SMs' CTAs
-        std::vector<int> groups = { 1, 2, 4 };
+        // CTAs per tile: 1 (the trials above), 2, 4, 8, the library's own choice for this sample (0), and the size at
+        // which the sample's tiles fill the resident CTAs
+        std::vector<int> groups = { 1, 2, 4, 8, 0 };
         const int resident = g->sm_count * 2;
         if (tiles < resident) {
             groups.push_back(std::max(1, resident / tiles));
         }
         std::sort(groups.begin(), groups.end());
         groups.erase(std::unique(groups.begin(), groups.end()), groups.end());
+        groups.erase(std::remove(groups.begin(), groups.end(), 1), groups.end());
 
         double best_rate = -1.0;
         double scale = 1.0;
@@ -134,18 +135,20 @@ int ngx_graph_autotune(ngx_graph* g, int task, int64_t sample_sources, ngx_tunin
                 shape = sh;
             }
         }
+        // groups of several CTAs per tile run with the default block shape (512 x 2)
         for (const int gs : groups) {
-            if (gs == tile_ctas) {
+            if (gs == 1) {
                 continue;
             }
             double rate = 0.0;
-            if (const int rc = trial(g, task, sources, pick_delta(mean, 0.0, scale), shape, gs, &rate); rc != NGX_OK) {
+            if (const int rc = trial(g, task, sources, pick_delta(mean, 0.0, scale), kShapes[0], gs, &rate); rc != NGX_OK) {
                 return rc;
             }
             ++trials;
             if (rate > best_rate) {
                 best_rate = rate;
                 tile_ctas = gs;
+                shape = kShapes[0];
             }
         }
         t.delta_scale = scale;

@@ -28,7 +28,7 @@ def test_autotune_apsp_keeps_results(graph):
         after = g.apsp(per_source=True, hist_bins=256, hist_max=20.0)
     assert t["delta_scale"] in (0.125, 0.25, 0.5, 1.0, 2.0), t
     assert (t["block_threads"], t["ctas_per_sm"]) in SHAPES, t
-    assert t["tile_ctas"] >= 1 and t["trials"] >= 8 and t["gteps"] > 0, t
+    assert t["tile_ctas"] >= 0 and t["trials"] >= 8 and t["gteps"] > 0, t  # 0: the library's own choice
     for k in ("sum_distances", "sum_inverse", "diameter", "unreachable", "reached_pairs", "traversed_arcs", "hist_overflow"):
         assert getattr(before, k) == getattr(after, k), k
     assert np.array_equal(before.hist, after.hist)
