@@ -574,6 +574,10 @@ def run_uneven_batch(args, ngx, torch, rank, world, barrier, max_over_ranks, sum
     peak, peak_kind = measured_peaks()
     achieved = alg / (kernel_ms / args.steps / 1e3) / 1e9
     b.close()
+    # the e2e job builds its own handle: release this one's graph and workspaces first (on the largest graphs the two
+    # would not fit on the device together)
+    g.close()
+    torch.cuda.synchronize()
     e2e = None
     if not args.no_e2e:
         pinned = [(n, torch.from_numpy(rp).pin_memory().numpy(), torch.from_numpy(c).pin_memory().numpy(),
@@ -668,6 +672,10 @@ def run_scc(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ran
     alg = 2 * (4 * arcs + 8 * c.n) + 4 * c.n
     peak, peak_kind = measured_peaks()
     achieved = alg / (elapsed / args.steps) / 1e9
+    # the e2e job builds its own handle: release this one's graph and workspaces first (on the largest graphs the two
+    # would not fit on the device together)
+    g.close()
+    torch.cuda.synchronize()
     e2e = None
     if not args.no_e2e:
         pinned = [torch.from_numpy(x).pin_memory().numpy() for x in (c.row_ptr, c.col, c.w)]
@@ -879,6 +887,10 @@ def main():
     # graph is created from the pinned host CSR (uploaded once for the job), then every step passes its host source
     # list and reads its results (betweenness / gradients, per-source summaries, histogram) back, then the graph is
     # destroyed. The graph upload is counted in the per-step H2D bytes as its share over the K steps.
+    # the e2e job builds its own handle: release this one's graph and workspaces first (on the largest graphs the two
+    # would not fit on the device together)
+    g.close()
+    torch.cuda.synchronize()
     e2e = None
     if not args.no_e2e:
         pinned = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in (("row_ptr", c.row_ptr), ("col", c.col), ("w", c.w))}

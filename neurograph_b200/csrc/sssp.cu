@@ -20,7 +20,10 @@
 namespace ngx {
 
 namespace {
-constexpr int kBatchedUnroll = 4;
+#ifndef NGX_BATCHED_UNROLL
+#define NGX_BATCHED_UNROLL 4  // (arc, source) pairs in flight per lane in the distance phase
+#endif
+constexpr int kBatchedUnroll = NGX_BATCHED_UNROLL;
 constexpr int kPlainWarpsMax = 16;
 constexpr int kBatchedDefaultBlock = 512;
 constexpr int kMaxGroupSize = 512;  // CTAs sharing one tile at most (above any SM count x resident CTAs per SM used here)
