@@ -198,7 +198,10 @@ int choose_group_size(int requested, int64_t resident, int64_t num_tiles, int64_
     }
     group = std::max<int64_t>(group, resident / std::max<int64_t>(1, num_tiles));
     if (affordable_slots < std::min(resident, num_tiles)) {
-        group = std::max<int64_t>(group, resident / std::max<int64_t>(1, affordable_slots));
+        // enough CTAs per slot that the affordable slots hold every resident CTA (rounded up: the slot count then
+        // follows from the group size, and no CTA is left without a slot)
+        const int64_t slots = std::max<int64_t>(1, affordable_slots);
+        group = std::max<int64_t>(group, (resident + slots - 1) / slots);
     }
     return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({ group, resident, static_cast<int64_t>(kMaxGroupSize) })));
 }
