@@ -38,6 +38,10 @@ namespace ngx {
 
 constexpr unsigned kFullMask = 0xFFFFFFFFu;
 
+#ifndef NGX_PEND_DEDUPE
+#define NGX_PEND_DEDUPE 0
+#endif
+
 struct TileOutputs {
     unsigned long long* acc_sum;    // per graph: kAccDigits words of the exact sum of distances, then kAccDigits for 1/d
     unsigned long long* acc_inv;    // unused by the tile kernel (acc_sum + kAccDigits of each graph)
@@ -274,8 +278,14 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
                             reach.add(x[u], bit);  // the first distance of (x, s): x joins the tile's reached vertices
                         }
                         if (nd[u] < theta) {
+#if NGX_PEND_DEDUPE
+                            // the first pending source of x for the next iteration queues x (the next pending mask
+                            // is all zero when an iteration starts)
+                            push = atomicOr(&pend_nxt[x[u]], bit) == 0u;
+#else
                             atomicOr(&pend_nxt[x[u]], bit);
                             push = atomicExch(&stamp[x[u]], next_stamp) != next_stamp;
+#endif
                         } else {
                             atomicOr(&far[x[u]], bit);
                         }
