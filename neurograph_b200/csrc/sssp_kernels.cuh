@@ -6,7 +6,8 @@
 //
 // Per tile the CTA runs delta-stepping with a common bucket bound theta for all its sources:
 //   near phase   vertices whose pending (vertex, source) pairs lie below theta are expanded; an improvement below
-//                theta is queued for the next iteration, one at or above theta is marked "far";
+//                theta marks the pair pending for the next iteration, one at or above theta marks it "far"; after
+//                the iteration the next queue is compacted from the pending masks (warp ballot + prefix);
 //   bucket step  when no near work is left, one pass over the far marks finds the smallest pending distance d_min,
 //                theta becomes (floor(d_min / delta) + 1) * delta, and the pairs below it move to the near queue.
 // Relaxation is fl(d[u] + len) compared and stored with a 64-bit atomicMin on the bit pattern, which orders
@@ -14,7 +15,7 @@
 // (PriorityQueueVariant.h:47-93: d[v] = min over arcs of fl(d[u] + |w|)), so distances are bit-identical.
 //
 // Race-freedom of the pending marks: expansions of iteration k read and clear pend[k % 2]; improvements made during
-// iteration k set pend[(k + 1) % 2] and the far marks; iterations are separated by __syncthreads(). A pair improved
+// iteration k set pend[(k + 1) % 2] and the far marks; iterations are separated by (group) barriers. A pair improved
 // while its vertex is being expanded is therefore always expanded again in the next iteration, with the new distance.
 // All distance reads go through L2 (__ldcg), where the atomics are performed.
 //
@@ -37,10 +38,6 @@
 namespace ngx {
 
 constexpr unsigned kFullMask = 0xFFFFFFFFu;
-
-#ifndef NGX_PEND_DEDUPE
-#define NGX_PEND_DEDUPE 0
-#endif
 
 struct TileOutputs {
     unsigned long long* acc_sum;    // per graph: kAccDigits words of the exact sum of distances, then kAccDigits for 1/d
@@ -106,7 +103,7 @@ struct TileShared {
     int qlen[2];
     int cur;
     int stop;
-    unsigned stamp;                 // id of the iteration about to run (queue dedup)
+    unsigned stamp;                 // id of the DAG pass about to run (dedup of its level lists)
     int done;                       // bucket step: no pending far pair is left
     double theta;
     double theta_next;              // bucket step: the bound below which pass 2 moves pairs to the near queue
@@ -178,21 +175,27 @@ struct Reach {
 // Expands vertex v for the k sources pending on it. The deg(v) x k (arc, source) pairs are spread over the 32 lanes:
 // pair p = 32 i + lane takes arc p / k and the (p % k)-th pending source, so no lane idles when few sources are
 // pending, and when all 32 are, every iteration reads one whole distance row d[x][0..31] (256 contiguous bytes).
-// kTrack (betweenness / adjoint): each improvement of d[x][s] to nb offers the key (top 32 bits of nb, arc index) to
-// pred_key[x][s] with an atomic minimum, so the key of the smallest distance wins whatever the order of the stores;
-// a relaxation that ties with d[x][s] sets bit s of tie[x]. Every DAG arc is relaxed with final distances, so a
-// (x, s) whose tie bit stayed clear has exactly one DAG predecessor: the arc in its key (the DAG count pass checks it).
-// For that, no (v, s) may be expanded twice with one distance (the repeat would look like a tie): an expansion reads
-// the newest distance, and the improvement that produced it has queued another expansion. last[v][s] keeps the
-// distance of the latest expansion, and sources whose distance has not changed since are dropped from the next.
+// An improvement below theta sets the pair's bit in pend_nxt (the next iteration's queue is compacted from those
+// masks after the iteration), one at or above theta its far mark. The kUnroll relaxations of a lane are issued back
+// to back and waited for together.
+// APSP mode: the atomic minimum is not waited for. An improvement is judged against the distance read before it, so
+// a relaxation that lost a race to a smaller value may still set a pending bit or a far mark: the pair is then
+// expanded once more with its (smaller) current distance, or its superseded far mark is cleared or moved by the next
+// expansion or bucket step, which changes the work and never the fixed point.
+// kTrack (betweenness / adjoint): the atomic minimum returns the old value. Each improvement of d[x][s] to nb offers
+// the key (top 32 bits of nb, arc index) to pred_key[x][s] with an atomic minimum, so the key of the smallest
+// distance wins whatever the order of the stores; a relaxation that ties with d[x][s] sets bit s of tie[x]. Every
+// DAG arc is relaxed with final distances, so a (x, s) whose tie bit stayed clear has exactly one DAG predecessor: the
+// arc in its key (the DAG count pass checks it). For that, no (v, s) may be expanded twice with one distance (the
+// repeat would look like a tie): last[v][s] keeps the distance of the latest expansion, and sources whose distance has
+// not changed since are dropped from the next.
 // The caller has taken v's pending mask (amask, non-zero), cleared it and v's superseded far marks, and read its row
 // offsets (beg, deg): see expand_queue.
 template <int kUnroll, bool kTrack, bool kReach>
 __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32_t amask, int64_t beg, int deg, int lane,
-                                               unsigned long long* __restrict__ dist, uint32_t* pend_nxt, uint32_t* far, int32_t* q_nxt,
-                                               int* qlen_nxt, uint32_t* stamp, unsigned next_stamp, double theta, unsigned long long& expansions,
-                                               unsigned long long& lane_expansions, unsigned long long* pred_key, uint32_t* tie,
-                                               unsigned long long* last, const Reach& reach) {
+                                               unsigned long long* __restrict__ dist, uint32_t* pend_nxt, uint32_t* far, double theta,
+                                               unsigned long long& expansions, unsigned long long& lane_expansions, unsigned long long* pred_key,
+                                               uint32_t* tie, unsigned long long* last, const Reach& reach) {
     const uint32_t amask0 = amask;
     int k = __popc(amask);
     // lane r < k holds the r-th pending source and its distance to v
@@ -223,6 +226,10 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
     lane_expansions += static_cast<unsigned long long>(k);
     const double rank_dv = __longlong_as_double(static_cast<long long>(rank_bits));
     const Arc* arcs = g.arcs + beg;
+    // v's arc records (16 B each) into L1 ahead of the pair loop, one 128-byte line per lane
+    if (lane * 8 < deg) {
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(arcs + lane * 8));
+    }
     // position of this lane's first pair, and the per-iteration advance of 32 pairs
     int a = lane / k;
     int r = lane - a * k;
@@ -258,53 +265,45 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
                 a += 1;
             }
         }
+        // the atomic minima (cur[u] becomes the old value where it is waited for)
+        bool tried[kUnroll];
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
-            bool push = false;
-            if (valid[u]) {
-                const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd[u]));
-                if (nb < cur[u]) {
-                    const unsigned long long old = atomicMin(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]], nb);
-                    if constexpr (kTrack) {
-                        if (nb < old) {
-                            atomicMin(&pred_key[static_cast<int64_t>(x[u]) * kTile + src[u]], ((nb >> 32) << 32) | eidx[u]);
-                        } else if (nb == old) {
-                            atomicOr(&tie[x[u]], 1u << src[u]);
-                        }
-                    }
-                    if (nb < old) {
-                        const uint32_t bit = 1u << src[u];
-                        if (kReach && old == kInfBits) {
-                            reach.add(x[u], bit);  // the first distance of (x, s): x joins the tile's reached vertices
-                        }
-                        if (nd[u] < theta) {
-#if NGX_PEND_DEDUPE
-                            // the first pending source of x for the next iteration queues x (the next pending mask
-                            // is all zero when an iteration starts)
-                            push = atomicOr(&pend_nxt[x[u]], bit) == 0u;
-#else
-                            atomicOr(&pend_nxt[x[u]], bit);
-                            push = atomicExch(&stamp[x[u]], next_stamp) != next_stamp;
-#endif
-                        } else {
-                            atomicOr(&far[x[u]], bit);
-                        }
-                    }
-                } else if (kTrack && nb == cur[u]) {
-                    atomicOr(&tie[x[u]], 1u << src[u]);
+            const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd[u]));
+            tried[u] = valid[u] && nb < cur[u];
+            if (tried[u]) {
+                if constexpr (kTrack) {
+                    cur[u] = atomicMin(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]], nb);
+                } else {
+                    atomicMin(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]], nb);
                 }
             }
-            const unsigned pmask = __ballot_sync(kFullMask, push);
-            if (pmask != 0u) {
-                int base = 0;
-                const int leader = __ffs(pmask) - 1;
-                if (lane == leader) {
-                    base = atomicAdd(qlen_nxt, __popc(pmask));
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd[u]));
+            if (tried[u]) {
+                const unsigned long long old = cur[u];
+                if constexpr (kTrack) {
+                    if (nb < old) {
+                        atomicMin(&pred_key[static_cast<int64_t>(x[u]) * kTile + src[u]], ((nb >> 32) << 32) | eidx[u]);
+                    } else if (nb == old) {
+                        atomicOr(&tie[x[u]], 1u << src[u]);
+                    }
                 }
-                base = __shfl_sync(kFullMask, base, leader);
-                if (push) {
-                    q_nxt[base + __popc(pmask & lanemask_lt())] = x[u];
+                if (nb < old) {
+                    const uint32_t bit = 1u << src[u];
+                    if (kReach && old == kInfBits) {
+                        reach.add(x[u], bit);  // the first distance of (x, s): x joins the tile's reached vertices
+                    }
+                    if (nd[u] < theta) {
+                        atomicOr(&pend_nxt[x[u]], bit);
+                    } else {
+                        atomicOr(&far[x[u]], bit);
+                    }
                 }
+            } else if (kTrack && valid[u] && nb == cur[u]) {
+                atomicOr(&tie[x[u]], 1u << src[u]);
             }
         }
     }
@@ -316,9 +315,8 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
 template <int kUnroll, bool kTrack, bool kReach>
 __device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* q_cur, int qlen, int lane, int* grab, int chunk,
                                              unsigned long long* __restrict__ dist, uint32_t* pend_cur, uint32_t* pend_nxt, uint32_t* far,
-                                             int32_t* q_nxt, int* qlen_nxt, uint32_t* stamp, unsigned next_stamp, double theta,
-                                             unsigned long long& expansions, unsigned long long& lane_expansions, unsigned long long* pred_key,
-                                             uint32_t* tie, unsigned long long* last, const Reach& reach) {
+                                             double theta, unsigned long long& expansions, unsigned long long& lane_expansions,
+                                             unsigned long long* pred_key, uint32_t* tie, unsigned long long* last, const Reach& reach) {
     for (;;) {
         int base = 0;
         if (lane == 0) {
@@ -355,8 +353,32 @@ __device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* 
             const int v = __shfl_sync(kFullMask, vj, j);
             const int64_t beg = __shfl_sync(kFullMask, bj, j);
             const int deg = __shfl_sync(kFullMask, dj, j);
-            batched_expand<kUnroll, kTrack, kReach>(g, v, amask, beg, deg, lane, dist, pend_nxt, far, q_nxt, qlen_nxt, stamp, next_stamp, theta,
-                                            expansions, lane_expansions, pred_key, tie, last, reach);
+            batched_expand<kUnroll, kTrack, kReach>(g, v, amask, beg, deg, lane, dist, pend_nxt, far, theta, expansions, lane_expansions,
+                                                    pred_key, tie, last, reach);
+        }
+    }
+}
+
+// The next iteration's queue: the group's warps scan the pending masks `pend` (over the tile's reached vertices when
+// it keeps a reach list: no other vertex can be pending) and append every vertex with a pending source to `q`, 32 at
+// a time with one ballot and one atomic per warp.
+template <bool kReach>
+__device__ __forceinline__ void compact_queue(const uint32_t* pend, int32_t* q, int* qlen, int64_t span, const Reach& reach, int lane, int gw,
+                                              int gwarps) {
+    for (int64_t vb = static_cast<int64_t>(gw) * 32; vb < span; vb += static_cast<int64_t>(gwarps) * 32) {
+        const int64_t i = vb + lane;
+        const int64_t v = i < span ? (kReach ? static_cast<int64_t>(__ldcg(&reach.list[i])) : i) : 0;
+        const uint32_t m = i < span ? __ldcg(&pend[v]) : 0u;
+        const unsigned bal = __ballot_sync(kFullMask, m != 0u);
+        if (bal != 0u) {
+            int qb = 0;
+            if (lane == 0) {
+                qb = atomicAdd(qlen, __popc(bal));
+            }
+            qb = __shfl_sync(kFullMask, qb, 0);
+            if (m != 0u) {
+                q[qb + __popc(bal & lanemask_lt())] = static_cast<int32_t>(v);
+            }
         }
     }
 }
@@ -482,7 +504,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     bool first_tile = true;
 
     for (;;) {
-        // ---- the next work item, taken for the whole group; the slot's queue stamp counts on across tiles
+        // ---- the next work item, taken for the whole group; the slot's stamp counts on across tiles
         sync([&](volatile TileShared& c) {
             if (first_tile) {
                 c.stamp = 1u;
@@ -533,8 +555,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
             const int v = s_src[lane];
             if (v >= 0) {
                 dist[static_cast<int64_t>(v) * kTile + lane] = 0ull;
-                atomicOr(&pend0[v], 1u << lane);
-                if (atomicExch(&stamp[v], s.stamp) != s.stamp) {
+                // pend0 is all zero between tiles: the first lane of a source repeated in the tile queues it
+                if (atomicOr(&pend0[v], 1u << lane) == 0u) {
                     q0[atomicAdd(&ctl()->qlen[0], 1)] = v;
                 }
                 if (kReach) {
@@ -557,16 +579,12 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 uint32_t* pend_nxt = cur ? pend0 : pend1;
                 const int32_t* q_cur = cur ? q1 : q0;
                 int32_t* q_nxt = cur ? q0 : q1;
-                const unsigned next_stamp = s.stamp + 1u;
                 const double theta = s.theta;
                 expand_queue<kUnroll, kMode != kModeApsp, kReach>(g, q_cur, qlen, lane, &ctl()->grab, expand_chunk(qlen, NGX_GWARPS), dist, pend_cur, pend_nxt,
-                                                          far, q_nxt, &ctl()->qlen[cur ^ 1], stamp, next_stamp, theta, expansions, lane_expansions,
-                                                          reinterpret_cast<unsigned long long*>(sigma), tie,
+                                                          far, theta, expansions, lane_expansions, reinterpret_cast<unsigned long long*>(sigma), tie,
                                                           reinterpret_cast<unsigned long long*>(delta), reach);
                 sync([&](volatile TileShared& c) {
                     c.qlen[cur] = 0;
-                    c.cur = cur ^ 1;
-                    c.stamp = next_stamp;
                     c.grab = 0;
                     c.iterations = c.iterations + 1;
                     if (c.iterations > p.max_iterations) {
@@ -580,6 +598,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 if (s.stop != 0) {
                     break;
                 }
+                // the next iteration's queue, from its pending masks (reach list: touched_len is final here)
+                compact_queue<kReach>(pend_nxt, q_nxt, &ctl()->qlen[cur ^ 1], kReach ? static_cast<int64_t>(s.touched_len) : n, reach, lane,
+                                      NGX_GW, NGX_GWARPS);
+                sync([&](volatile TileShared& c) { c.cur = cur ^ 1; });
             }
             if (s.stop != 0) {
                 break;
