@@ -573,10 +573,8 @@ def run_uneven_batch(args, ngx, torch, rank, world, barrier, max_over_ranks, sum
     alg = (per_arc * arcs + per_vertex * reached * args.steps) / args.steps
     peak, peak_kind = measured_peaks()
     achieved = alg / (kernel_ms / args.steps / 1e3) / 1e9
+    # the e2e job builds its own handle: release this one's graphs and workspaces first
     b.close()
-    # the e2e job builds its own handle: release this one's graph and workspaces first (on the largest graphs the two
-    # would not fit on the device together)
-    g.close()
     torch.cuda.synchronize()
     e2e = None
     if not args.no_e2e:
@@ -666,7 +664,6 @@ def run_scc(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ran
     arcs = int(c.m)
     value = sum_over_ranks(float(arcs * args.steps)) / elapsed / 1e9
     assert out["number_components"] == first["number_components"]
-    g.close()
     # compulsory bytes of one call: both CSRs read once (4 B target per arc and direction, 8 B row offset per vertex
     # and direction) and the component array written once
     alg = 2 * (4 * arcs + 8 * c.n) + 4 * c.n
