@@ -280,22 +280,17 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
     const size_t group_bytes = static_cast<size_t>(group_stride_words(group)) * 8;
     const size_t slot_bytes = data_bytes + group_bytes;
     int64_t slots = std::min<int64_t>(num_tiles, resident / group);
-    const size_t order_max = (static_cast<size_t>(resident + 1) * 4 + 255) & ~static_cast<size_t>(255);  // the CTA order, below
-    slots = std::min<int64_t>(slots, static_cast<int64_t>((budget > order_max ? budget - order_max : 0) / slot_bytes));
+    slots = std::min<int64_t>(slots, static_cast<int64_t>(budget / slot_bytes));
     if (slots <= 0) {
         return fail(NGX_OUT_OF_MEMORY, "not enough device memory for one workspace slot (" + std::to_string(slot_bytes) + " bytes)");
     }
-    // the launch's CTA order (arrival count + one word per CTA), 256-byte rounded
-    const size_t order_bytes = (static_cast<size_t>(slots * group + 1) * 4 + 255) & ~static_cast<size_t>(255);
-    if (const int rc = ensure_workspace(g, static_cast<size_t>(slots) * slot_bytes + order_bytes); rc != NGX_OK) {
+    if (const int rc = ensure_workspace(g, static_cast<size_t>(slots) * slot_bytes); rc != NGX_OK) {
         return rc;
     }
     char* ws = static_cast<char*>(g->d_workspace);
-    // group storage first (256-byte aligned slots), the CTA order, then the slot arrays
+    // group storage first (256-byte aligned slots), then the slot arrays
     unsigned long long* group_ws = reinterpret_cast<unsigned long long*>(ws);
     ws += static_cast<size_t>(slots) * group_bytes;
-    unsigned* cta_order = reinterpret_cast<unsigned*>(ws);
-    ws += order_bytes;
     SsspParams p{};
     p.g = g->csr(opts->metric);
     p.g.n = n;
@@ -322,7 +317,6 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
     p.group_size = group;
     p.group_stride = group_stride_words(group);
     p.group_ws = group_ws;
-    p.cta_order = cta_order;
     if (track) {
         ws = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(ws) + 255) & ~uintptr_t(255));
         p.ws_reach = reinterpret_cast<uint32_t*>(ws);
@@ -394,7 +388,7 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
     cudaError_t err = cudaSuccess;
     if (batched) {
         void* args[] = { &p, &bp };
-        err = cudaMemsetAsync(group_ws, 0, static_cast<size_t>(slots) * group_bytes + order_bytes, g->stream);
+        err = cudaMemsetAsync(group_ws, 0, static_cast<size_t>(slots) * group_bytes, g->stream);
         if (err == cudaSuccess) {
             err = launch_tile_kernel(kernel, slots * group, block, smem, g->stream, group, args);
         }

@@ -82,7 +82,6 @@ struct SsspParams {
     int group_size;
     int64_t group_stride;          // words of group storage per slot (group_stride_words)
     unsigned long long* group_ws;  // slots * group_stride words, zero at launch
-    unsigned* cta_order;           // 1 + grid words, zero at launch: arrivals, then each CTA's SM
     TileOutputs out;
 };
 
@@ -145,41 +144,11 @@ inline int64_t group_stride_words(int group_size) {
 // This CTA's view of its tile group (see SsspParams::group_*). A group of one CTA keeps the control block in the CTA's
 // shared memory (`local`), where its counters are shared-memory atomics; larger groups keep it in global memory.
 template <typename Params>
-__device__ __forceinline__ Group<TileShared> tile_group(const Params& p, TileShared* local, int vblock) {
-    unsigned long long* const gws = p.group_ws + (vblock / p.group_size) * p.group_stride;
+__device__ __forceinline__ Group<TileShared> tile_group(const Params& p, TileShared* local) {
+    unsigned long long* const gws = p.group_ws + (blockIdx.x / p.group_size) * p.group_stride;
     TileShared* const ctl = p.group_size == 1 ? local : reinterpret_cast<TileShared*>(gws);
     return Group<TileShared>{ ctl, reinterpret_cast<GroupBarrier*>(gws + kCtlWords), gws + kCtlWords + 1, p.group_size,
-                              static_cast<int>(vblock % p.group_size), p.error };
-}
-
-// The CTA's place in the launch ordered by SM: CTAs on nearby SMs form the groups. Every CTA of the (cooperative)
-// launch publishes its SM and waits, bounded in time, until all have; its place is the number of CTAs before it in
-// (SM key, blockIdx) order. On a timeout the run's error flag is set and blockIdx.x is returned.
-__device__ __forceinline__ int cta_place_by_sm(unsigned* order, int* error) {
-    unsigned smid;
-    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
-#if NGX_DIE_GROUPS == 2
-    const unsigned key = ((smid & 1u) << 16) | smid;
-#else
-    const unsigned key = smid;
-#endif
-    __stcg(&order[1 + blockIdx.x], key);
-    __threadfence();
-    atomicAdd(&order[0], 1u);
-    const unsigned long long t0 = global_ns();
-    while (ld_acquire_gpu(&order[0]) < gridDim.x) {
-        if (global_ns() - t0 > kGroupWaitNs) {
-            atomicCAS(error, kDevOk, kDevTimeout);
-            return static_cast<int>(blockIdx.x);
-        }
-        __nanosleep(256);
-    }
-    int place = 0;
-    for (unsigned j = 0; j < gridDim.x; ++j) {
-        const unsigned kj = __ldcg(&order[1 + j]);
-        place += (kj < key || (kj == key && j < blockIdx.x)) ? 1 : 0;
-    }
-    return place;
+                              static_cast<int>(blockIdx.x % p.group_size), p.error };
 }
 
 // Queue entries a warp takes at a time: all 32 when the near queue is long, fewer towards the end of a frontier so
@@ -436,20 +405,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     const int64_t n_slot = p.g.n;  // every slot holds the largest graph of the batch
     // The CTAs blockIdx.x / group_size share workspace slot `slot` and work on its tiles together. The group's
     // pointers and indices are recomputed from the launch parameters where they are used (fewer live registers).
-    __shared__ int s_vblock;
-    if (tid == 0) {
-#if NGX_DIE_GROUPS
-        s_vblock = kMulti ? cta_place_by_sm(p.cta_order, p.error) : static_cast<int>(blockIdx.x);
-#else
-        s_vblock = static_cast<int>(blockIdx.x);
-#endif
-    }
-    __syncthreads();
-#define NGX_VBLOCK (kMulti ? s_vblock : static_cast<int>(blockIdx.x))
-    const int64_t slot = NGX_VBLOCK / p.group_size;
-    const auto grp = [&]() { return tile_group(p, &s, NGX_VBLOCK); };
+    const int64_t slot = blockIdx.x / p.group_size;
+    const auto grp = [&]() { return tile_group(p, &s); };
     const auto ctl = [&]() {
-        return kMulti ? reinterpret_cast<TileShared*>(p.group_ws + (NGX_VBLOCK / p.group_size) * p.group_stride) : &s;
+        return kMulti ? reinterpret_cast<TileShared*>(p.group_ws + (blockIdx.x / p.group_size) * p.group_stride) : &s;
     };
     // a group barrier whose last arrival applies `update` to the control block (a block barrier without kMulti)
     const auto sync = [&](auto&& update) {
@@ -465,9 +424,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
     };
     const auto sync0 = [&]() { sync([](volatile TileShared&) {}); };
     // this thread's (warp's) index among the group's threads (warps), and their counts
-#define NGX_GT (kMulti ? static_cast<int64_t>(NGX_VBLOCK % p.group_size) * blockDim.x + threadIdx.x : static_cast<int64_t>(threadIdx.x))
+#define NGX_GT (kMulti ? static_cast<int64_t>(blockIdx.x % p.group_size) * blockDim.x + threadIdx.x : static_cast<int64_t>(threadIdx.x))
 #define NGX_GTHREADS (kMulti ? static_cast<int64_t>(p.group_size) * blockDim.x : static_cast<int64_t>(blockDim.x))
-#define NGX_GW (kMulti ? static_cast<int>(NGX_VBLOCK % p.group_size) * static_cast<int>(blockDim.x >> 5) + static_cast<int>(threadIdx.x >> 5) \
+#define NGX_GW (kMulti ? static_cast<int>(blockIdx.x % p.group_size) * static_cast<int>(blockDim.x >> 5) + static_cast<int>(threadIdx.x >> 5) \
                        : static_cast<int>(threadIdx.x >> 5))
 #define NGX_GWARPS (kMulti ? p.group_size * static_cast<int>(blockDim.x >> 5) : static_cast<int>(blockDim.x >> 5))
     unsigned long long expansions = 0, lane_expansions = 0;
@@ -1069,7 +1028,6 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
 #undef NGX_GTHREADS
 #undef NGX_GW
 #undef NGX_GWARPS
-#undef NGX_VBLOCK
 }
 
 // ------------------------------------------------------------------------------------------ plain form
