@@ -207,6 +207,11 @@ class ClockSampler:
                 "power_w_max": max(power) if power else None}
 
 
+def peak_label(kind):
+    """How the roofline's peak was obtained: the measured copy bandwidth, or the fallback figure."""
+    return "measured hbm_gbs (MEASURED_PEAKS.json)" if kind == "measured" else "fallback 6.65 TB/s (no MEASURED_PEAKS.json)"
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -606,7 +611,7 @@ def run_uneven_batch(args, ngx, torch, rank, world, barrier, max_over_ranks, sum
         "gpu_launches": args.steps * 2,
         "clocks": clock_info,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)", "traffic": None,
+                     "peak_kind": peak_label(peak_kind), "traffic": None,
                      "algorithmic_bytes_per_launch": alg, "kernel": "tile_kernel<Brandes> (ngx_batch_run)"},
         "e2e": e2e,
         "cpu_baseline": None,
@@ -721,7 +726,7 @@ def run_scc(args, ngx, torch, rank, world, barrier, max_over_ranks, sum_over_ran
         "gpu_launches": None,
         "clocks": clock_info,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)", "traffic": None,
+                     "peak_kind": peak_label(peak_kind), "traffic": None,
                      "algorithmic_bytes_per_launch": alg,
                      "kernel": "the whole ngx_scc call (trim, colour, peel passes with host-read change flags); bytes: "
                                "both CSRs read once + components written once"},
@@ -865,19 +870,22 @@ def main():
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
     traffic_per_arc = profiled_traffic_per_arc(args.mode)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_kind": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                "peak_kind": peak_label(peak_kind),
                 "traffic": None if traffic_per_arc is None else traffic_per_arc * arcs / launches,
                 "algorithmic_bytes_per_launch": alg_bytes / launches,
                 "kernel": {"brandes": "tile_kernel<Brandes> (ngx_brandes)", "grad": "tile_kernel<Grad> (ngx_apsp_grad)",
                            "apsp": "tile_kernel<Apsp> (ngx_apsp)", "plain": "sssp_plain_kernel (ngx_apsp, plain form)"}[args.mode]}
 
-    # forms on the same graph: plain per-source GPU APSP vs batched APSP (one wave of sources each)
+    # forms on the same graph: the plain per-source GPU form (one source per CTA) against the batched one, for APSP
+    # and for APSP + histogram + Brandes (the same outputs as the timed steps)
     forms = {}
     if rank == 0 and not args.no_forms:
         sample = batches[0][: SLOTS_PER_WAVE * 4]
         rp = g.apsp(sources=sample, mode="plain", delta=0.1)
+        rpb = g.brandes(sources=sample, mode="plain", delta=0.1, hist_bins=HIST_BINS, hist_max=hist_max)[1]
         rb = g.apsp(sources=batches[0], delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max)
-        forms = {"plain_apsp_gteps": rp.gteps, "batched_apsp_gteps": rb.gteps, "batched_apsp_brandes_gteps": arcs / (kernel_ms / 1e3) / 1e9,
+        forms = {"plain_apsp_gteps": rp.gteps, "batched_apsp_gteps": rb.gteps, "plain_apsp_brandes_gteps": rpb.gteps,
+                 "batched_apsp_brandes_gteps": arcs / (kernel_ms / 1e3) / 1e9,
                  "plain_sources": int(len(sample)), "batched_sources": int(len(batches[0]))}
 
     # e2e through the C ABI from host buffers: the job of K steps as a user runs it, all inside the timed region: the

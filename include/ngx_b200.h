@@ -232,6 +232,9 @@ NGX_API int ngx_sssp_rows(ngx_graph* graph, const ngx_apsp_opts* opts, double* r
 /*
  * Brandes betweenness (regular metric) of the requested sources: bc (n entries) is overwritten with the sum over
  * sources of the pair dependencies; result (optional) receives the APSP summaries of the same run.
+ * opts->mode NGX_MODE_PLAIN runs one source per CTA (the per-source form, for comparison); its dependency sums run
+ * in another order than the batched form's, so the two agree to rounding, not bit for bit. The gradient entry
+ * points below have the batched form only.
  */
 NGX_API int ngx_brandes(ngx_graph* graph, const ngx_apsp_opts* opts, double* bc, ngx_apsp_result* result);
 

@@ -388,10 +388,12 @@ class Graph:
         return rows
 
     def brandes(self, sources=None, delta=0.0, hist_bins=0, hist_max=0.0, per_source=False, block_threads=0,
-                ctas_per_sm=0, max_iterations=0, fixed=False, exact=False, tile_ctas=0):
+                ctas_per_sm=0, max_iterations=0, fixed=False, exact=False, tile_ctas=0, mode="batched"):
         """Betweenness (sum of pair dependencies over the sources) and the run's APSP result. fixed=True returns the
-        unconverted sums instead (ngx_brandes_fixed): an (n, 2) uint64 array of 128-bit fixed-point words."""
-        opts, srcs, k = self._opts(sources, "regular", "batched", delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations,
+        unconverted sums instead (ngx_brandes_fixed): an (n, 2) uint64 array of 128-bit fixed-point words.
+        mode="plain" runs one source per CTA (the per-source baseline form); its dependencies are summed in another
+        order than the batched form's, so its betweenness agrees with the batched one to rounding, not bit for bit."""
+        opts, srcs, k = self._opts(sources, "regular", mode, delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations,
                                    tile_ctas)
         r, hist, per = self._result_struct(hist_bins, per_source, k, exact)
         if fixed:

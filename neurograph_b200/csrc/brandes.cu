@@ -61,7 +61,9 @@ int dag_run(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, ngx_apsp_res
     }
     NGX_CUDA_TRY(cudaSetDevice(g->device));
     ngx_apsp_opts o = *opts;
-    o.mode = NGX_MODE_BATCHED;
+    if (tile_mode != kModeBrandes || o.mode != NGX_MODE_PLAIN) {
+        o.mode = NGX_MODE_BATCHED;  // the adjoint has the batched form only
+    }
     const size_t n = static_cast<size_t>(g->n);
     const size_t m = static_cast<size_t>(g->m_user);
     DagOutputs extra;

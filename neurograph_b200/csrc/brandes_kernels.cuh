@@ -58,6 +58,11 @@ inline size_t brandes_slot_bytes(int64_t n, bool adjoint) {
            nt * 4 + (nt + 1) * 4 + static_cast<size_t>(n) * 4 + nt * kSuccPerPair * 4 + 1024;
 }
 
+// Per-CTA bytes of the plain (one source per CTA) Brandes form: sigma, delta, counts, level list, level offsets.
+inline size_t plain_brandes_slot_bytes(int64_t n) {
+    return static_cast<size_t>(n) * (8 + 8 + 4 + 4) + static_cast<size_t>(n + 2) * 4 + 256;
+}
+
 __device__ __forceinline__ bool on_dag(unsigned long long du_bits, double len, unsigned long long dv_bits) {
     return static_cast<unsigned long long>(__double_as_longlong(__dadd_rn(__longlong_as_double(static_cast<long long>(du_bits)), len))) == dv_bits;
 }

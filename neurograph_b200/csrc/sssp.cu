@@ -224,7 +224,8 @@ cudaError_t launch_tile_kernel(const void* kernel, int64_t grid, int block, size
 
 int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const TileJob& job, int64_t hist_bins, double hist_max, RunOutputs& o,
                  DagOutputs* extra, float* kernel_ms, bool synchronous) {
-    const bool batched = opts->mode == NGX_MODE_BATCHED || tile_mode != kModeApsp;
+    // the plain (one source per CTA) form runs APSP and Brandes; the adjoint is batched only
+    const bool batched = opts->mode == NGX_MODE_BATCHED || tile_mode == kModeGrad;
     const int width = batched ? kTile : 1;
     const int64_t num_tiles = batched ? job.num_items : job.num_sources;
     const int block = opts->block_threads > 0 ? opts->block_threads : (batched ? kBatchedDefaultBlock : 512);
@@ -237,7 +238,8 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
         return NGX_OK;
     }
 
-    const void* kernel = reinterpret_cast<const void*>(&sssp_plain_kernel);
+    const void* kernel = tile_mode == kModeBrandes ? reinterpret_cast<const void*>(&sssp_plain_kernel<true>)
+                                                   : reinterpret_cast<const void*>(&sssp_plain_kernel<false>);
     // reach lists (several strongly connected components) and tile groups run with the default block shape only
     const bool default_shape = block == kBatchedDefaultBlock && (opts->ctas_per_sm == 0 || opts->ctas_per_sm >= 2);
     if (batched && opts->tile_ctas > 1 && !default_shape) {
@@ -267,8 +269,8 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
     const int64_t n = job.n_max;
     const int64_t resident = static_cast<int64_t>(g->sm_count) * per_sm;
     const size_t reach_bytes = track ? static_cast<size_t>(n) * 8 + 512 : 0;  // reach mask + reached list
-    const size_t data_bytes =
-        sssp_slot_bytes(n, width) + (tile_mode != kModeApsp ? brandes_slot_bytes(n, tile_mode == kModeGrad) : 0) + reach_bytes;
+    const size_t dag_bytes = tile_mode == kModeApsp ? 0 : batched ? brandes_slot_bytes(n, tile_mode == kModeGrad) : plain_brandes_slot_bytes(n);
+    const size_t data_bytes = sssp_slot_bytes(n, width) + dag_bytes + reach_bytes;
     const size_t budget = workspace_budget(g);
     // the group size decides the group storage per slot, which the slot count must leave room for
     const int64_t affordable = static_cast<int64_t>(budget / (data_bytes + static_cast<size_t>(group_stride_words(kMaxGroupSize)) * 8));
@@ -325,7 +327,23 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
         ws += static_cast<size_t>(slots) * n * 4;
     }
     BrandesParams bp{};
-    if (tile_mode != kModeApsp) {
+    if (tile_mode == kModeBrandes && !batched) {
+        // plain form: sigma, delta, predecessor counts and the level list per vertex, the level offsets
+        ws = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(ws) + 255) & ~uintptr_t(255));
+        bp.rg = g->reverse_csr();
+        bp.ws_sigma = reinterpret_cast<double*>(ws);
+        ws += static_cast<size_t>(slots) * n * 8;
+        bp.ws_delta = reinterpret_cast<double*>(ws);
+        ws += static_cast<size_t>(slots) * n * 8;
+        bp.ws_cnt = reinterpret_cast<uint32_t*>(ws);
+        ws += static_cast<size_t>(slots) * n * 4;
+        bp.ws_list = reinterpret_cast<int32_t*>(ws);
+        ws += static_cast<size_t>(slots) * n * 4;
+        bp.ws_loff = reinterpret_cast<int32_t*>(ws);
+        if (extra != nullptr) {
+            bp.bc = extra->bc;
+        }
+    } else if (tile_mode != kModeApsp) {
         const size_t nt = static_cast<size_t>(n) * kTile;
         ws = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(ws) + 255) & ~uintptr_t(255));
         bp.rg = g->reverse_csr();
@@ -393,7 +411,11 @@ int launch_tiles(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const T
             err = launch_tile_kernel(kernel, slots * group, block, smem, g->stream, group, args);
         }
     } else {
-        sssp_plain_kernel<<<static_cast<unsigned>(slots), block, smem, g->stream>>>(p);
+        if (tile_mode == kModeBrandes) {
+            sssp_plain_kernel<true><<<static_cast<unsigned>(slots), block, smem, g->stream>>>(p, bp);
+        } else {
+            sssp_plain_kernel<false><<<static_cast<unsigned>(slots), block, smem, g->stream>>>(p, bp);
+        }
         err = cudaGetLastError();
     }
     if (!synchronous) {

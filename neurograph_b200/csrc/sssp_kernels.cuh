@@ -1046,7 +1046,140 @@ __device__ __forceinline__ void plain_push(bool push, int x, int lane, int32_t* 
     }
 }
 
-__global__ void __launch_bounds__(512, 2) sssp_plain_kernel(const SsspParams p) {
+// Brandes for the one source of a plain tile (BrandesVariant.h:79-159), by one CTA with warp-per-vertex passes over
+// the final distances: DAG predecessor counts from each vertex's in-arcs; Kahn levels over the out-arcs (the last
+// predecessor of x to be done appends x to the next level); sigma of each new level pulled over its in-arcs (integer
+// sums, exact in FP64 below 2^53); dependencies pulled over the out-arcs, level by level from the last,
+// delta[u] = sum over DAG arcs u -> x of sigma[u] * ((1 + delta[x]) / sigma[x]), each lane's terms in arc order and
+// the lanes combined by a fixed shuffle tree; every vertex but the source adds delta[u] to its 128-bit fixed-point
+// betweenness. The arrays are per CTA: sigma, delta, cnt, list (n each) and loff (n + 2).
+__device__ __forceinline__ double warp_sum_fixed_order(double x) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        x += __shfl_xor_sync(kFullMask, x, off);
+    }
+    return x;
+}
+
+__device__ void plain_brandes(const DeviceCsr& g, const DeviceCsr& rg, int64_t n, int src, const unsigned long long* dist, double* sigma,
+                              double* delta, uint32_t* cnt, int32_t* list, int32_t* loff, unsigned long long* bc, TileShared& s, int tid,
+                              int lane, int warp, int nwarps) {
+    // DAG predecessors of every reached vertex
+    for (int64_t v = warp; v < n; v += nwarps) {
+        const unsigned long long dv = __ldcg(&dist[v]);
+        unsigned c = 0;
+        if (dv != kInfBits && v != src) {
+            const int64_t beg = __ldg(&rg.row_ptr[v]);
+            const int64_t end = __ldg(&rg.row_ptr[v + 1]);
+            for (int64_t e = beg + lane; e < end; e += 32) {
+                const Arc a = ldg_arc(&rg.arcs[e]);
+                c += on_dag(__ldcg(&dist[a.col]), a.len, dv) ? 1u : 0u;
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            c += __shfl_xor_sync(kFullMask, c, off);
+        }
+        if (lane == 0) {
+            cnt[v] = c;
+            sigma[v] = v == src ? 1.0 : 0.0;
+            delta[v] = 0.0;
+        }
+    }
+    if (tid == 0) {
+        list[0] = src;
+        loff[0] = 0;
+        loff[1] = 1;
+        s.level = 0u;
+        s.next_len = 0;
+    }
+    __syncthreads();
+    // Kahn levels, and sigma of each new level
+    for (;;) {
+        const unsigned level = s.level;
+        const int start = loff[level];
+        const int len = loff[level + 1] - start;
+        if (len == 0) {
+            break;
+        }
+        for (int i = warp; i < len; i += nwarps) {
+            const int u = list[start + i];
+            const unsigned long long du = __ldcg(&dist[u]);
+            const int64_t beg = __ldg(&g.row_ptr[u]);
+            const int64_t end = __ldg(&g.row_ptr[u + 1]);
+            for (int64_t e0 = beg; e0 < end; e0 += 32) {
+                const int64_t e = e0 + lane;
+                bool ready = false;
+                int x = 0;
+                if (e < end) {
+                    const Arc a = ldg_arc(&g.arcs[e]);
+                    x = a.col;
+                    ready = on_dag(du, a.len, __ldcg(&dist[x])) && atomicSub(&cnt[x], 1u) == 1u;
+                }
+                plain_push(ready, x, lane, list + start + len, &s.next_len);
+            }
+        }
+        __syncthreads();
+        const int next = start + len;
+        const int next_len = s.next_len;
+        for (int i = warp; i < next_len; i += nwarps) {
+            const int x = __ldcg(&list[next + i]);
+            const unsigned long long dx = __ldcg(&dist[x]);
+            const int64_t beg = __ldg(&rg.row_ptr[x]);
+            const int64_t end = __ldg(&rg.row_ptr[x + 1]);
+            double acc = 0.0;
+            for (int64_t e = beg + lane; e < end; e += 32) {
+                const Arc a = ldg_arc(&rg.arcs[e]);
+                if (on_dag(__ldcg(&dist[a.col]), a.len, dx)) {
+                    acc += __ldcg(&sigma[a.col]);
+                }
+            }
+            acc = warp_sum_fixed_order(acc);
+            if (lane == 0) {
+                sigma[x] = acc;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            loff[level + 2] = next + next_len;
+            s.level = level + 1u;
+            s.next_len = 0;
+        }
+        __syncthreads();
+    }
+    // dependencies, from the last level to the source's
+    for (int level = static_cast<int>(s.level) - 1; level >= 0; --level) {
+        const int start = loff[level];
+        const int len = loff[level + 1] - start;
+        for (int i = warp; i < len; i += nwarps) {
+            const int u = __ldcg(&list[start + i]);
+            const unsigned long long du = __ldcg(&dist[u]);
+            const double su = __ldcg(&sigma[u]);
+            const int64_t beg = __ldg(&g.row_ptr[u]);
+            const int64_t end = __ldg(&g.row_ptr[u + 1]);
+            double acc = 0.0;
+            for (int64_t e = beg + lane; e < end; e += 32) {
+                const Arc a = ldg_arc(&g.arcs[e]);
+                if (on_dag(du, a.len, __ldcg(&dist[a.col]))) {
+                    acc += su * ((1.0 + __ldcg(&delta[a.col])) / __ldcg(&sigma[a.col]));
+                }
+            }
+            acc = warp_sum_fixed_order(acc);
+            if (lane == 0) {
+                delta[u] = acc;
+                if (u != src && acc != 0.0) {
+                    unsigned long long lo, hi;
+                    fixed_parts(acc, lo, hi);
+                    fixed_add_parts(&bc[2 * static_cast<int64_t>(u)], lo, hi);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <bool kBrandes>
+__global__ void __launch_bounds__(512, 2) sssp_plain_kernel(const SsspParams p, const BrandesParams b) {
     extern __shared__ __align__(16) unsigned long long smem[];
     const int nwarps_max = 16;
     unsigned long long* s_acc_sum = smem;                             // nwarps_max * kAccDigits (one per warp)
@@ -1237,6 +1370,10 @@ __global__ void __launch_bounds__(512, 2) sssp_plain_kernel(const SsspParams p) 
         }
         if (s.stop != 0) {
             break;
+        }
+        if constexpr (kBrandes) {
+            plain_brandes(p.g, b.rg, n, src, dist, b.ws_sigma + slot * n, b.ws_delta + slot * n, b.ws_cnt + slot * n, b.ws_list + slot * n,
+                          b.ws_loff + slot * (n + 2), b.bc, s, tid, lane, warp, nwarps);
         }
 
         // epilogue: one accumulator pair per warp, combined exactly
