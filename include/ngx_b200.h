@@ -90,7 +90,8 @@ typedef struct {
     int mode;                /* ngx_mode */
     const int64_t* sources;  /* host list of source vertices, or NULL for all n in id order */
     int64_t num_sources;     /* entries in sources (ignored when sources is NULL) */
-    double delta;            /* bucket width of the delta-stepping; <= 0 picks one from the arc lengths */
+    double delta;            /* bucket width of the delta-stepping; <= 0: the tuned width, else 2 / sqrt(mean out-degree)
+                                x the mean arc length (the factor clamped to 0.125-2) */
     int block_threads;       /* threads per CTA; 0 picks the default */
     int ctas_per_sm;         /* concurrent CTAs per SM; 0 picks the default (bounded by the memory budget) */
     int64_t hist_bins;       /* bins of the shortest-path distance histogram; 0 = no histogram */
@@ -293,7 +294,8 @@ typedef struct {
     int task;               /* ngx_task: APSP summaries; + Brandes betweenness; + CPL / efficiency gradient */
     int metric;             /* ngx_metric (APSP only; betweenness and the gradient use |w|) */
     double delta_scale;     /* bucket width = delta_scale x the graph's mean arc length; <= 0: its size class's tuned
-                               scale (1.0 until ngx_batch_autotune has run) */
+                               scale, or before ngx_batch_autotune has run 2 / sqrt(the graph's mean out-degree),
+                               clamped to 0.125-2 */
     int block_threads;      /* 0 = default */
     int64_t hist_bins;      /* distance histogram bins per graph; 0 = none */
     double hist_max;        /* histogram bound, the same for all graphs; must be > 0 when hist_bins > 0 */

@@ -70,7 +70,8 @@ std::vector<GraphDesc> graph_table(const ngx_graph* g, int metric, double delta_
     std::vector<GraphDesc> descs(g->parts.size());
     for (size_t i = 0; i < g->parts.size(); ++i) {
         const GraphPart& part = g->parts[i];
-        const double scale = delta_scale > 0.0 ? delta_scale : (g->class_scale[size_class(part.n)] > 0.0 ? g->class_scale[size_class(part.n)] : 1.0);
+        const double scale = delta_scale > 0.0 ? delta_scale : (g->class_scale[size_class(part.n)] > 0.0 ? g->class_scale[size_class(part.n)]
+                                                                                     : default_delta_scale(part.n, part.m_stored));
         const double mean = metric == NGX_METRIC_INVERSE ? part.mean_len_inverse : part.mean_len_regular;
         descs[i] = GraphDesc{ part.n, part.m_stored, part.row_off, part.vertex_off, part.n, part.vertex_off, pick_delta(mean, 0.0, scale) };
     }
@@ -497,8 +498,9 @@ int ngx_batch_autotune(ngx_graph* g, int task, double* class_scales) {
                 }
             }
             int best_group = 1;
-            for (const int gs : { 2, 4 }) {
-                // groups of several CTAs per tile run with the default block shape
+            for (const int gs : { 0, 2, 4 }) {
+                // groups of several CTAs per tile run with the default block shape; 0 = the library's own rule (by L2
+                // residency and the slots memory affords), which is what a run with tile_ctas 0 gets
                 aopts.block_threads = kShapes[0].block;
                 aopts.ctas_per_sm = kShapes[0].per_sm;
                 aopts.tile_ctas = gs;

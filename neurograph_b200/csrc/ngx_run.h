@@ -57,6 +57,11 @@ struct DagOutputs {
 int check_opts(const ngx_graph* g, const ngx_apsp_opts* opts);
 int run_apsp(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* result, double* rows, int tile_mode, DagOutputs* extra);
 int prepare_sources(const ngx_graph* g, const ngx_apsp_opts* opts, std::vector<int32_t>& sources);
+// Bucket width when the caller gives none, as a multiple of the mean arc length: 2 / sqrt(mean out-degree), clamped
+// to 0.125-2. Dense graphs want narrow buckets (many arcs relax into each bucket: a wide one re-relaxes more pairs),
+// sparse ones wide buckets (few arcs per bucket: a narrow one runs many nearly empty phases). Measured best widths:
+// 0.15-0.25 x the mean at out-degree 100, 0.5 on a batch of out-degree 5-60, 1.0 or more at out-degree 6.
+double default_delta_scale(int64_t n, int64_t m);
 double pick_delta(double mean_len, double requested, double scale);
 int alloc_outputs(ngx_graph* g, int64_t num_graphs, int64_t num_sources, int64_t hist_bins, bool want_rows, RunOutputs& o, bool persistent);
 void free_outputs(ngx_graph* g, RunOutputs& o);

@@ -138,7 +138,8 @@ int run_apsp_noalloc(ngx_graph* g, const ngx_apsp_opts* opts, ngx_apsp_result* r
     o.num_sources = k;
 
     const GraphPart& part = g->parts[0];
-    const double delta = pick_delta(opts->metric == NGX_METRIC_INVERSE ? part.mean_len_inverse : part.mean_len_regular, opts->delta, 1.0);
+    const double delta = pick_delta(opts->metric == NGX_METRIC_INVERSE ? part.mean_len_inverse : part.mean_len_regular, opts->delta,
+                                    default_delta_scale(part.n, part.m_stored));
     const GraphDesc desc{ part.n, part.m_stored, part.row_off, 0, k, part.vertex_off, delta };
     NGX_CUDA_TRY(cudaMemsetAsync(scratch, 0, zeroed, g->stream));
     NGX_CUDA_TRY(cudaMemcpyAsync(o.graphs, &desc, sizeof(desc), cudaMemcpyHostToDevice, g->stream));

@@ -53,6 +53,12 @@ int prepare_sources(const ngx_graph* g, const ngx_apsp_opts* opts, std::vector<i
     return NGX_OK;
 }
 
+double default_delta_scale(int64_t n, int64_t m) {
+    const double degree = n > 0 ? static_cast<double>(m) / static_cast<double>(n) : 1.0;
+    const double scale = 2.0 / std::sqrt(degree > 1.0 ? degree : 1.0);
+    return scale < 0.125 ? 0.125 : (scale > 2.0 ? 2.0 : scale);
+}
+
 double pick_delta(double mean_len, double requested, double scale) {
     if (requested > 0.0 && std::isfinite(requested)) {
         return requested;
@@ -626,7 +632,8 @@ int run_sources(ngx_graph* g, const ngx_apsp_opts* opts, int tile_mode, const st
         return rc;
     }
     const GraphPart& part = g->parts[0];
-    const double delta = pick_delta(opts->metric == NGX_METRIC_INVERSE ? part.mean_len_inverse : part.mean_len_regular, opts->delta, 1.0);
+    const double delta = pick_delta(opts->metric == NGX_METRIC_INVERSE ? part.mean_len_inverse : part.mean_len_regular, opts->delta,
+                                    default_delta_scale(part.n, part.m_stored));
     const GraphDesc desc{ part.n, part.m_stored, part.row_off, 0, num_sources, part.vertex_off, delta };
     NGX_CUDA_TRY(cudaMemsetAsync(o.block, 0, o.zeroed_bytes, g->stream));
     NGX_CUDA_TRY(cudaMemcpyAsync(o.graphs, &desc, sizeof(desc), cudaMemcpyHostToDevice, g->stream));

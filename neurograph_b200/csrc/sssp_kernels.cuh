@@ -151,10 +151,12 @@ __device__ __forceinline__ Group<TileShared> tile_group(const Params& p, TileSha
                               static_cast<int>(blockIdx.x % p.group_size), p.error };
 }
 
-// Queue entries a warp takes at a time: all 32 when the near queue is long, fewer towards the end of a frontier so
-// that the group's warps share it evenly.
-__device__ __forceinline__ int expand_chunk(int qlen, int group_warps) {
-    const int c = qlen / (2 * group_warps);
+// Queue entries a warp takes at a time (guided self-scheduling): the entries not yet handed out over twice the group's
+// warps, clamped to 1..32, so a near iteration starts with large chunks (one round of loads serves many entries) and
+// ends with single entries (a vertex expansion takes tens of microseconds: a coarse last chunk would leave the other
+// warps of the group waiting at the barrier that closes the iteration).
+__device__ __forceinline__ int expand_chunk(int remaining, int group_warps) {
+    const int c = remaining / (2 * group_warps);
     return c < 1 ? 1 : (c > 32 ? 32 : c);
 }
 
@@ -309,20 +311,25 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
     }
 }
 
-// One near iteration of a tile: the warps of the group take the queue `chunk` entries at a time from a shared counter;
+// One near iteration of a tile: the warps of the group take the queue in chunks (expand_chunk) from a shared counter;
 // lane j fetches entry j's vertex, its pending mask, far marks and row offsets (one round of parallel loads), clears the
 // mask and the superseded far marks, and the warp then expands the vertices one after another.
 template <int kUnroll, bool kTrack, bool kReach>
-__device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* q_cur, int qlen, int lane, int* grab, int chunk,
+__device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* q_cur, int qlen, int lane, int* grab, int group_warps,
                                              unsigned long long* __restrict__ dist, uint32_t* pend_cur, uint32_t* pend_nxt, uint32_t* far,
                                              double theta, unsigned long long& expansions, unsigned long long& lane_expansions,
                                              unsigned long long* pred_key, uint32_t* tie, unsigned long long* last, const Reach& reach) {
     for (;;) {
         int base = 0;
+        int chunk = 0;
         if (lane == 0) {
+            // the grab counter is in shared memory for single-CTA tiles and in global memory for groups: a volatile
+            // generic load reads either (for global memory, from L2)
+            chunk = expand_chunk(qlen - *reinterpret_cast<volatile int*>(grab), group_warps);
             base = atomicAdd(grab, chunk);
         }
         base = __shfl_sync(kFullMask, base, 0);
+        chunk = __shfl_sync(kFullMask, chunk, 0);
         if (base >= qlen) {
             break;
         }
@@ -580,7 +587,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) tile_kernel(const SsspPara
                 const int32_t* q_cur = cur ? q1 : q0;
                 int32_t* q_nxt = cur ? q0 : q1;
                 const double theta = s.theta;
-                expand_queue<kUnroll, kMode != kModeApsp, kReach>(g, q_cur, qlen, lane, &ctl()->grab, expand_chunk(qlen, NGX_GWARPS), dist, pend_cur, pend_nxt,
+                expand_queue<kUnroll, kMode != kModeApsp, kReach>(g, q_cur, qlen, lane, &ctl()->grab, NGX_GWARPS, dist, pend_cur, pend_nxt,
                                                           far, theta, expansions, lane_expansions, reinterpret_cast<unsigned long long*>(sigma), tie,
                                                           reinterpret_cast<unsigned long long*>(delta), reach);
                 sync([&](volatile TileShared& c) {

@@ -79,7 +79,7 @@ int ngx_graph_autotune(ngx_graph* g, int task, int64_t sample_sources, ngx_tunin
         const int64_t wave = static_cast<int64_t>(g->sm_count) * 2 * kTile;
         const int64_t k = std::min<int64_t>(g->n, sample_sources > 0 ? sample_sources : wave);
         if (k == 0) {
-            t.delta_scale = 1.0;
+            t.delta_scale = default_delta_scale(g->parts[0].n, g->parts[0].m_stored);
             t.block_threads = 512;
             t.ctas_per_sm = 2;
             t.tile_ctas = 1;

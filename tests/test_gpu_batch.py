@@ -174,7 +174,8 @@ def test_autotune_keeps_results():
         after, _ = b.run("apsp")
     # one launch shape for the whole batch
     assert (shape["block_threads"], shape["ctas_per_sm"]) in ((512, 2), (384, 2), (256, 3), (256, 4)), shape
-    assert shape["tile_ctas"] in (1, 2, 4) and shape["trials"] == 6 and shape["gteps"] > 0, shape
+    # 0: the library's own group rule won the trials
+    assert shape["tile_ctas"] in (0, 1, 2, 4) and shape["trials"] == 7 and shape["gteps"] > 0, shape
     classes = {int(np.floor(np.log2(n))) for n, *_ in graphs if n > 0}
     for c in range(ngx.SIZE_CLASSES):
         if c in classes:
