@@ -86,7 +86,8 @@ def parse():
                          "handle; scc: strongly connected components of the connectome (ngx_scc) beside the reference's SCC; "
                          "c1: the plain small integer-weight connectome (N=5000), all sources per step, beside the reference "
                          "itself built from source")
-    ap.add_argument("--delta", type=float, default=0.25)
+    ap.add_argument("--delta", type=float, default=0.0,
+                    help="bucket width; 0 = the library's default (2/sqrt(mean out-degree) x the mean arc length)")
     ap.add_argument("--mode", choices=["brandes", "apsp", "grad", "plain"], default="brandes",
                     help="what one step runs: APSP+Brandes (the headline), APSP only, APSP+gradient, or the plain per-source form")
     ap.add_argument("--block-threads", type=int, default=0, help="tile kernel block size (0 = the library default)")
@@ -99,7 +100,6 @@ def parse():
         # every step is the whole all-sources job of the small graph; the bucket width follows the integer weights
         args.n, args.degree, args.length_scale = WORKLOAD_C1["n"], WORKLOAD_C1["mean_degree"], WORKLOAD_C1["length_scale"]
         args.sources_per_step = WORKLOAD_C1["n"]
-        args.delta = 0.0
     return args
 
 
