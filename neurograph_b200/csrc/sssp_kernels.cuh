@@ -173,6 +173,57 @@ struct Reach {
     }
 };
 
+// The relaxations of kUnroll (arc, source) pairs per lane, their loads done: pair u relaxes d[x[u]][src[u]] with nd[u]
+// (cur[u] = the distance read before). The atomic minima are issued back to back and waited for together (APSP mode:
+// not waited for at all), then the marks; see batched_expand for what each mode does with an improvement.
+template <int kUnroll, bool kTrack, bool kReach>
+__device__ __forceinline__ void relax_pairs(const int (&x)[kUnroll], const int (&src)[kUnroll], const double (&nd)[kUnroll],
+                                            unsigned long long (&cur)[kUnroll], const uint32_t (&eidx)[kUnroll], const bool (&valid)[kUnroll],
+                                            unsigned long long* __restrict__ dist, uint32_t* pend_nxt, uint32_t* far, double theta,
+                                            unsigned long long* pred_key, uint32_t* tie, const Reach& reach) {
+    // the atomic minima (cur[u] becomes the old value where it is waited for)
+    bool tried[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+        const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd[u]));
+        tried[u] = valid[u] && nb < cur[u];
+        if (tried[u]) {
+            if constexpr (kTrack) {
+                cur[u] = atomicMin(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]], nb);
+            } else {
+                atomicMin(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]], nb);
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+        const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd[u]));
+        if (tried[u]) {
+            const unsigned long long old = cur[u];
+            if constexpr (kTrack) {
+                if (nb < old) {
+                    atomicMin(&pred_key[static_cast<int64_t>(x[u]) * kTile + src[u]], ((nb >> 32) << 32) | eidx[u]);
+                } else if (nb == old) {
+                    atomicOr(&tie[x[u]], 1u << src[u]);
+                }
+            }
+            if (nb < old) {
+                const uint32_t bit = 1u << src[u];
+                if (kReach && old == kInfBits) {
+                    reach.add(x[u], bit);  // the first distance of (x, s): x joins the tile's reached vertices
+                }
+                if (nd[u] < theta) {
+                    atomicOr(&pend_nxt[x[u]], bit);
+                } else {
+                    atomicOr(&far[x[u]], bit);
+                }
+            }
+        } else if (kTrack && valid[u] && nb == cur[u]) {
+            atomicOr(&tie[x[u]], 1u << src[u]);
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------------------ batched form
 // Expands vertex v for the k sources pending on it. The deg(v) x k (arc, source) pairs are spread over the 32 lanes:
 // pair p = 32 i + lane takes arc p / k and the (p % k)-th pending source, so no lane idles when few sources are
@@ -267,53 +318,117 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
                 a += 1;
             }
         }
-        // the atomic minima (cur[u] becomes the old value where it is waited for)
-        bool tried[kUnroll];
+        relax_pairs<kUnroll, kTrack, kReach>(x, src, nd, cur, eidx, valid, dist, pend_nxt, far, theta, pred_key, tie, reach);
+    }
+}
+
+// Queue entries with fewer (arc, pending source) pairs than this fill less than one iteration of batched_expand's
+// pair loop (32 lanes x kUnroll pairs); consecutive ones are expanded together by packed_expand.
+constexpr int kPackPairs = 128;
+
+// Expands a group of m small queue entries together, so that one iteration of the pair loop serves several vertices.
+// Lane i < m holds entry i: its vertex gv, pending mask gmask (non-zero), first arc gbeg and out-degree gdeg; the
+// entries have at most 32 pending sources in all. Lane t then holds the t-th (entry, pending source) of the group and
+// that source's distance to the entry's vertex, and the group's pairs are dealt to the lanes entry after entry: pair
+// q of entry i (0 <= q < k_i deg_i) is arc q / k_i with the (q % k_i)-th pending source, as in batched_expand. The
+// relaxations, the repeat check of the DAG modes (a repeated (vertex, source) only drops its own pairs here) and the
+// counters are batched_expand's.
+template <int kUnroll, bool kTrack, bool kReach>
+__device__ __forceinline__ void packed_expand(const DeviceCsr& g, int m, int gv, uint32_t gmask, int64_t gbeg, int gdeg, int lane,
+                                              unsigned long long* __restrict__ dist, uint32_t* pend_nxt, uint32_t* far, double theta,
+                                              unsigned long long& expansions, unsigned long long& lane_expansions, unsigned long long* pred_key,
+                                              uint32_t* tie, unsigned long long* last, const Reach& reach) {
+    // per entry (lane i < m): pending sources k_i, pairs, offsets of its ranks and pairs in the group, 16-bit reciprocal
+    const int ki = lane < m ? __popc(gmask) : 0;
+    const int pi = lane < m ? ki * gdeg : 0;
+    int kinc = ki, pinc = pi;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int ku = __shfl_up_sync(kFullMask, kinc, off);
+        const int pu = __shfl_up_sync(kFullMask, pinc, off);
+        if (lane >= off) {
+            kinc += ku;
+            pinc += pu;
+        }
+    }
+    const int ri = kinc - ki;
+    const int si = pinc - pi;
+    const int ktot = __shfl_sync(kFullMask, kinc, 31);
+    const int ptot = __shfl_sync(kFullMask, pinc, 31);
+    // floor(q / k) = (q * ceil(2^16 / k)) >> 16 exactly for q < 2^7 and k <= 32
+    const int mgi = lane < m ? (65536 + ki - 1) / ki : 0;
+    // lane t < ktot: its entry (the number of entries whose ranks start at or below t, minus one) and rank
+    const unsigned starts = __reduce_or_sync(kFullMask, lane < m ? (1u << ri) : 0u);
+    const int et = lane < ktot ? __popc(starts & ((2u << lane) - 1u)) - 1 : 0;
+    const uint32_t emask = __shfl_sync(kFullMask, gmask, et);
+    const int ev = __shfl_sync(kFullMask, gv, et);
+    const int er = __shfl_sync(kFullMask, ri, et);
+    const int rank_src = lane < ktot ? static_cast<int>(__fns(emask, 0, lane - er + 1)) : 0;
+    const unsigned long long rank_bits = __ldcg(&dist[static_cast<int64_t>(ev) * kTile + rank_src]);
+    bool rank_ok = lane < ktot;
+    if constexpr (kTrack) {
+        unsigned long long* const slot = &last[static_cast<int64_t>(ev) * kTile + rank_src];
+        if (rank_ok && __ldcg(slot) == rank_bits) {
+            rank_ok = false;  // expanded with this distance already
+        } else if (rank_ok) {
+            *slot = rank_bits;
+        }
+    }
+    const unsigned ok_mask = __ballot_sync(kFullMask, rank_ok);
+    if (ok_mask == 0u) {
+        return;
+    }
+    expansions += static_cast<unsigned long long>(m);
+    lane_expansions += static_cast<unsigned long long>(__popc(ok_mask));
+    const double rank_dv = __longlong_as_double(static_cast<long long>(rank_bits));
+    if (lane < m) {
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(g.arcs + gbeg));
+    }
+    for (int p0 = 0; p0 < ptot; p0 += 32 * kUnroll) {
+        int x[kUnroll];
+        int src[kUnroll];
+        double nd[kUnroll];
+        unsigned long long cur[kUnroll];
+        uint32_t eidx[kUnroll];
+        bool valid[kUnroll];
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
-            const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd[u]));
-            tried[u] = valid[u] && nb < cur[u];
-            if (tried[u]) {
-                if constexpr (kTrack) {
-                    cur[u] = atomicMin(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]], nb);
-                } else {
-                    atomicMin(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]], nb);
-                }
-            }
-        }
+            const int q = p0 + u * 32 + lane;
+            // the entry of pair q: the last one whose pairs start at or below q
+            int e = 0;
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-            const unsigned long long nb = static_cast<unsigned long long>(__double_as_longlong(nd[u]));
-            if (tried[u]) {
-                const unsigned long long old = cur[u];
-                if constexpr (kTrack) {
-                    if (nb < old) {
-                        atomicMin(&pred_key[static_cast<int64_t>(x[u]) * kTile + src[u]], ((nb >> 32) << 32) | eidx[u]);
-                    } else if (nb == old) {
-                        atomicOr(&tie[x[u]], 1u << src[u]);
-                    }
-                }
-                if (nb < old) {
-                    const uint32_t bit = 1u << src[u];
-                    if (kReach && old == kInfBits) {
-                        reach.add(x[u], bit);  // the first distance of (x, s): x joins the tile's reached vertices
-                    }
-                    if (nd[u] < theta) {
-                        atomicOr(&pend_nxt[x[u]], bit);
-                    } else {
-                        atomicOr(&far[x[u]], bit);
-                    }
-                }
-            } else if (kTrack && valid[u] && nb == cur[u]) {
-                atomicOr(&tie[x[u]], 1u << src[u]);
+            for (int step = 16; step > 0; step >>= 1) {
+                const int c = e + step;
+                const int sc = __shfl_sync(kFullMask, si, c & 31);
+                e = (c < m && sc <= q) ? c : e;
+            }
+            const int local = q - __shfl_sync(kFullMask, si, e);
+            const int ke = __shfl_sync(kFullMask, ki, e);
+            const int a = (local * __shfl_sync(kFullMask, mgi, e)) >> 16;
+            const int t = (__shfl_sync(kFullMask, ri, e) + local - a * ke) & 31;
+            const int64_t beg_e = __shfl_sync(kFullMask, gbeg, e);
+            src[u] = __shfl_sync(kFullMask, rank_src, t);
+            const double dvs = __shfl_sync(kFullMask, rank_dv, t);
+            valid[u] = q < ptot && ((ok_mask >> t) & 1u);
+            eidx[u] = static_cast<uint32_t>(beg_e + a);
+            x[u] = 0;
+            nd[u] = 0.0;
+            cur[u] = 0ull;
+            if (valid[u]) {
+                const Arc arc = ldg_arc(&g.arcs[beg_e + a]);
+                x[u] = arc.col;
+                nd[u] = __dadd_rn(dvs, arc.len);
+                cur[u] = __ldcg(&dist[static_cast<int64_t>(x[u]) * kTile + src[u]]);
             }
         }
+        relax_pairs<kUnroll, kTrack, kReach>(x, src, nd, cur, eidx, valid, dist, pend_nxt, far, theta, pred_key, tie, reach);
     }
 }
 
 // One near iteration of a tile: the warps of the group take the queue in chunks (expand_chunk) from a shared counter;
 // lane j fetches entry j's vertex, its pending mask, far marks and row offsets (one round of parallel loads), clears the
-// mask and the superseded far marks, and the warp then expands the vertices one after another.
+// mask and the superseded far marks, and the warp then expands the vertices one after another: one at a time when a
+// vertex has a loop iteration's worth of (arc, source) pairs or more, else with its small neighbours in the chunk.
 template <int kUnroll, bool kTrack, bool kReach>
 __device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* q_cur, int qlen, int lane, int* grab, int group_warps,
                                              unsigned long long* __restrict__ dist, uint32_t* pend_cur, uint32_t* pend_nxt, uint32_t* far,
@@ -352,16 +467,53 @@ __device__ __forceinline__ void expand_queue(const DeviceCsr& g, const int32_t* 
                 }
             }
         }
-        for (int j = 0; j < count; ++j) {
-            const uint32_t amask = __shfl_sync(kFullMask, mj, j);
-            if (amask == 0u) {
-                continue;
+        // entries with fewer pairs than one loop iteration holds go in groups (packed_expand), the others one by one
+        const int kj = __popc(mj);
+        const unsigned any_mask = __ballot_sync(kFullMask, lane < count && mj != 0u);
+        const unsigned small_mask = __ballot_sync(kFullMask, lane < count && mj != 0u && kj * dj < kPackPairs);
+        int j = 0;
+        while (j < count) {
+            const unsigned rest = any_mask & ~((1u << j) - 1u);
+            if (rest == 0u) {
+                break;
             }
-            const int v = __shfl_sync(kFullMask, vj, j);
-            const int64_t beg = __shfl_sync(kFullMask, bj, j);
-            const int deg = __shfl_sync(kFullMask, dj, j);
-            batched_expand<kUnroll, kTrack, kReach>(g, v, amask, beg, deg, lane, dist, pend_nxt, far, theta, expansions, lane_expansions,
-                                                    pred_key, tie, last, reach);
+            j = __ffs(rest) - 1;  // the next entry with pending sources
+            unsigned fit = 0u;
+            if ((small_mask >> j) & 1u) {
+                // the small entries from j up to the next large one, as many as hold 32 pending sources
+                const unsigned large_after = any_mask & ~small_mask & ~((1u << j) - 1u);
+                const int stop = large_after != 0u ? __ffs(large_after) - 1 : 32;
+                const unsigned run = small_mask & ~((1u << j) - 1u) & (stop >= 32 ? kFullMask : ((1u << stop) - 1u));
+                const bool in_run = (run >> lane) & 1u;
+                int kin = in_run ? kj : 0;
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const int ku = __shfl_up_sync(kFullMask, kin, off);
+                    if (lane >= off) {
+                        kin += ku;
+                    }
+                }
+                fit = __ballot_sync(kFullMask, in_run && kin <= 32);
+            }
+            if (__popc(fit) > 1) {
+                const int m = __popc(fit);
+                const int sl = lane < m ? static_cast<int>(__fns(fit, 0, lane + 1)) : 0;
+                const int gv = __shfl_sync(kFullMask, vj, sl);
+                const uint32_t gmask = __shfl_sync(kFullMask, mj, sl);
+                const int64_t gbeg = __shfl_sync(kFullMask, bj, sl);
+                const int gdeg = __shfl_sync(kFullMask, dj, sl);
+                packed_expand<kUnroll, kTrack, kReach>(g, m, gv, gmask, gbeg, gdeg, lane, dist, pend_nxt, far, theta, expansions,
+                                                       lane_expansions, pred_key, tie, last, reach);
+                j = 32 - __clz(fit);
+            } else {
+                const uint32_t amask = __shfl_sync(kFullMask, mj, j);
+                const int v = __shfl_sync(kFullMask, vj, j);
+                const int64_t beg = __shfl_sync(kFullMask, bj, j);
+                const int deg = __shfl_sync(kFullMask, dj, j);
+                batched_expand<kUnroll, kTrack, kReach>(g, v, amask, beg, deg, lane, dist, pend_nxt, far, theta, expansions, lane_expansions,
+                                                        pred_key, tie, last, reach);
+                ++j;
+            }
         }
     }
 }
