@@ -456,7 +456,9 @@ int ngx_batch_autotune(ngx_graph* g, int task, double* class_scales) {
                 continue;
             }
             double best_rate = -1.0, best_scale = 1.0;
-            for (const double scale : kScales) {
+            const GraphPart& probe_part = g->parts[static_cast<size_t>(probe[static_cast<size_t>(c)])];
+            const double own = default_delta_scale(probe_part.n, probe_part.m_stored);  // the untuned width, tried too
+            for (const double scale : { own, kScales[0], kScales[1], kScales[2], kScales[3], kScales[4], kScales[5] }) {
                 double rate = 0.0;
                 if (const int rc = time_wave(g, mode, probe[static_cast<size_t>(c)], scale, aopts, &rate); rc != NGX_OK) {
                     return rc;

@@ -90,24 +90,24 @@ int ngx_graph_autotune(ngx_graph* g, int task, int64_t sample_sources, ngx_tunin
         }
         const std::vector<int64_t> sources(g->source_order.begin(), g->source_order.begin() + k);
         const double mean = g->parts[0].mean_len_regular;
-        static const double kScales[] = { 0.125, 0.25, 0.5, 1.0, 2.0 };
+        // bucket widths: the library's default for this graph's degree first, then fixed multiples of the mean length
+        const double kScales[] = { default_delta_scale(g->parts[0].n, g->parts[0].m_stored), 0.125, 0.25, 0.5, 1.0, 2.0 };
         static const Shape kShapes[] = { { 512, 2 }, { 384, 2 }, { 256, 3 }, { 256, 4 } };
         const int tiles = static_cast<int>((k + kTile - 1) / kTile);
-        // CTAs per tile: 1 (the trials above), 2, 4, 8, the library's own choice for this sample (0), and the size at
-        // which the sample's tiles fill the resident CTAs
-        std::vector<int> groups = { 1, 2, 4, 8, 0 };
+        // CTAs per tile: the library's own choice (0: the bucket-width trials run with it, as untuned runs do), 1, 2,
+        // 4, 8, and the size at which the sample's tiles fill the resident CTAs
+        std::vector<int> groups = { 1, 2, 4, 8 };
         const int resident = g->sm_count * 2;
         if (tiles < resident) {
             groups.push_back(std::max(1, resident / tiles));
         }
         std::sort(groups.begin(), groups.end());
         groups.erase(std::unique(groups.begin(), groups.end()), groups.end());
-        groups.erase(std::remove(groups.begin(), groups.end(), 1), groups.end());
 
         double best_rate = -1.0;
         double scale = 1.0;
         Shape shape = kShapes[0];
-        int tile_ctas = 1;
+        int tile_ctas = 0;
         int trials = 0;
         // one parameter at a time: bucket width, then block shape, then CTAs per tile
         for (const double sc : kScales) {
@@ -137,9 +137,6 @@ int ngx_graph_autotune(ngx_graph* g, int task, int64_t sample_sources, ngx_tunin
         }
         // groups of several CTAs per tile run with the default block shape (512 x 2)
         for (const int gs : groups) {
-            if (gs == 1) {
-                continue;
-            }
             double rate = 0.0;
             if (const int rc = trial(g, task, sources, pick_delta(mean, 0.0, scale), kShapes[0], gs, &rate); rc != NGX_OK) {
                 return rc;

@@ -179,7 +179,8 @@ def test_autotune_keeps_results():
     classes = {int(np.floor(np.log2(n))) for n, *_ in graphs if n > 0}
     for c in range(ngx.SIZE_CLASSES):
         if c in classes:
-            assert scales[c] in (0.125, 0.25, 0.5, 1.0, 2.0, 4.0), (c, scales[c])
+            # a fixed multiple of the mean arc length, or the class's default width (2 / sqrt(mean out-degree))
+            assert 0.125 <= scales[c] <= 4.0, (c, scales[c])
         else:
             assert scales[c] == 0.0
     for i in range(len(graphs)):
