@@ -95,6 +95,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the plain/batched APSP comparison runs")
+    ap.add_argument("--autotune", action="store_true",
+                    help="run the library's autotuner for the mode before the warm-up (outside the timed region) and use its "
+                         "bucket width and block shape for every step, the e2e job included")
     args = ap.parse_args()
     if args.workload == "c1":
         # every step is the whole all-sources job of the small graph; the bucket width follows the integer weights
@@ -792,15 +795,32 @@ def main():
     g.set_stream(stream.cuda_stream)
     # one step = one wave of the all-sources job in the library's order (tiles of nearby sources)
     batches = source_batches(c.n, args.sources_per_step, args.warmup + args.steps, rank, world, order=g.source_order())
+    tuning = None
+    if args.autotune and args.mode in ("apsp", "brandes", "grad"):
+        # the tuned width is passed on as an explicit delta, so that the e2e job's fresh handle runs with it too
+        tuning = g.autotune(args.mode)
+        args.delta = float(tuning["delta_scale"] * g.layout()["mean_lengths"][0])
+        if (tuning["block_threads"], tuning["ctas_per_sm"]) != (512, 2):
+            args.block_threads, args.ctas_per_sm = int(tuning["block_threads"]), int(tuning["ctas_per_sm"])
+        log(f"[bench] autotune: {tuning} -> delta {args.delta:.6g}")
+
+    # page-locked result arrays, allocated once and reused by every step (the device writes them directly, with no
+    # staging copy and no first-touch page faults on freshly allocated host memory)
+    def pinned(size):
+        return torch.empty(max(size, 1), dtype=torch.float64).pin_memory().numpy()
+
+    bc_out = pinned(c.n) if args.mode == "brandes" else None
+    grad_out = (pinned(g.m), pinned(g.m)) if args.mode == "grad" else None
 
     def step(graph, sources, hist_max):
         """One step of the selected mode; returns (result, host outputs)."""
         if args.mode == "brandes":
             bc, r = graph.brandes(sources=sources, delta=args.delta, hist_bins=HIST_BINS, hist_max=hist_max, per_source=True,
-                                  block_threads=args.block_threads, ctas_per_sm=args.ctas_per_sm)
+                                  block_threads=args.block_threads, ctas_per_sm=args.ctas_per_sm, out=bc_out)
             return r, [bc]
         if args.mode == "grad":
-            dcpl, deff, r = graph.apsp_grad(sources=sources, delta=args.delta, block_threads=args.block_threads, ctas_per_sm=args.ctas_per_sm)
+            dcpl, deff, r = graph.apsp_grad(sources=sources, delta=args.delta, block_threads=args.block_threads, ctas_per_sm=args.ctas_per_sm,
+                                            out=grad_out)
             return r, [dcpl, deff]
         mode = "plain" if args.mode == "plain" else "batched"
         r = graph.apsp(sources=sources, mode=mode, delta=args.delta if mode == "batched" else 0.1, hist_bins=HIST_BINS, hist_max=hist_max,
@@ -937,7 +957,8 @@ def main():
         "metric": metric, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * elapsed_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(WORKLOAD, **workload_overrides(args), n=c.n, arcs=c.m, mode=args.mode, sources_per_step=args.sources_per_step, delta=args.delta, hist_bins=HIST_BINS,
+        "config": dict(WORKLOAD, **workload_overrides(args), n=c.n, arcs=c.m, mode=args.mode, sources_per_step=args.sources_per_step, delta=args.delta,
+                       **({"autotune": tuning} if tuning is not None else {}), hist_bins=HIST_BINS,
                        hist_max=hist_max, parallelism=f"sources sharded over {world} GPU(s), no data-path collective",
                        l2=(f"graph ({graph_bytes / 1e6:.1f} MB CSR + reverse CSR) fits in L2: L2 flushed between steps by a "
                            f"{2 * L2_BYTES >> 20} MiB write outside the timed intervals") if flush else

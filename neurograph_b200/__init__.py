@@ -187,6 +187,13 @@ class ApspResult:
         return self.traversed_arcs / (self.kernel_ms * 1e-3) / 1e9 if self.kernel_ms > 0 else 0.0
 
 
+def _out_array(a, size):
+    """A caller's output array, checked: C-contiguous float64 with at least `size` entries."""
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"] or a.size < size or not a.flags["WRITEABLE"]:
+        raise ValueError(f"out arrays must be writeable C-contiguous float64 arrays of at least {size} entries")
+    return a.reshape(-1)
+
+
 class Graph:
     """A graph resident on one GPU (device CSR + reverse CSR)."""
 
@@ -388,20 +395,24 @@ class Graph:
         return rows
 
     def brandes(self, sources=None, delta=0.0, hist_bins=0, hist_max=0.0, per_source=False, block_threads=0,
-                ctas_per_sm=0, max_iterations=0, fixed=False, exact=False, tile_ctas=0, mode="batched"):
+                ctas_per_sm=0, max_iterations=0, fixed=False, exact=False, tile_ctas=0, mode="batched", out=None):
         """Betweenness (sum of pair dependencies over the sources) and the run's APSP result. fixed=True returns the
         unconverted sums instead (ngx_brandes_fixed): an (n, 2) uint64 array of 128-bit fixed-point words.
         mode="plain" runs one source per CTA (the per-source baseline form); its dependencies are summed in another
-        order than the batched form's, so its betweenness agrees with the batched one to rounding, not bit for bit."""
+        order than the batched form's, so its betweenness agrees with the batched one to rounding, not bit for bit.
+        out: a C-contiguous float64 array of at least max(n, 1) entries to write the betweenness into (a view of it is
+        returned)."""
         opts, srcs, k = self._opts(sources, "regular", mode, delta, hist_bins, hist_max, block_threads, ctas_per_sm, max_iterations,
                                    tile_ctas)
         r, hist, per = self._result_struct(hist_bins, per_source, k, exact)
         if fixed:
+            if out is not None:
+                raise ValueError("out= takes converted betweenness; the fixed-point words are returned as a new array")
             words = np.zeros((max(self.n, 1), 2), np.uint64)
             _check(library().ngx_brandes_fixed(self._handle, C.byref(opts), words.ctypes.data, C.byref(r)))
             bc = words[: self.n]
         else:
-            bc = np.zeros(max(self.n, 1), np.float64)
+            bc = _out_array(out, max(self.n, 1)) if out is not None else np.zeros(max(self.n, 1), np.float64)
             _check(library().ngx_brandes(self._handle, C.byref(opts), bc.ctypes.data, C.byref(r)))
             bc = bc[: self.n]
         out = self._result(r, hist, per, k)
@@ -409,18 +420,23 @@ class Graph:
             out.acc_digits = r._digits
         return bc, out
 
-    def apsp_grad(self, sources=None, delta=0.0, block_threads=0, ctas_per_sm=0, max_iterations=0, fixed=False, tile_ctas=0):
+    def apsp_grad(self, sources=None, delta=0.0, block_threads=0, ctas_per_sm=0, max_iterations=0, fixed=False, tile_ctas=0,
+                  out=None):
         """Gradients of CPL and efficiency w.r.t. every arc length, and the run's APSP result. fixed=True returns the
-        unconverted sums instead (ngx_apsp_grad_fixed): two (m, 2) uint64 arrays, before the division by R."""
+        unconverted sums instead (ngx_apsp_grad_fixed): two (m, 2) uint64 arrays, before the division by R.
+        out=(dcpl, deff): two C-contiguous float64 arrays of at least max(m, 1) entries to write into (for instance
+        page-locked ones reused from call to call, which the device writes directly); views of them are returned."""
         opts, srcs, k = self._opts(sources, "regular", "batched", delta, 0, 0.0, block_threads, ctas_per_sm, max_iterations, tile_ctas)
         r, hist, per = self._result_struct(0, False, k)
         if fixed:
+            if out is not None:
+                raise ValueError("out= takes converted gradients; the fixed-point words are returned as new arrays")
             dcpl = np.zeros((max(self.m, 1), 2), np.uint64)
             deff = np.zeros((max(self.m, 1), 2), np.uint64)
             _check(library().ngx_apsp_grad_fixed(self._handle, C.byref(opts), dcpl.ctypes.data, deff.ctypes.data, C.byref(r)))
         else:
-            dcpl = np.zeros(max(self.m, 1), np.float64)
-            deff = np.zeros(max(self.m, 1), np.float64)
+            dcpl, deff = (_out_array(out[0], max(self.m, 1)), _out_array(out[1], max(self.m, 1))) if out is not None else \
+                (np.zeros(max(self.m, 1), np.float64), np.zeros(max(self.m, 1), np.float64))
             _check(library().ngx_apsp_grad(self._handle, C.byref(opts), dcpl.ctypes.data, deff.ctypes.data, C.byref(r)))
         return dcpl[: self.m], deff[: self.m], self._result(r, hist, per, k)
 

@@ -88,3 +88,27 @@ def test_autograd_function_matches_the_adjoint_and_finite_differences():
             vals.append(o[0].item() + 2.0 * o[1].item())
         fd = (vals[0] - vals[1]) / (2 * h)
         assert abs(fd - want[e]) <= 1e-4 * max(1e-12, abs(want[e])) + 1e-9, (e, fd, want[e])
+
+
+def test_caller_output_arrays():
+    """out= writes the gradients (and, for brandes, the betweenness) into the caller's arrays, page-locked ones
+    included, with the same values as freshly allocated outputs; arrays of the wrong kind are refused."""
+    import torch
+
+    c = synth.connectome(600, 8, 0.2, weights="lognormal", seed=17, use_gpu=False)
+    pinned = [torch.empty(c.m, dtype=torch.float64).pin_memory().numpy() for _ in range(3)]
+    with ngx.Graph(c.n, c.row_ptr, c.col, c.w) as g:
+        dcpl, deff, _ = g.apsp_grad()
+        for _ in range(2):  # twice: the arrays are reused
+            a, b, _ = g.apsp_grad(out=(pinned[0], pinned[1]))
+            assert np.array_equal(a, dcpl) and np.array_equal(b, deff)
+            assert a.ctypes.data == pinned[0].ctypes.data
+        bc, _ = g.brandes()
+        bc_out = np.full(c.n, -1.0)
+        bc2, _ = g.brandes(out=bc_out)
+        assert np.array_equal(bc2, bc) and bc2.ctypes.data == bc_out.ctypes.data
+        for bad in (np.zeros(c.m, np.float32), np.zeros(c.m - 1), np.zeros((c.m, 2))[:, 0]):
+            with pytest.raises(ValueError):
+                g.apsp_grad(out=(bad, pinned[2]))
+        with pytest.raises(ValueError):
+            g.brandes(out=bc_out, fixed=True)
