@@ -92,3 +92,15 @@ def test_exact_sums_on_the_host():
     for bad in ([-1.0], [float("nan")], [float("inf")]):
         with pytest.raises(ngx.NgxError):
             ngx.exact_accumulate(bad)
+
+
+def test_caller_output_arrays_are_checked():
+    """out= arrays (betweenness, gradients) must be writeable C-contiguous float64 arrays with room for every entry;
+    anything else is refused before the library is called."""
+    good = np.zeros(8)
+    assert ngx._out_array(good, 8) is not None and ngx._out_array(good, 5).size == 8
+    ro = np.zeros(8)
+    ro.flags.writeable = False
+    for bad in (np.zeros(8, np.float32), np.zeros(7), np.zeros((8, 2))[:, 0], ro, [0.0] * 8):
+        with pytest.raises(ValueError):
+            ngx._out_array(bad, 8)
