@@ -323,8 +323,10 @@ __device__ __forceinline__ void batched_expand(const DeviceCsr& g, int v, uint32
 }
 
 // Queue entries with fewer (arc, pending source) pairs than this fill less than one iteration of batched_expand's
-// pair loop (32 lanes x kUnroll pairs); consecutive ones are expanded together by packed_expand.
+// pair loop (32 lanes x 4 pairs at the library's unroll); consecutive ones are expanded together by packed_expand,
+// whose division of a pair index by the entry's source count is exact only below 2^7 pairs per entry.
 constexpr int kPackPairs = 128;
+static_assert(kPackPairs <= 128, "packed_expand divides pair indices below 2^7 by a 16-bit reciprocal");
 
 // Expands a group of m small queue entries together, so that one iteration of the pair loop serves several vertices.
 // Lane i < m holds entry i: its vertex gv, pending mask gmask (non-zero), first arc gbeg and out-degree gdeg; the
